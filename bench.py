@@ -1,0 +1,308 @@
+#!/usr/bin/env python
+"""Throughput of the B200 DSMC timestep: particle-steps per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+A step is one full timestep of the reference (System::step + sampler,
+dsmc/main.cpp:57-64: accelerate, move with diffuse walls, cell re-binning,
+NTC collide, sampling) over every particle of the workload, which is the
+packed_256 geometry (256^3 voxels, r = 6 voxel spheres to porosity 0.5,
+2^3-voxel cells, 30 simulators per cell, ~3.1e7 particles; seeded synthetic
+geometry from the reference's own generator semantics).  Multi-GPU runs are
+independent replicas (different draw seeds), one per rank: weak scaling.
+
+--impl reference runs the reference's own CPU solver (oracle/_ref/dsmc_ref,
+built from the reference sources) on a bounded sample of the same workload
+on the host cores, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "DSMC particle-steps/s on 1 B200"
+UNIT = "particle-steps/s"
+BYTES_PER_PARTICLE_STEP = 64  # read + write of the 32-byte particle record
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        self.path.unlink(missing_ok=True)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return world, rank, local, pg
+
+
+def allreduce_max(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def cpu_reference(steps: int, replicas: int | None = None):
+    """The reference's own CPU solver on the bounded sample of the workload."""
+    from oracle import run_reference
+    from master_b200 import workloads
+    w = workloads.PACKED_256_SAMPLE
+    s = w.settings(statistics_interval=100)
+    g = w.geometry()
+    cores = replicas or max(1, min(os.cpu_count() or 1, 32))
+    res = run_reference.run_replicas(s, g, timesteps=steps, replicas=cores)
+    mol = res["reports"][0].get("molecules")
+    return {
+        "value": res["particle_steps_per_s"], "unit": UNIT, "cores": cores, "kind": "reference",
+        "sample": (f"{cores} independent single-rank runs of the reference solver (oracle/_ref/dsmc_ref, g++ -O3) on "
+                   f"a 64^3 box of the same voxel size, sphere radius, porosity, gas and simulator weight "
+                   f"({mol} particles each), {steps} timesteps; its own stage timers (moving+colliding+"
+                   f"accelerating+sampling)"),
+    }
+
+
+def run_reference_arm(args, world, rank, pg):
+    if rank != 0:
+        return 0
+    steps = max(args.steps, 1)
+    t0 = time.time()
+    try:
+        cb = cpu_reference(steps=min(steps, 200))
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU solver could not run: {e}"}))
+        return 0
+    line = {
+        "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": min(steps, 200),
+        "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": "packed_256 (bounded 64^3 sample on host cores)", "parallelism": "replicas"},
+        "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.time() - t0,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="packed_256")
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--cpu-steps", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world, rank, local, pg = dist_setup(args)
+    if args.impl == "reference":
+        rc = run_reference_arm(args, world, rank, pg)
+        if pg is not None:
+            pg.destroy_process_group()
+        return rc
+
+    import ctypes as C
+    import torch
+    from master_b200 import capi, workloads
+    from master_b200.system import System
+
+    torch.cuda.set_device(local)
+    lib = capi.load()
+    W = workloads.WORKLOADS[args.workload]
+    settings = W.settings(rng_seed=1000 + rank, statistics_interval=1)
+    geometry = W.geometry()
+    system = System(settings, geometry, device=local)
+    N = system.num_molecules
+    stream = torch.cuda.ExternalStream(lib.dsmc_stream(system.ctx.handle))
+
+    # warm-up (untimed)
+    system.step(args.warmup)
+    system.ctx.sync()
+
+    # ---- device-resident throughput ---------------------------------------
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier(pg)
+        torch.cuda.synchronize()
+        system.ctx.sync()
+        ev0.record(stream)
+        system.step(args.steps)
+        ev1.record(stream)
+        ev1.synchronize()
+        torch.cuda.synchronize()
+        barrier(pg)
+    clocks = clk.summary()
+    ms_rank = ev0.elapsed_time(ev1)
+    ms_max = allreduce_max(pg, ms_rank)
+    n_total = allreduce_sum(pg, float(N))
+    value = n_total * args.steps / (ms_max / 1e3)
+    err, spill = system.ctx.device_status()
+    tal = system.tallies()
+
+    # ---- end to end through the C ABI with host buffers --------------------
+    k_e2e = args.e2e_steps or args.steps
+    r_host, v_host = system.get_particles()
+    r_pin = torch.from_numpy(r_host).pin_memory()
+    v_pin = torch.from_numpy(v_host).pin_memory()
+    r_out = torch.empty_like(r_pin).pin_memory()
+    v_out = torch.empty_like(v_pin).pin_memory()
+    counters = (C.c_int64 * 8)()
+    got = C.c_int64()
+    D = C.POINTER(C.c_double)
+    barrier(pg)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    system.ctx.check(lib.dsmc_particles_set(system.ctx.handle, system.id, N, C.cast(r_pin.data_ptr(), D),
+                                            C.cast(v_pin.data_ptr(), D)))
+    for _ in range(k_e2e):
+        system.ctx.check(lib.dsmc_step(system.ctx.handle, 1))
+        system.ctx.check(lib.dsmc_counters_get(system.ctx.handle, system.id, counters))
+    system.ctx.check(lib.dsmc_particles_get(system.ctx.handle, system.id, N, C.cast(r_out.data_ptr(), D),
+                                            C.cast(v_out.data_ptr(), D), None, C.byref(got)))
+    e2e_s = time.perf_counter() - t0
+    e2e_s = allreduce_max(pg, e2e_s)
+    e2e_value = n_total * k_e2e / e2e_s
+
+    # ---- roofline of the fused pass (the only kernel in the timed loop) -----
+    peak, peak_kind = measured_peaks()
+    achieved = BYTES_PER_PARTICLE_STEP * N * args.steps / (ms_rank / 1e3) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "fused_pass_traffic.json"
+    if tfile.exists():
+        try:
+            t = json.loads(tfile.read_text())
+            traffic = float(t["dram_bytes_per_particle_step"]) * N
+        except Exception:
+            traffic = None
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "fp32 state + fp64 tallies", "data": "synthetic",
+        "config": {"workload": W.name, "voxels": W.n, "cells": W.cells, "particles_per_gpu": N,
+                   "particles_total": int(n_total), "atoms_per_molecule": W.atoms_per_molecule,
+                   "parallelism": f"replicas x{world}", "l2": "particle state 2 x %.1f GB > 126 MB L2" % (
+                       system.info().slots * 32 / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": BYTES_PER_PARTICLE_STEP * N},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48 * N / k_e2e,
+                "d2h_bytes_per_step": (48 * N + 64 * k_e2e) / k_e2e, "steps": k_e2e},
+        "gpu_launches": args.steps,
+        "clocks": clocks,
+        "device_status": {"error_bits": err, "spill": spill},
+        "physics": {"temperature_K": tal.temperature, "collisions": tal.collisions,
+                    "wall_collisions": tal.wall_collisions, "reseeds": tal.reseeds},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_reference(steps=args.cpu_steps)
+        except Exception as e:  # noqa: BLE001
+            line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    system.ctx.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

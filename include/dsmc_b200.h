@@ -1,0 +1,231 @@
+/*
+ * dsmc_b200.h - C ABI of the B200 DSMC timestep (libdsmc_b200.so).
+ *
+ * Drop-in for the timestep of andeplane/master's DSMC solver
+ * (code/base_code/program/dsmc/): the mover with diffuse walls, the cell
+ * re-binning ("sort"), the no-time-counter collide and the sampler that
+ * System::step (dsmc/system.cpp:22-47) and StatisticsSampler::sample
+ * (dsmc/statisticssampler.cpp:42-65) run once per timestep.
+ *
+ * Conventions: plain C types, caller-owned host buffers that are copied in
+ * and out, device memory owned by the context, int status (0 = DSMC_OK), no
+ * exceptions across the boundary.  One context per host thread; calls on a
+ * context are ordered on its CUDA stream and are not re-entrant.  Units are
+ * the reference's reduced units (dsmc/unitconverter.cpp:3-21): length 1 um,
+ * mass 1 amu, energy 1.65088e-21 J.  Arrays of voxels use the reference's
+ * order, index i*ny*nz + j*nz + k (dsmc/grid.h:139-145).
+ */
+#ifndef DSMC_B200_H
+#define DSMC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------- */
+#define DSMC_OK 0
+#define DSMC_ERR_ARG 1         /* bad argument or null pointer */
+#define DSMC_ERR_IO 2          /* file missing, short or malformed */
+#define DSMC_ERR_CUDA 3        /* CUDA runtime error (message in dsmc_last_error) */
+#define DSMC_ERR_CAPACITY 4    /* a size limit of this build was exceeded */
+#define DSMC_ERR_CONFIG 5      /* voxel/cell configuration rejected (dsmc/system.cpp:221-239) */
+#define DSMC_ERR_STATE 6       /* particle state invalid: in solid, non-finite, ... */
+#define DSMC_ERR_NOT_FOUND 7   /* ini key missing (dsmc/cinifile.h:61) */
+#define DSMC_ERR_NO_DEVICE 8   /* no CUDA device, or the kernels were not built for it */
+
+/* ---- precision of a context ---------------------------------------- */
+#define DSMC_PREC_SPLIT32 0    /* int voxel + fp32 offset, fp32 velocity, fp64 tallies */
+#define DSMC_PREC_FP64 1       /* the reference's fp64 positions and arithmetic */
+
+/* ---- settings: the fields of Settings (dsmc/settings.h:11-49) ------- */
+typedef struct dsmc_settings {
+    int timesteps;
+    int statistics_interval;
+    int atoms_per_molecule;     /* F_N, simulator weight (an int in the reference) */
+    int cells_x, cells_y, cells_z;
+    int flow_direction;         /* axis of gravity and flux; <0: none */
+    int sampling_bins;
+    int seed;                   /* reference ini seed */
+    int max_molecules_per_node;
+    int nx, ny, nz;             /* MPI processor grid of the reference; 1 1 1 here */
+    double mass;                /* amu */
+    double temperature;         /* K (SI, as the ini) */
+    double wall_temperature;    /* K */
+    double gravity;             /* reduced acceleration */
+    double density;             /* m^-3 (SI, as the ini) */
+    double diam;                /* um */
+    double Lx, Ly, Lz;          /* um */
+    double dt;                  /* reduced time */
+    double alpha_n, alpha_t;
+    double viscosity;
+    int surface_model;          /* 0 = thermal (diffuse) walls */
+    int sample_begin;           /* first step sampled (0: from the start) */
+    uint64_t rng_seed;          /* key of the counter-based draws */
+    char world[512];            /* world folder (the ini's `world`) */
+} dsmc_settings;
+
+/* Fills the reference's Python-driver defaults (dsmcconfig.py:14-77). */
+int dsmc_settings_defaults(dsmc_settings *s);
+/* Parses a dsmc.ini with the reference's CIniFile rules (dsmc/cinifile.h:28-104):
+ * `key = value` lines, getint = (int)strtod, getbool = "true".  Replaces
+ * Settings::Settings (dsmc/settings.cpp:3-44). */
+int dsmc_settings_load_ini(const char *path, dsmc_settings *s);
+
+/* ---- world files ---------------------------------------------------- */
+typedef struct dsmc_world_header {
+    float porosity_global;
+    float porosity;
+    uint32_t global_nx, global_ny, global_nz;
+    uint32_t nx, ny, nz;        /* stored dimensions (3x the rank's block with halo) */
+} dsmc_world_header;
+
+/* Reads the header of a world file (dsmc/dsmc_io.cpp:183-220). */
+int dsmc_world_read_header(const char *path, dsmc_world_header *h);
+/* Reads a single-rank world file and strips the 3x3x3 periodic halo: the
+ * outputs hold global_nx*global_ny*global_nz voxels (normals etc. 3 floats
+ * each).  Replaces DSMC_IO::read_grid_matrix (dsmc/dsmc_io.cpp:183-220). */
+int dsmc_world_read(const char *path, uint8_t *voxels, float *normals, float *tangents1,
+                    float *tangents2);
+/* Writes world files in the reference layout, one per rank of a px*py*pz
+ * grid, each with its 3x3x3 halo (ComplexGeometry::save_to_file,
+ * dsmc/complexgeometry.cpp:220-318).  folder/%04d.bin and folder/porosity.txt. */
+int dsmc_world_write(const char *folder, uint32_t nx, uint32_t ny, uint32_t nz, const uint8_t *voxels,
+                     const float *normals, const float *tangents1, const float *tangents2, int px,
+                     int py, int pz);
+
+/* ---- geometry generation -------------------------------------------- */
+typedef struct dsmc_sphere_params {
+    int nx, ny, nz;
+    double radius;              /* box-normalised, e.g. 4 voxels / 64 = 0.0625 */
+    int spheres_type;           /* 0: spheres_num spheres; 1: until wanted_porosity */
+    int spheres_num;
+    double wanted_porosity;
+    int seed;                   /* the ini seed; the generator uses -|seed| */
+    int inverted;               /* 1: spheres are solid */
+    int prevent_overlap;
+    int number_of_neighbor_averages;
+} dsmc_sphere_params;
+
+/* Packed-sphere geometry with normals, tangents and boundary voxels,
+ * identical to ComplexGeometry::create_packed_spheres + make_periodic +
+ * calculate_normals + calculate_tangents + find_boundary_points
+ * (dsmc/complexgeometry.cpp:401-513, 853-871, 928-1063).  Outputs hold
+ * nx*ny*nz voxels.  porosity_out: fraction of empty voxels. */
+int dsmc_geometry_packed_spheres(const dsmc_sphere_params *p, uint8_t *voxels, float *normals,
+                                 float *tangents1, float *tangents2, float *porosity_out);
+/* Normals, tangents and boundary typing of an arbitrary solid mask (0/1),
+ * in place (ComplexGeometry::calculate_normals_tangents_and_inner_points,
+ * dsmc/complexgeometry.cpp:196-201).  On the CPU. */
+int dsmc_geometry_finish(uint32_t nx, uint32_t ny, uint32_t nz, int number_of_neighbor_averages,
+                         uint8_t *voxels, float *normals, float *tangents1, float *tangents2);
+/* The same stencil on the GPU (device_id), identical output. */
+int dsmc_geometry_finish_gpu(int device_id, uint32_t nx, uint32_t ny, uint32_t nz,
+                             int number_of_neighbor_averages, uint8_t *voxels, float *normals,
+                             float *tangents1, float *tangents2);
+
+/* ---- context ---------------------------------------------------------- */
+typedef struct dsmc_ctx dsmc_ctx;
+
+int dsmc_ctx_create(int device_id, int precision, dsmc_ctx **out);
+void dsmc_ctx_destroy(dsmc_ctx *ctx);
+/* Message of the last failed call on ctx (or of the last failed context-free
+ * call on this thread when ctx is NULL). */
+const char *dsmc_last_error(const dsmc_ctx *ctx);
+int dsmc_sync(dsmc_ctx *ctx);
+
+/* Adds one system (one geometry and its gas; the reference's System,
+ * dsmc/system.cpp:241-382) from a halo-free voxel grid.  Builds the cells as
+ * System::setup_cells does (dsmc/system.cpp:432-490) and validates the
+ * voxel/cell divisibility (dsmc/system.cpp:221-239).  Returns its id. */
+int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t ny, uint32_t nz,
+                    const uint8_t *voxels, const float *normals, const float *tangents1,
+                    const float *tangents2, float porosity_global, int *sys_id);
+/* Same, reading s->world/0000.bin. */
+int dsmc_system_add_world(dsmc_ctx *ctx, const dsmc_settings *s, int *sys_id);
+
+typedef struct dsmc_system_info {
+    int64_t num_particles;
+    int num_cells_total;
+    int num_active_cells;
+    double volume;              /* effective (empty) volume */
+    double porosity;
+    double atoms_per_molecule;
+    double dt;
+    int64_t expected_particles; /* density*volume/atoms_per_molecule (dsmc/system.cpp:323) */
+    int slots;                  /* particle slots reserved per buffer */
+} dsmc_system_info;
+int dsmc_system_info_get(dsmc_ctx *ctx, int sys_id, dsmc_system_info *info);
+
+/* Maxwellian velocities and uniform positions in empty voxels, as
+ * System::setup_molecules (dsmc/system.cpp:398-430); draws come from one
+ * counter-based stream per particle.  n < 0: the reference's count. */
+int dsmc_particles_init(dsmc_ctx *ctx, int sys_id, int64_t n);
+/* Replaces a system's particles by n particles in the reference's state-file
+ * layout: r[3n], v[3n] fp64 (dsmc/dsmc_io.cpp:82-159).  Particle i gets id i. */
+int dsmc_particles_set(dsmc_ctx *ctx, int sys_id, int64_t n, const double *r, const double *v);
+int dsmc_particles_count(dsmc_ctx *ctx, int sys_id, int64_t *n);
+/* Copies the particles out ordered by id (r[3n], v[3n]; cell: the reference's
+ * global cell index of each particle, may be NULL). */
+int dsmc_particles_get(dsmc_ctx *ctx, int sys_id, int64_t cap, double *r, double *v, int32_t *cell,
+                       int64_t *n);
+
+/* Advances every system by nsteps timesteps: accelerate, move, re-bin,
+ * collide and sample, one fused kernel pass per step (System::step +
+ * StatisticsSampler::sample, dsmc/main.cpp:57-64). */
+int dsmc_step(dsmc_ctx *ctx, int nsteps);
+
+/* The stages of System::step as separate calls, for callers that drive the
+ * stage order themselves (all systems of the context):
+ *   move     = steps += 1; accelerate (dsmc/system.cpp:133-144) + move with
+ *              periodic wrap (dsmc/system.cpp:107-120)
+ *   sort     = update_molecule_cells (dsmc/system.cpp:146-157)
+ *   collide  = prepare + collide of every active cell (dsmc/system.cpp:122-131)
+ *   sample   = the per-cell moment tallies on the sampling cadence */
+int dsmc_stage_move(dsmc_ctx *ctx);
+int dsmc_stage_sort(dsmc_ctx *ctx);
+int dsmc_stage_collide(dsmc_ctx *ctx);
+int dsmc_stage_sample(dsmc_ctx *ctx);
+
+typedef struct dsmc_tallies {
+    uint64_t step;              /* System::steps */
+    uint64_t collisions;        /* System::collisions */
+    uint64_t wall_collisions;   /* ColliderBase::num_collisions */
+    uint64_t reseeds;           /* particles re-seeded by the mover's find_position */
+    uint64_t particle_steps;
+    int64_t count_periodic[3];  /* MoleculeMover::count_periodic */
+    uint64_t samples;           /* sampled steps in the cell moments */
+    uint64_t candidates;        /* NTC candidate pairs */
+    double kinetic_energy;      /* current, reduced units (MeasureEnergy) */
+    double temperature;         /* current, K (MeasureTemperature) */
+    double flux;                /* F_N*count_periodic[flow]/(t - t0) (MeasureNumberFlowRate) */
+    double time;                /* t, reduced */
+} dsmc_tallies;
+int dsmc_tallies_get(dsmc_ctx *ctx, int sys_id, dsmc_tallies *t);
+int dsmc_tallies_reset(dsmc_ctx *ctx, int sys_id);
+
+/* Per active cell: global cell index (dsmc/system.h:130-132), particle count,
+ * vr_max, selection remainder, and 8 fp64 moment sums over the sampled steps
+ * (n, sum vx, vy, vz, sum vx^2, vy^2, vz^2, sum |v|^2).  Any pointer may be NULL. */
+int dsmc_cells_get(dsmc_ctx *ctx, int sys_id, int cap, int32_t *global_index, int32_t *count,
+                   double *vr_max, double *rest, double *moments, double *volume, int *num_cells);
+int dsmc_cells_set_state(dsmc_ctx *ctx, int sys_id, const double *vr_max, const double *rest);
+
+/* Reads the status of the last pass: bit flags of device-side errors. */
+int dsmc_device_status(dsmc_ctx *ctx, uint32_t *error_bits, uint32_t *spill);
+
+/* The CUDA stream (cudaStream_t) the context enqueues its work on, for
+ * callers that order or time their own work against it. */
+void *dsmc_stream(dsmc_ctx *ctx);
+
+/* Raw running counters of one system, without synchronising the device
+ * beyond the copy: collisions, wall collisions, reseeds, particle steps,
+ * count_periodic[3], samples (8 values, as int64). */
+int dsmc_counters_get(dsmc_ctx *ctx, int sys_id, int64_t out[8]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DSMC_B200_H */

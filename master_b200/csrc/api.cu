@@ -1,0 +1,961 @@
+// C ABI of libdsmc_b200: context, systems, particle I/O and the timestep
+// pipeline.  Host code only; the kernels are in kernels_split.cu and
+// kernels_fp64.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "dsmc_b200.h"
+#include "dsmc_internal.h"
+#include "dsmc_layout.h"
+#include "kernels.h"
+
+namespace dsmc {
+
+template <class T> struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t count) {
+        release();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        else p = nullptr;
+        return e;
+    }
+    cudaError_t ensure(size_t count) { return count <= n && p ? cudaSuccess : alloc(count); }
+};
+
+struct SysHost {
+    dsmc_settings settings;
+    int n[3], cells[3];
+    float porosity_global, porosity;
+    double volume, atoms_per_molecule;
+    int64_t expected;
+    int64_t num_particles = 0;
+    uint32_t id_count = 0;  // ids handed out: 0 .. id_count-1
+    int active_begin = 0, active_end = 0;
+    std::vector<int> cell_global;     // per active cell
+    std::vector<int> pixels, total_pixels;
+    std::vector<double> volume_cell, coeff;
+    std::vector<int> cell_map;        // global -> local active index
+    DevBuf<uint8_t> vox;
+    DevBuf<float> nrm, t1, t2;
+    DevBuf<int> cell_map_dev;         // global -> absolute active index
+    SysDev dev;
+    double t0_reduced = 0;            // time of the last tally reset
+    double sqrt_t_over_m = 0;
+    double vr_max0 = 0;
+};
+
+}  // namespace dsmc
+
+using namespace dsmc;
+
+struct dsmc_ctx {
+    int device = 0;
+    int precision = DSMC_PREC_SPLIT32;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    std::string error;
+    Units units;
+    std::vector<std::unique_ptr<SysHost>> systems;
+
+    // device tables
+    DevBuf<SysDev> sys_dev;
+    DevBuf<SysTally> tally;
+    DevBuf<Status> status;
+    // cells (all systems)
+    int num_cells = 0;
+    DevBuf<int> cell_sys, cell_global;
+    DevBuf<unsigned> cell_base, cell_cap, count0, count1, key;
+    DevBuf<double> vr_max, rest, coeff, mom;
+    std::vector<unsigned> h_base, h_cap;
+    size_t slots = 0;
+    int smem_cap = 32;
+    // particles
+    DevBuf<unsigned char> A0, A1, B0, B1;
+    DevBuf<SpillRec> spill;
+    unsigned spill_cap = 1u << 16;
+    int cur = 0;
+    bool pending = false;     // the last step's collide/sample has not run yet
+    bool keys_valid = false;  // a stand-alone move stage left new cell keys
+    // staging
+    DevBuf<unsigned char> fA, fB;
+    DevBuf<int> fkey;
+    DevBuf<unsigned> hist;
+    DevBuf<unsigned long long> cursor;
+    DevBuf<double> io_r, io_v;
+    DevBuf<int> io_cell;
+    // launch shape of the cell pass
+    int block = 256;
+    int grid = 0;
+
+    size_t rec_half() const { return precision == DSMC_PREC_FP64 ? 32 : 16; }
+};
+
+namespace {
+
+int fail(dsmc_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->error = msg;
+    else set_thread_error(msg);
+    return code;
+}
+
+int cuda_fail(dsmc_ctx *ctx, cudaError_t e, const char *what) {
+    return fail(ctx, DSMC_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                  \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);  \
+    } while (0)
+
+bool is_fp64(const dsmc_ctx *ctx) { return ctx->precision == DSMC_PREC_FP64; }
+
+CellArrays cell_arrays(dsmc_ctx *ctx) {
+    CellArrays c;
+    c.num_cells = ctx->num_cells;
+    c.sys = ctx->cell_sys.p;
+    c.global = ctx->cell_global.p;
+    c.base = ctx->cell_base.p;
+    c.cap = ctx->cell_cap.p;
+    c.count[0] = ctx->count0.p;
+    c.count[1] = ctx->count1.p;
+    c.vr_max = ctx->vr_max.p;
+    c.rest = ctx->rest.p;
+    c.coeff = ctx->coeff.p;
+    c.mom = ctx->mom.p;
+    c.key = ctx->key.p;
+    return c;
+}
+
+ParticleArrays particle_arrays(dsmc_ctx *ctx) {
+    ParticleArrays p;
+    p.A[0] = ctx->A0.p;
+    p.A[1] = ctx->A1.p;
+    p.B[0] = ctx->B0.p;
+    p.B[1] = ctx->B1.p;
+    p.spill = ctx->spill.p;
+    p.spill_cap = ctx->spill_cap;
+    return p;
+}
+
+int upload_sys_table(dsmc_ctx *ctx) {
+    std::vector<SysDev> t;
+    for (auto &s : ctx->systems) t.push_back(s->dev);
+    CK(ctx->sys_dev.ensure(std::max<size_t>(t.size(), 1)));
+    if (!t.empty())
+        CK(cudaMemcpyAsync(ctx->sys_dev.p, t.data(), t.size() * sizeof(SysDev), cudaMemcpyHostToDevice, ctx->stream));
+    return DSMC_OK;
+}
+
+Status read_status(dsmc_ctx *ctx, cudaError_t *err) {
+    Status st;
+    std::memset(&st, 0, sizeof(st));
+    *err = cudaMemcpyAsync(&st, ctx->status.p, sizeof(Status), cudaMemcpyDeviceToHost, ctx->stream);
+    if (*err == cudaSuccess) *err = cudaStreamSynchronize(ctx->stream);
+    return st;
+}
+
+// Rebuilds every cell table and slot buffer from flat staged particles.
+// fA/fB/fkey hold `total` records; hist holds per-cell counts.
+int relayout(dsmc_ctx *ctx, long long total) {
+    const int C = ctx->num_cells;
+    std::vector<unsigned> counts(C);
+    if (C) CK(cudaMemcpyAsync(counts.data(), ctx->hist.p, C * sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    // Capacity per cell: twice the larger of the expected and the present
+    // occupancy plus 24 slots, a multiple of 4 (Poisson tails beyond it are
+    // below 1e-12 per cell and step; an overflow spills and the host repacks).
+    ctx->h_base.assign(C, 0);
+    ctx->h_cap.assign(C, 0);
+    size_t slots = 0;
+    unsigned maxcap = 4;
+    for (auto &sp : ctx->systems) {
+        SysHost &s = *sp;
+        double total_pixels = 0;
+        for (int p : s.pixels) total_pixels += p;
+        const double nsys = (double)s.num_particles;
+        for (int a = s.active_begin; a < s.active_end; ++a) {
+            const double expect = total_pixels > 0 ? nsys * s.pixels[a - s.active_begin] / total_pixels : 0;
+            const double want = std::max(expect, (double)counts[a]);
+            unsigned cap = (unsigned)std::ceil(2.0 * want + 24.0);
+            cap = (cap + 3u) & ~3u;
+            ctx->h_base[a] = (unsigned)slots;
+            ctx->h_cap[a] = cap;
+            slots += cap;
+            maxcap = std::max(maxcap, cap);
+        }
+    }
+    if (slots >= (size_t)0xffffffffu) return fail(ctx, DSMC_ERR_CAPACITY, "more than 2^32 particle slots");
+    if (maxcap > 4096) return fail(ctx, DSMC_ERR_CAPACITY, "a cell needs more than 4096 slots");
+    ctx->smem_cap = (int)((maxcap + 31u) & ~31u);
+    ctx->slots = slots;
+    const size_t half = ctx->rec_half();
+    CK(ctx->A0.ensure(slots * half));
+    CK(ctx->A1.ensure(slots * half));
+    CK(ctx->B0.ensure(slots * half));
+    CK(ctx->B1.ensure(slots * half));
+    CK(ctx->key.ensure(slots));
+    CK(ctx->cell_base.ensure(C));
+    CK(ctx->cell_cap.ensure(C));
+    if (C) {
+        CK(cudaMemcpyAsync(ctx->cell_base.p, ctx->h_base.data(), C * sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->cell_cap.p, ctx->h_cap.data(), C * sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemsetAsync(ctx->count0.p, 0, C * sizeof(unsigned), ctx->stream));
+        CK(cudaMemsetAsync(ctx->count1.p, 0, C * sizeof(unsigned), ctx->stream));
+    }
+    ctx->cur = 0;
+    CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(unsigned) * 2, ctx->stream));  // error, spill
+    unsigned zero = 0;
+    CK(cudaMemcpyAsync(&ctx->status.p->halted, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+    if (total > 0) {
+        cudaError_t e = is_fp64(ctx)
+                            ? fp64::launch_insert(cell_arrays(ctx), particle_arrays(ctx), 0, total, ctx->fA.p,
+                                                  ctx->fB.p, ctx->fkey.p, &ctx->status.p->error, ctx->stream)
+                            : split32::launch_insert(cell_arrays(ctx), particle_arrays(ctx), 0, total, ctx->fA.p,
+                                                     ctx->fB.p, ctx->fkey.p, &ctx->status.p->error, ctx->stream);
+        CK(e);
+    }
+    // Launch shape of the cell pass: a persistent grid at full occupancy.
+    const int bps = is_fp64(ctx) ? fp64::pass_blocks_per_sm(PASS_FUSED, ctx->block, ctx->smem_cap)
+                                 : split32::pass_blocks_per_sm(PASS_FUSED, ctx->block, ctx->smem_cap);
+    if (bps <= 0) return fail(ctx, DSMC_ERR_CUDA, "cell pass cannot be resident (shared memory)");
+    is_fp64(ctx) ? fp64::pass_blocks_per_sm(PASS_INPLACE, ctx->block, ctx->smem_cap)
+                 : split32::pass_blocks_per_sm(PASS_INPLACE, ctx->block, ctx->smem_cap);
+    is_fp64(ctx) ? fp64::pass_blocks_per_sm(PASS_SORT, ctx->block, ctx->smem_cap)
+                 : split32::pass_blocks_per_sm(PASS_SORT, ctx->block, ctx->smem_cap);
+    ctx->grid = bps * ctx->num_sms;
+    Status st;
+    cudaError_t e;
+    st = read_status(ctx, &e);
+    CK(e);
+    if (st.error & DSMC_EBIT_FATAL) return fail(ctx, DSMC_ERR_STATE, "particles could not be placed in cells");
+    return DSMC_OK;
+}
+
+// Stages every present particle (all systems, or all but `skip`) into fA/fB.
+int stage_present(dsmc_ctx *ctx, long long extra, int skip, long long *staged) {
+    long long present = 0;
+    for (size_t s = 0; s < ctx->systems.size(); ++s)
+        if ((int)s != skip) present += ctx->systems[s]->num_particles;
+    Status st;
+    cudaError_t e;
+    st = read_status(ctx, &e);
+    CK(e);
+    const long long total = present + st.spill + extra;
+    const size_t half = ctx->rec_half();
+    CK(ctx->fA.ensure(std::max<long long>(total, 1) * half));
+    CK(ctx->fB.ensure(std::max<long long>(total, 1) * half));
+    CK(ctx->fkey.ensure(std::max<long long>(total, 1)));
+    CK(ctx->hist.ensure(std::max(ctx->num_cells, 1)));
+    CK(ctx->cursor.ensure(1));
+    CK(cudaMemsetAsync(ctx->hist.p, 0, std::max(ctx->num_cells, 1) * sizeof(unsigned), ctx->stream));
+    CK(cudaMemsetAsync(ctx->cursor.p, 0, sizeof(unsigned long long), ctx->stream));
+    *staged = 0;
+    if (ctx->A0.p && ctx->num_cells) {
+        for (size_t s = 0; s < ctx->systems.size(); ++s) {
+            if ((int)s == skip) continue;
+            SysHost &h = *ctx->systems[s];
+            if (h.active_end <= h.active_begin) continue;
+            e = is_fp64(ctx) ? fp64::launch_gather(cell_arrays(ctx), particle_arrays(ctx), ctx->cur, h.active_begin,
+                                                   h.active_end, std::min(st.spill, ctx->spill_cap), ctx->fA.p,
+                                                   ctx->fB.p, ctx->fkey.p, ctx->hist.p, ctx->cursor.p,
+                                                   (unsigned long long)total, &ctx->status.p->error, ctx->stream)
+                             : split32::launch_gather(cell_arrays(ctx), particle_arrays(ctx), ctx->cur,
+                                                      h.active_begin, h.active_end, std::min(st.spill, ctx->spill_cap),
+                                                      ctx->fA.p, ctx->fB.p, ctx->fkey.p, ctx->hist.p, ctx->cursor.p,
+                                                      (unsigned long long)total, &ctx->status.p->error, ctx->stream);
+            CK(e);
+        }
+        unsigned long long got = 0;
+        CK(cudaMemcpyAsync(&got, ctx->cursor.p, sizeof(got), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        *staged = (long long)got;
+    }
+    return DSMC_OK;
+}
+
+// Runs the collide + sample of the last step if it is still pending.
+int flush_pending(dsmc_ctx *ctx);
+
+int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, int advance) {
+    PassParams P;
+    P.sys = ctx->sys_dev.p;
+    P.tally = ctx->tally.p;
+    P.status = ctx->status.p;
+    P.cells = cell_arrays(ctx);
+    P.parts = particle_arrays(ctx);
+    P.cur = ctx->cur;
+    P.do_collide = do_collide;
+    P.do_move = do_move;
+    P.do_sample = do_sample;
+    P.smem_cap = ctx->smem_cap;
+    P.advance_step = advance;
+    cudaError_t e = is_fp64(ctx) ? fp64::launch_pass(mode, P, ctx->grid, ctx->block, ctx->stream)
+                                 : split32::launch_pass(mode, P, ctx->grid, ctx->block, ctx->stream);
+    CK(e);
+    return DSMC_OK;
+}
+
+// After a batch of passes: find how many ran, fix the buffer parity, and
+// repack if one of them spilled.
+int settle(dsmc_ctx *ctx, unsigned step_before, int cur_before, int *ran) {
+    cudaError_t e;
+    Status st = read_status(ctx, &e);
+    CK(e);
+    *ran = (int)(st.step - step_before);
+    ctx->cur = cur_before ^ (*ran & 1);
+    if (st.error & DSMC_EBIT_FATAL) {
+        char buf[160];
+        std::snprintf(buf, sizeof(buf), "device error bits 0x%x after step %u (1 cell, 4 reseed, 8 spill list, 16 "
+                      "staging, 32 non-finite)", st.error, st.step);
+        return fail(ctx, DSMC_ERR_STATE, buf);
+    }
+    if (st.halted && st.spill) {
+        long long staged = 0;
+        int rc = stage_present(ctx, 0, -1, &staged);
+        if (rc) return rc;
+        return relayout(ctx, staged);
+    }
+    return DSMC_OK;
+}
+
+int flush_pending(dsmc_ctx *ctx) {
+    if (!ctx->pending) return DSMC_OK;
+    int rc = launch(ctx, PASS_INPLACE, 1, 0, 1, 0);
+    if (rc) return rc;
+    ctx->pending = false;
+    return DSMC_OK;
+}
+
+int rebuild_cells(dsmc_ctx *ctx) {
+    // Keep the cell state and tallies of the systems already present: a new
+    // system's cells are appended after theirs.
+    const int C_old = ctx->num_cells;
+    std::vector<double> old_vr(C_old), old_rest(C_old), old_mom(8 * (size_t)C_old);
+    std::vector<SysTally> old_tally(ctx->systems.size() > 0 ? ctx->systems.size() - 1 : 0);
+    if (C_old > 0) {
+        CK(cudaMemcpyAsync(old_vr.data(), ctx->vr_max.p, C_old * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(old_rest.data(), ctx->rest.p, C_old * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(old_mom.data(), ctx->mom.p, 8 * C_old * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (!old_tally.empty())
+        CK(cudaMemcpyAsync(old_tally.data(), ctx->tally.p, old_tally.size() * sizeof(SysTally), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    // Concatenate the active cells of all systems.
+    int C = 0;
+    for (auto &s : ctx->systems) C += (int)s->cell_global.size();
+    std::vector<int> sys(C), glob(C);
+    std::vector<double> vr(C), rest(C, 0.0), coeff(C);
+    int a = 0;
+    for (size_t si = 0; si < ctx->systems.size(); ++si) {
+        SysHost &s = *ctx->systems[si];
+        s.active_begin = a;
+        for (size_t c = 0; c < s.cell_global.size(); ++c, ++a) {
+            sys[a] = (int)si;
+            glob[a] = s.cell_global[c];
+            vr[a] = s.vr_max0;
+            coeff[a] = s.coeff[c];
+        }
+        s.active_end = a;
+        s.dev.active_begin = s.active_begin;
+        s.dev.active_end = s.active_end;
+        std::vector<int> map_abs(s.cell_map.size());
+        for (size_t g = 0; g < s.cell_map.size(); ++g) map_abs[g] = s.cell_map[g] < 0 ? -1 : s.cell_map[g] + s.active_begin;
+        CK(s.cell_map_dev.ensure(map_abs.size()));
+        CK(cudaMemcpyAsync(s.cell_map_dev.p, map_abs.data(), map_abs.size() * sizeof(int), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        s.dev.cell_map = s.cell_map_dev.p;
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    ctx->num_cells = C;
+    const size_t Cn = std::max(C, 1);
+    CK(ctx->cell_sys.alloc(Cn));
+    CK(ctx->cell_global.alloc(Cn));
+    CK(ctx->count0.alloc(Cn));
+    CK(ctx->count1.alloc(Cn));
+    CK(ctx->vr_max.alloc(Cn));
+    CK(ctx->rest.alloc(Cn));
+    CK(ctx->coeff.alloc(Cn));
+    CK(ctx->mom.alloc(8 * Cn));
+    CK(ctx->hist.alloc(Cn));
+    if (C) {
+        CK(cudaMemcpyAsync(ctx->cell_sys.p, sys.data(), C * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->cell_global.p, glob.data(), C * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->vr_max.p, vr.data(), C * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->rest.p, rest.data(), C * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->coeff.p, coeff.data(), C * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemsetAsync(ctx->mom.p, 0, 8 * C * sizeof(double), ctx->stream));
+        CK(cudaMemsetAsync(ctx->count0.p, 0, C * sizeof(unsigned), ctx->stream));
+        CK(cudaMemsetAsync(ctx->count1.p, 0, C * sizeof(unsigned), ctx->stream));
+        if (C_old > 0 && C_old <= C) {
+            CK(cudaMemcpyAsync(ctx->vr_max.p, old_vr.data(), C_old * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaMemcpyAsync(ctx->rest.p, old_rest.data(), C_old * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaMemcpyAsync(ctx->mom.p, old_mom.data(), 8 * C_old * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        }
+    }
+    CK(ctx->tally.alloc(std::max<size_t>(ctx->systems.size(), 1)));
+    CK(cudaMemsetAsync(ctx->tally.p, 0, std::max<size_t>(ctx->systems.size(), 1) * sizeof(SysTally), ctx->stream));
+    if (!old_tally.empty())
+        CK(cudaMemcpyAsync(ctx->tally.p, old_tally.data(), old_tally.size() * sizeof(SysTally), cudaMemcpyHostToDevice,
+                           ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return upload_sys_table(ctx);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *dsmc_last_error(const dsmc_ctx *ctx) { return ctx ? ctx->error.c_str() : thread_error(); }
+
+int dsmc_ctx_create(int device_id, int precision, dsmc_ctx **out) {
+    if (!out || (precision != DSMC_PREC_SPLIT32 && precision != DSMC_PREC_FP64)) return DSMC_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return fail(nullptr, DSMC_ERR_NO_DEVICE, "no CUDA device");
+    if (device_id < 0 || device_id >= ndev) return fail(nullptr, DSMC_ERR_ARG, "device id out of range");
+    e = cudaSetDevice(device_id);
+    if (e != cudaSuccess) return fail(nullptr, DSMC_ERR_CUDA, cudaGetErrorString(e));
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, device_id);
+    if (prop.major != 10) return fail(nullptr, DSMC_ERR_NO_DEVICE, "kernels are built for sm_100a (B200) only");
+    std::unique_ptr<dsmc_ctx> ctx(new dsmc_ctx);
+    ctx->device = device_id;
+    ctx->precision = precision;
+    ctx->num_sms = prop.multiProcessorCount;
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(nullptr, DSMC_ERR_CUDA, cudaGetErrorString(e));
+    if (ctx->status.alloc(1) != cudaSuccess) return fail(nullptr, DSMC_ERR_CUDA, "status alloc");
+    cudaMemset(ctx->status.p, 0, sizeof(Status));
+    if (ctx->spill.alloc(ctx->spill_cap) != cudaSuccess) return fail(nullptr, DSMC_ERR_CUDA, "spill alloc");
+    if (ctx->tally.alloc(1) != cudaSuccess) return fail(nullptr, DSMC_ERR_CUDA, "tally alloc");
+    cudaMemset(ctx->tally.p, 0, sizeof(SysTally));
+    *out = ctx.release();
+    return DSMC_OK;
+}
+
+void dsmc_ctx_destroy(dsmc_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStream_t s = ctx->stream;
+    delete ctx;
+    cudaStreamDestroy(s);
+}
+
+int dsmc_sync(dsmc_ctx *ctx) {
+    if (!ctx) return DSMC_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DSMC_OK;
+}
+
+int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t ny, uint32_t nz,
+                    const uint8_t *voxels, const float *normals, const float *tangents1, const float *tangents2,
+                    float porosity_global, int *sys_id) {
+    if (!ctx || !s || !voxels || !normals || !tangents1 || !tangents2 || !sys_id) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    if (nx == 0 || ny == 0 || nz == 0 || nx > 2048 || ny > 2048 || nz > 1024)
+        return fail(ctx, DSMC_ERR_CAPACITY, "voxel grid limited to 2048 x 2048 x 1024");
+    if (s->cells_x <= 0 || s->cells_y <= 0 || s->cells_z <= 0) return fail(ctx, DSMC_ERR_CONFIG, "cells must be > 0");
+    if (s->nx != 1 || s->ny != 1 || s->nz != 1)
+        return fail(ctx, DSMC_ERR_CONFIG, "one system is one domain: processor grid must be 1 1 1");
+    if (s->surface_model != 0) return fail(ctx, DSMC_ERR_CONFIG, "only thermal walls are built");
+    // System::validate_number_of_cells (dsmc/system.cpp:221-239).
+    if (nx % s->cells_x || ny % s->cells_y || nz % s->cells_z)
+        return fail(ctx, DSMC_ERR_CONFIG, "Error: voxel-cell-cpu configuration not good.");
+    // Settle pending work and stage the particles already present.
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    long long staged = 0;
+    rc = stage_present(ctx, 0, -1, &staged);
+    if (rc) return rc;
+
+    std::unique_ptr<SysHost> h(new SysHost);
+    h->settings = *s;
+    h->n[0] = nx;
+    h->n[1] = ny;
+    h->n[2] = nz;
+    h->cells[0] = s->cells_x;
+    h->cells[1] = s->cells_y;
+    h->cells[2] = s->cells_z;
+    const uint64_t V = (uint64_t)nx * ny * nz;
+    uint64_t empty = 0;
+    for (uint64_t i = 0; i < V; ++i) empty += voxels[i] == DSMC_VOX_EMPTY;
+    h->porosity = (float)empty / (float)V;
+    h->porosity_global = porosity_global > 0 ? porosity_global : (float)((double)empty / V);
+    const Units &u = ctx->units;
+    const double L[3] = {s->Lx, s->Ly, s->Lz};
+    // System::initialize (dsmc/system.cpp:241-382).
+    const double temperature = u.temperature_from_SI(s->temperature);
+    const double wall_temperature = u.temperature_from_SI(s->wall_temperature);
+    const double density = u.number_density_from_SI(s->density);
+    h->atoms_per_molecule = s->atoms_per_molecule;
+    h->vr_max0 = 3 * std::sqrt(temperature);
+    h->sqrt_t_over_m = std::sqrt(temperature / s->mass);
+    double volume = L[0] * L[1] * L[2];
+    volume = volume / 1 * h->porosity;
+    h->volume = volume;
+    h->expected = (int64_t)(density * volume / h->atoms_per_molecule);
+    // System::setup_cells (dsmc/system.cpp:432-490): cells numbered in order
+    // of first touch by a k-outer, i-inner voxel sweep; cells with no empty
+    // voxel are dropped.
+    const int cx = s->cells_x, cy = s->cells_y, cz = s->cells_z;
+    const int ncells = cx * cy * cz;
+    std::vector<int> first(ncells, -1), tot, pix, order;
+    for (uint32_t k = 0; k < nz; ++k) {
+        const int c_z = (int)((float)k / nz * cz);
+        for (uint32_t j = 0; j < ny; ++j) {
+            const int c_y = (int)((float)j / ny * cy);
+            for (uint32_t i = 0; i < nx; ++i) {
+                const int c_x = (int)((float)i / nx * cx);
+                const int ci = c_x * cy * cz + c_y * cz + c_z;
+                if (first[ci] < 0) {
+                    first[ci] = (int)order.size();
+                    order.push_back(ci);
+                    tot.push_back(0);
+                    pix.push_back(0);
+                }
+                tot[first[ci]]++;
+                pix[first[ci]] += voxels[((uint64_t)i * ny + j) * nz + k] < DSMC_VOX_WALL;
+            }
+        }
+    }
+    h->cell_map.assign(ncells, -1);
+    const double system_volume = L[0] * L[1] * L[2];
+    for (size_t c = 0; c < order.size(); ++c) {
+        if (pix[c] == 0) continue;
+        // Cell::update_volume (dsmc/cell.cpp:27-40)
+        const double vol = system_volume / (ncells) * (float)pix[c] / tot[c];
+        const double coeff = 0.5 * h->atoms_per_molecule * M_PI * s->diam * s->diam * s->dt / vol;
+        h->cell_map[order[c]] = (int)h->cell_global.size();
+        h->cell_global.push_back(order[c]);
+        h->pixels.push_back(pix[c]);
+        h->total_pixels.push_back(tot[c]);
+        h->volume_cell.push_back(vol);
+        h->coeff.push_back(coeff);
+    }
+    // Device geometry.
+    CK(h->vox.alloc(V));
+    CK(h->nrm.alloc(3 * V));
+    CK(h->t1.alloc(3 * V));
+    CK(h->t2.alloc(3 * V));
+    CK(cudaMemcpyAsync(h->vox.p, voxels, V, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(h->nrm.p, normals, 3 * V * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(h->t1.p, tangents1, 3 * V * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(h->t2.p, tangents2, 3 * V * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+    SysDev &d = h->dev;
+    std::memset(&d, 0, sizeof(d));
+    for (int a = 0; a < 3; ++a) {
+        d.n[a] = h->n[a];
+        d.cells[a] = h->cells[a];
+        d.vpc[a] = h->n[a] / h->cells[a];
+        d.inv_vpc[a] = 1.0f / d.vpc[a];
+        d.L[a] = L[a];
+        d.invL[a] = 1.0 / L[a];
+        d.vox_len[a] = L[a] / h->n[a];
+        // Grid constants (dsmc/grid.cpp:41-46): float-rounded, one rank.
+        d.ref_scale[a] = (double)(float)(d.invL[a] * h->n[a]);
+        d.ref_shift[a] = (double)(float)(-0.0 * d.invL[a] * h->n[a] + (double)h->n[a]);
+        d.inv_vox_f[a] = (float)(h->n[a] / L[a]);
+        d.L_f[a] = (float)L[a];
+    }
+    d.vox = h->vox.p;
+    d.nrm = h->nrm.p;
+    d.t1 = h->t1.p;
+    d.t2 = h->t2.p;
+    d.dt = s->dt;
+    d.dt_f = (float)s->dt;
+    d.flow_dir = (s->flow_direction < 0 || s->flow_direction > 2 || s->gravity == 0) ? -1 : s->flow_direction;
+    d.accel_dt = s->gravity * s->dt;
+    d.accel_dt_f = (float)d.accel_dt;
+    d.wall_s = std::sqrt(wall_temperature / s->mass);
+    d.wall_s_f = (float)d.wall_s;
+    d.seed = s->rng_seed;
+    d.sample_interval = s->statistics_interval;
+    d.sample_begin = s->sample_begin;
+
+    ctx->systems.push_back(std::move(h));
+    *sys_id = (int)ctx->systems.size() - 1;
+    // The staged keys index the old cell numbering; rebuild with the new
+    // system appended at the end, so earlier systems keep their cell ids.
+    rc = rebuild_cells(ctx);
+    if (rc) return rc;
+    CK(ctx->hist.ensure(std::max(ctx->num_cells, 1)));
+    CK(cudaMemsetAsync(ctx->hist.p, 0, std::max(ctx->num_cells, 1) * sizeof(unsigned), ctx->stream));
+    if (staged > 0) {
+        // recount the staged keys into the new histogram
+        std::vector<int> keys(staged);
+        CK(cudaMemcpyAsync(keys.data(), ctx->fkey.p, staged * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        std::vector<unsigned> hc(ctx->num_cells, 0);
+        for (int k : keys)
+            if (k >= 0) hc[k]++;
+        CK(cudaMemcpyAsync(ctx->hist.p, hc.data(), hc.size() * sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    return relayout(ctx, staged);
+}
+
+int dsmc_system_add_world(dsmc_ctx *ctx, const dsmc_settings *s, int *sys_id) {
+    if (!ctx || !s) return DSMC_ERR_ARG;
+    char path[600];
+    std::snprintf(path, sizeof(path), "%s/%04d.bin", s->world, 0);
+    dsmc_world_header hd;
+    int rc = dsmc_world_read_header(path, &hd);
+    if (rc) return fail(ctx, rc, thread_error());
+    const uint64_t V = (uint64_t)hd.global_nx * hd.global_ny * hd.global_nz;
+    std::vector<uint8_t> vox(V);
+    std::vector<float> n(3 * V), a(3 * V), b(3 * V);
+    rc = dsmc_world_read(path, vox.data(), n.data(), a.data(), b.data());
+    if (rc) return fail(ctx, rc, thread_error());
+    return dsmc_system_add(ctx, s, hd.global_nx, hd.global_ny, hd.global_nz, vox.data(), n.data(), a.data(), b.data(),
+                           hd.porosity_global, sys_id);
+}
+
+int dsmc_system_info_get(dsmc_ctx *ctx, int sys_id, dsmc_system_info *info) {
+    if (!ctx || !info || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+    SysHost &h = *ctx->systems[sys_id];
+    info->num_particles = h.num_particles;
+    info->num_cells_total = h.cells[0] * h.cells[1] * h.cells[2];
+    info->num_active_cells = (int)h.cell_global.size();
+    info->volume = h.volume;
+    info->porosity = h.porosity;
+    info->atoms_per_molecule = h.atoms_per_molecule;
+    info->dt = h.settings.dt;
+    info->expected_particles = h.expected;
+    info->slots = (int)ctx->slots;
+    return DSMC_OK;
+}
+
+static int place_particles(dsmc_ctx *ctx, int sys_id, long long n, const double *r, const double *v) {
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    long long staged = 0;
+    rc = stage_present(ctx, n, sys_id, &staged);
+    if (rc) return rc;
+    SysHost &h = *ctx->systems[sys_id];
+    const size_t half = ctx->rec_half();
+    unsigned char *A = ctx->fA.p + staged * half;
+    unsigned char *B = ctx->fB.p + staged * half;
+    int *key = ctx->fkey.p + staged;
+    cudaError_t e;
+    if (r) {
+        CK(ctx->io_r.ensure(3 * std::max<long long>(n, 1)));
+        CK(ctx->io_v.ensure(3 * std::max<long long>(n, 1)));
+        if (n) {
+            CK(cudaMemcpyAsync(ctx->io_r.p, r, 3 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+            CK(cudaMemcpyAsync(ctx->io_v.p, v, 3 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+            e = is_fp64(ctx) ? fp64::launch_from_fp64(ctx->sys_dev.p, sys_id, ctx->io_r.p, ctx->io_v.p, 0, n, A, B, key,
+                                                      ctx->hist.p, &ctx->status.p->error, ctx->stream)
+                             : split32::launch_from_fp64(ctx->sys_dev.p, sys_id, ctx->io_r.p, ctx->io_v.p, 0, n, A, B,
+                                                         key, ctx->hist.p, &ctx->status.p->error, ctx->stream);
+            CK(e);
+        }
+    } else if (n) {
+        e = is_fp64(ctx) ? fp64::launch_init(ctx->sys_dev.p, sys_id, h.sqrt_t_over_m, n, A, B, key, ctx->hist.p,
+                                             &ctx->status.p->error, ctx->stream)
+                         : split32::launch_init(ctx->sys_dev.p, sys_id, h.sqrt_t_over_m, n, A, B, key, ctx->hist.p,
+                                                &ctx->status.p->error, ctx->stream);
+        CK(e);
+    }
+    Status st = read_status(ctx, &e);
+    CK(e);
+    if (st.error & DSMC_EBIT_FATAL) {
+        cudaMemsetAsync(ctx->status.p, 0, sizeof(unsigned), ctx->stream);
+        return fail(ctx, DSMC_ERR_STATE, "a particle lies in a solid voxel or a cell with no free volume");
+    }
+    h.num_particles = n;
+    h.id_count = (uint32_t)n;
+    return relayout(ctx, staged + n);
+}
+
+int dsmc_particles_set(dsmc_ctx *ctx, int sys_id, int64_t n, const double *r, const double *v) {
+    if (!ctx || sys_id < 0 || sys_id >= (int)ctx->systems.size() || n < 0 || (n && (!r || !v))) return DSMC_ERR_ARG;
+    if (n > 0xffffffffLL) return fail(ctx, DSMC_ERR_CAPACITY, "at most 2^32 particles per system");
+    return place_particles(ctx, sys_id, n, r, v);
+}
+
+int dsmc_particles_init(dsmc_ctx *ctx, int sys_id, int64_t n) {
+    if (!ctx || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+    SysHost &h = *ctx->systems[sys_id];
+    if (n < 0) n = h.expected;
+    if (n > h.settings.max_molecules_per_node && h.settings.max_molecules_per_node > 0) {
+        char buf[200];
+        std::snprintf(buf, sizeof(buf), "Node 0 wants to create %lld molecules (MAX_MOLECULE_NUM=%d)", (long long)n,
+                      h.settings.max_molecules_per_node);
+        return fail(ctx, DSMC_ERR_CAPACITY, buf);
+    }
+    return place_particles(ctx, sys_id, n, nullptr, nullptr);
+}
+
+int dsmc_particles_count(dsmc_ctx *ctx, int sys_id, int64_t *n) {
+    if (!ctx || !n || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+    *n = ctx->systems[sys_id]->num_particles;
+    return DSMC_OK;
+}
+
+int dsmc_particles_get(dsmc_ctx *ctx, int sys_id, int64_t cap, double *r, double *v, int32_t *cell, int64_t *n) {
+    if (!ctx || !r || !v || !n || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    SysHost &h = *ctx->systems[sys_id];
+    *n = h.num_particles;
+    if (cap < h.num_particles) return fail(ctx, DSMC_ERR_CAPACITY, "output buffers smaller than the particle count");
+    const long long N = h.num_particles;
+    CK(ctx->io_r.ensure(3 * std::max<long long>(N, 1)));
+    CK(ctx->io_v.ensure(3 * std::max<long long>(N, 1)));
+    CK(ctx->io_cell.ensure(std::max<long long>(N, 1)));
+    if (N == 0) return DSMC_OK;
+    cudaError_t e = is_fp64(ctx)
+                        ? fp64::launch_to_fp64(ctx->sys_dev.p, sys_id, cell_arrays(ctx), particle_arrays(ctx), ctx->cur,
+                                               0, N, ctx->io_r.p, ctx->io_v.p, ctx->io_cell.p, &ctx->status.p->error,
+                                               ctx->stream)
+                        : split32::launch_to_fp64(ctx->sys_dev.p, sys_id, cell_arrays(ctx), particle_arrays(ctx),
+                                                  ctx->cur, 0, N, ctx->io_r.p, ctx->io_v.p, ctx->io_cell.p,
+                                                  &ctx->status.p->error, ctx->stream);
+    CK(e);
+    CK(cudaMemcpyAsync(r, ctx->io_r.p, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(v, ctx->io_v.p, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (cell) CK(cudaMemcpyAsync(cell, ctx->io_cell.p, N * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DSMC_OK;
+}
+
+int dsmc_step(dsmc_ctx *ctx, int nsteps) {
+    if (!ctx || nsteps < 0) return DSMC_ERR_ARG;
+    if (ctx->systems.empty() || nsteps == 0) return DSMC_OK;
+    cudaSetDevice(ctx->device);
+    ctx->keys_valid = false;
+    int left = nsteps;
+    while (left > 0) {
+        cudaError_t e;
+        Status st = read_status(ctx, &e);
+        CK(e);
+        const unsigned step0 = st.step;
+        const int cur0 = ctx->cur;
+        const bool pending0 = ctx->pending;
+        // One fused pass per step: collide + sample of the previous step's
+        // cells, then accelerate + move + re-bin of this step.
+        for (int i = 0; i < left; ++i) {
+            const int prologue = (i == 0 && !pending0);
+            int rc = launch(ctx, PASS_FUSED, !prologue, 1, !prologue, 1);
+            if (rc) return rc;
+            ctx->cur ^= 1;
+        }
+        int ran = 0;
+        int rc = settle(ctx, step0, cur0, &ran);
+        if (rc) return rc;
+        if (ran <= 0) return fail(ctx, DSMC_ERR_STATE, "timestep pipeline made no progress");
+        ctx->pending = true;
+        left -= ran;
+    }
+    return DSMC_OK;
+}
+
+int dsmc_stage_move(dsmc_ctx *ctx) {
+    if (!ctx) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    rc = launch(ctx, PASS_INPLACE, 0, 1, 0, 1);
+    if (rc) return rc;
+    ctx->keys_valid = true;
+    return DSMC_OK;
+}
+
+int dsmc_stage_sort(dsmc_ctx *ctx) {
+    if (!ctx) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    if (!ctx->keys_valid) return DSMC_OK;  // nothing moved since the last re-bin
+    ctx->keys_valid = false;
+    cudaError_t e;
+    rc = launch(ctx, PASS_SORT, 0, 0, 0, 0);
+    if (rc) return rc;
+    ctx->cur ^= 1;
+    Status st2 = read_status(ctx, &e);
+    CK(e);
+    if (st2.error & DSMC_EBIT_FATAL) return fail(ctx, DSMC_ERR_STATE, "sort failed");
+    if (st2.spill) {
+        long long staged = 0;
+        rc = stage_present(ctx, 0, -1, &staged);
+        if (rc) return rc;
+        return relayout(ctx, staged);
+    }
+    return DSMC_OK;
+}
+
+int dsmc_stage_collide(dsmc_ctx *ctx) {
+    if (!ctx) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    return launch(ctx, PASS_INPLACE, 1, 0, 0, 0);
+}
+
+int dsmc_stage_sample(dsmc_ctx *ctx) {
+    if (!ctx) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    return launch(ctx, PASS_INPLACE, 0, 0, 1, 0);
+}
+
+int dsmc_tallies_get(dsmc_ctx *ctx, int sys_id, dsmc_tallies *t) {
+    if (!ctx || !t || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    SysHost &h = *ctx->systems[sys_id];
+    SysTally T;
+    CK(cudaMemcpyAsync(&T, ctx->tally.p + sys_id, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    cudaError_t e;
+    Status st = read_status(ctx, &e);
+    CK(e);
+    std::memset(t, 0, sizeof(*t));
+    t->step = st.step;
+    t->collisions = T.collisions;
+    t->wall_collisions = T.wall_hits;
+    t->reseeds = T.reseeds;
+    t->particle_steps = T.particle_steps;
+    for (int a = 0; a < 3; ++a) t->count_periodic[a] = T.count_periodic[a];
+    t->samples = T.samples;
+    t->candidates = T.candidates;
+    t->time = st.step * h.settings.dt;
+    // MeasureEnergy / MeasureTemperature (dsmc/statisticalproperty.cpp:21-71)
+    // from the current velocities, summed per cell and then in cell order.
+    const int C = h.active_end - h.active_begin;
+    if (C > 0 && ctx->A0.p) {
+        DevBuf<double> ce;
+        CK(ce.alloc(C));
+        e = is_fp64(ctx) ? fp64::launch_cell_energy(cell_arrays(ctx), particle_arrays(ctx), ctx->cur, h.active_begin,
+                                                    h.active_end, ce.p, ctx->stream)
+                         : split32::launch_cell_energy(cell_arrays(ctx), particle_arrays(ctx), ctx->cur,
+                                                       h.active_begin, h.active_end, ce.p, ctx->stream);
+        CK(e);
+        std::vector<double> hc(C);
+        CK(cudaMemcpyAsync(hc.data(), ce.p, C * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        double sum = 0;
+        for (double x : hc) sum += x;
+        t->kinetic_energy = sum * 0.5 * h.settings.mass * h.atoms_per_molecule;
+        if (h.num_particles > 0)
+            t->temperature = ctx->units.temperature_to_SI(2.0 / 3.0 * t->kinetic_energy /
+                                                          (h.num_particles * h.atoms_per_molecule));
+    }
+    const double elapsed = t->time - h.t0_reduced;
+    const int fd = h.settings.flow_direction;
+    if (fd >= 0 && fd < 3 && elapsed > 0) t->flux = h.atoms_per_molecule * T.count_periodic[fd] / elapsed;
+    return DSMC_OK;
+}
+
+int dsmc_tallies_reset(dsmc_ctx *ctx, int sys_id) {
+    if (!ctx || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    SysHost &h = *ctx->systems[sys_id];
+    CK(cudaMemsetAsync(ctx->tally.p + sys_id, 0, sizeof(SysTally), ctx->stream));
+    const int C = h.active_end - h.active_begin;
+    if (C > 0) CK(cudaMemsetAsync(ctx->mom.p + 8 * (size_t)h.active_begin, 0, 8 * (size_t)C * sizeof(double), ctx->stream));
+    cudaError_t e;
+    Status st = read_status(ctx, &e);
+    CK(e);
+    h.t0_reduced = st.step * h.settings.dt;
+    return DSMC_OK;
+}
+
+int dsmc_cells_get(dsmc_ctx *ctx, int sys_id, int cap, int32_t *global_index, int32_t *count, double *vr_max,
+                   double *rest, double *moments, double *volume, int *num_cells) {
+    if (!ctx || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    SysHost &h = *ctx->systems[sys_id];
+    const int C = h.active_end - h.active_begin;
+    if (num_cells) *num_cells = C;
+    if (cap < C) return fail(ctx, DSMC_ERR_CAPACITY, "output buffers smaller than the active cell count");
+    if (C == 0) return DSMC_OK;
+    const int a0 = h.active_begin;
+    if (global_index) std::memcpy(global_index, h.cell_global.data(), C * sizeof(int32_t));
+    if (volume) std::memcpy(volume, h.volume_cell.data(), C * sizeof(double));
+    if (count) {
+        unsigned *cp = ctx->cur ? ctx->count1.p : ctx->count0.p;
+        CK(cudaMemcpyAsync(count, cp + a0, C * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (vr_max) CK(cudaMemcpyAsync(vr_max, ctx->vr_max.p + a0, C * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (rest) CK(cudaMemcpyAsync(rest, ctx->rest.p + a0, C * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    if (moments)
+        CK(cudaMemcpyAsync(moments, ctx->mom.p + 8 * (size_t)a0, 8 * (size_t)C * sizeof(double), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DSMC_OK;
+}
+
+int dsmc_cells_set_state(dsmc_ctx *ctx, int sys_id, const double *vr_max, const double *rest) {
+    if (!ctx || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    SysHost &h = *ctx->systems[sys_id];
+    const int C = h.active_end - h.active_begin;
+    if (C == 0) return DSMC_OK;
+    if (vr_max) CK(cudaMemcpyAsync(ctx->vr_max.p + h.active_begin, vr_max, C * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if (rest) CK(cudaMemcpyAsync(ctx->rest.p + h.active_begin, rest, C * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DSMC_OK;
+}
+
+void *dsmc_stream(dsmc_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int dsmc_counters_get(dsmc_ctx *ctx, int sys_id, int64_t out[8]) {
+    if (!ctx || !out || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+    SysTally T;
+    CK(cudaMemcpyAsync(&T, ctx->tally.p + sys_id, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    out[0] = (int64_t)T.collisions;
+    out[1] = (int64_t)T.wall_hits;
+    out[2] = (int64_t)T.reseeds;
+    out[3] = (int64_t)T.particle_steps;
+    out[4] = T.count_periodic[0];
+    out[5] = T.count_periodic[1];
+    out[6] = T.count_periodic[2];
+    out[7] = (int64_t)T.samples;
+    return DSMC_OK;
+}
+
+int dsmc_device_status(dsmc_ctx *ctx, uint32_t *error_bits, uint32_t *spill) {
+    if (!ctx) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaError_t e;
+    Status st = read_status(ctx, &e);
+    CK(e);
+    if (error_bits) *error_bits = st.error;
+    if (spill) *spill = st.spill;
+    return DSMC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,141 @@
+// Device-side data layout of the DSMC timestep, shared by host and device code.
+//
+// One "system" is one voxel geometry with its gas (the reference's System,
+// dsmc/system.h:29-120).  Many systems advance together: their active cells
+// are concatenated into one cell range, and every kernel walks that range.
+//
+// Particles live in per-cell slot regions (a bucketed counting sort):
+//   active cell a owns slots [cell_base[a], cell_base[a] + cell_cap[a]) of
+//   each particle array, cell_count[b][a] of them occupied in buffer b.
+// Buffers b = 0/1 ping-pong: the fused pass reads buffer `cur` and inserts
+// every moved particle into its new cell's region of buffer `cur ^ 1`.
+//
+// Record formats (structure of arrays, 16-byte vectors):
+//   split precision:  A = uint4 {voxel (i | j<<11 | k<<22), ox, oy, oz (fp32 bits)}
+//                     B = float4 {vx, vy, vz, id (u32 bits)}
+//                     ox,oy,oz in [0,1) voxel units; v in reduced units.
+//   fp64 reference:   A = double4 {rx, ry, rz, id}   B = double4 {vx, vy, vz, 0}
+//                     the reference's own representation (dsmc/system.h:74-75).
+#pragma once
+#include <stdint.h>
+#include <vector_types.h>
+
+#define DSMC_VOX_EMPTY 0
+#define DSMC_VOX_WALL 1
+#define DSMC_VOX_BOUNDARY 2
+
+#define DSMC_TAG_MOVE 1u
+#define DSMC_TAG_COLLIDE 2u
+#define DSMC_TAG_INIT 3u
+
+// error bits reported in Status::error
+#define DSMC_EBIT_CELL 1u        // a particle ended in a cell with no free volume
+#define DSMC_EBIT_FACET 2u       // facet search found no face of the hit voxel
+#define DSMC_EBIT_RESEED 4u      // re-seeding found no empty voxel within its limit
+#define DSMC_EBIT_SPILL_FULL 8u  // the overflow list itself overflowed
+#define DSMC_EBIT_SMEM 16u       // a cell held more particles than the staging buffer
+#define DSMC_EBIT_NAN 32u        // non-finite position or velocity
+// bits that stop the pipeline (a failed facet search re-seeds the particle and goes on)
+#define DSMC_EBIT_FATAL (DSMC_EBIT_CELL | DSMC_EBIT_RESEED | DSMC_EBIT_SPILL_FULL | DSMC_EBIT_SMEM | DSMC_EBIT_NAN)
+
+#define DSMC_VOX_PACK(i, j, k) ((uint32_t)(i) | ((uint32_t)(j) << 11) | ((uint32_t)(k) << 22))
+#define DSMC_VOX_I(p) ((int)((p)&0x7FFu))
+#define DSMC_VOX_J(p) ((int)(((p) >> 11) & 0x7FFu))
+#define DSMC_VOX_K(p) ((int)((p) >> 22))
+
+namespace dsmc {
+
+struct SysDev {
+    // voxel grid (no halo; periodic index wrap replaces the reference's 27x copy)
+    int n[3];                  // voxels per axis
+    int cells[3];              // cells per axis
+    int vpc[3];                // voxels per cell per axis
+    float inv_vpc[3];
+    const uint8_t *vox;        // voxel type, index (i*ny + j)*nz + k
+    const float *nrm, *t1, *t2;  // 3 floats per voxel, same order
+    const int *cell_map;       // global cell (i*cy + j)*cz + k -> active cell id, -1 if solid
+    int active_begin, active_end;
+    // geometry constants
+    double L[3], invL[3];
+    double vox_len[3];         // L/n (the reference's Grid::voxel_size, dsmc/grid.cpp:17-19)
+    double ref_scale[3];       // (double)(float)(invL*n): Grid::one_over_length_*_times_global_n*
+    double ref_shift[3];       // (double)(float)(n):      Grid::constant_* (one rank, origin 0)
+    float inv_vox_f[3];        // n/L in fp32 (split-precision mover)
+    float L_f[3];
+    // physics
+    double dt;
+    float dt_f;
+    double accel_dt;           // gravity*dt along flow_dir
+    float accel_dt_f;
+    int flow_dir;              // -1: no acceleration
+    double wall_s;             // sqrt(T_wall/m) (dsmc/system.cpp:343)
+    float wall_s_f;
+    uint64_t seed;
+    int sample_interval;       // sample when step % interval == 0 and step >= sample_begin
+    int sample_begin;
+};
+
+struct SysTally {
+    unsigned long long collisions;
+    unsigned long long wall_hits;
+    unsigned long long reseeds;
+    unsigned long long particle_steps;
+    long long count_periodic[3];   // net boundary crossings (dsmc/moleculemover.h:29-38)
+    unsigned long long samples;    // sampled steps folded into the cell moments
+    unsigned long long candidates;
+};
+
+struct Status {
+    unsigned int error;        // DSMC_EBIT_* bits
+    unsigned int spill;        // particles written to the overflow list this pass
+    unsigned int step;         // current step number (the reference's System::steps)
+    unsigned int blocks_done;  // end-of-pass counter used to advance `step`
+    unsigned int halted;       // non-zero: a pass saw spill/error; later passes do nothing
+    unsigned int pad[3];
+};
+
+struct SpillRec {
+    uint4 a;
+    uint4 b;        // raw bits of B
+    double4 ra;     // fp64 records
+    double4 rb;
+    int cell;
+    int pad[3];
+};
+
+struct CellArrays {
+    int num_cells;             // total active cells over all systems
+    const int *sys;            // system of each active cell
+    const int *global;         // the reference's cell index (dsmc/system.h:130-132)
+    const unsigned *base;      // first slot
+    const unsigned *cap;       // slots
+    unsigned *count[2];        // occupancy per buffer
+    double *vr_max;            // (sigma*c_r)_max bookkeeping, fp64 (dsmc/cell.cpp:75-111)
+    double *rest;              // selection remainder (dsmc/cell.cpp:42-51)
+    const double *coeff;       // 0.5 F_N pi d^2 dt / V_cell (dsmc/cell.cpp:27-40)
+    double *mom;               // 8 fp64 per cell: n, sum v (3), sum v^2 (3), sum |v|^2
+    unsigned *key;             // per slot: new active cell after a stand-alone move stage
+};
+
+struct ParticleArrays {
+    void *A[2];
+    void *B[2];
+    SpillRec *spill;
+    unsigned spill_cap;
+};
+
+struct PassParams {
+    const SysDev *sys;
+    SysTally *tally;
+    Status *status;
+    CellArrays cells;
+    ParticleArrays parts;
+    int cur;                   // buffer read this pass
+    int do_collide;            // collide the cells of the pass's input (step - 1's sort)
+    int do_move;               // accelerate + move + re-bin (step)
+    int do_sample;             // sample after the collide, on the reference's cadence
+    int smem_cap;              // staging capacity per warp (particles)
+    int advance_step;          // increment Status::step at the end of the pass
+};
+
+}  // namespace dsmc

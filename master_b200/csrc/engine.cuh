@@ -1,0 +1,922 @@
+// The DSMC timestep kernels, templated on the precision policy.
+//
+// One kernel, `pass_kernel`, walks every active cell of every system (one warp
+// per cell, persistent grid) and, depending on its mode flags, performs
+//   collide (NTC, dsmc/cell.cpp:42-111) -> sample (cell moments)
+//   -> accelerate (dsmc/system.cpp:133-144) -> move with diffuse walls
+//      (dsmc/moleculemover.cpp:50-126) -> periodic wrap + flux tally
+//      (dsmc/moleculemover.h:29-38) -> re-bin into the new cell
+//      (dsmc/system.cpp:146-157)
+// on the cell's particles.  The fused production pass does all of them in one
+// read and one write of every particle.  The same device functions serve the
+// stand-alone stage passes.
+//
+// Included by kernels_split.cu (fp32 state, FMA allowed) and by
+// kernels_fp64.cu (the reference's fp64 arithmetic; built with -fmad=false so
+// every product and sum rounds as the reference's x86-64 build does).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dsmc_layout.h"
+#include "dsmc_philox.cuh"
+
+namespace dsmc {
+
+enum PassMode { MODE_FUSED = 0, MODE_INPLACE = 1, MODE_SORT = 2 };
+
+__device__ __forceinline__ float one_minus_ulp() { return __int_as_float(0x3f7fffff); }
+
+__device__ __forceinline__ int wrap_index(int c, int n) {
+    if (c >= 0 && c < n) return c;
+    if (c >= -n && c < 2 * n) return c < 0 ? c + n : c - n;
+    int x = c % n;
+    return x < 0 ? x + n : x;
+}
+
+__device__ __forceinline__ uint32_t voxel_linear(const SysDev &g, int i, int j, int k) {
+    return ((uint32_t)wrap_index(i, g.n[0]) * (uint32_t)g.n[1] + (uint32_t)wrap_index(j, g.n[1])) *
+               (uint32_t)g.n[2] +
+           (uint32_t)wrap_index(k, g.n[2]);
+}
+
+__device__ __forceinline__ int voxel_type(const SysDev &g, int i, int j, int k) {
+    return __ldg(g.vox + voxel_linear(g, i, j, k));
+}
+
+struct MoveTally {
+    int wall_hits, reseeds;
+    int cross[3];
+    unsigned err;
+};
+
+// ============================================================================
+// Split precision: int voxel + fp32 offset in [0,1) voxel units, fp32 velocity.
+// ============================================================================
+struct Split32 {
+    typedef float real;
+    typedef uint4 RecA;
+    typedef float4 RecB;
+
+    struct Particle {
+        int c[3];
+        float o[3];
+        float v[3];
+        uint32_t id;
+    };
+
+    static __device__ __forceinline__ void unpack(const uint4 &a, const float4 &b, Particle &p) {
+        p.c[0] = DSMC_VOX_I(a.x);
+        p.c[1] = DSMC_VOX_J(a.x);
+        p.c[2] = DSMC_VOX_K(a.x);
+        p.o[0] = __uint_as_float(a.y);
+        p.o[1] = __uint_as_float(a.z);
+        p.o[2] = __uint_as_float(a.w);
+        p.v[0] = b.x;
+        p.v[1] = b.y;
+        p.v[2] = b.z;
+        p.id = __float_as_uint(b.w);
+    }
+    static __device__ __forceinline__ void pack(const Particle &p, uint4 &a, float4 &b) {
+        a.x = DSMC_VOX_PACK(p.c[0], p.c[1], p.c[2]);
+        a.y = __float_as_uint(p.o[0]);
+        a.z = __float_as_uint(p.o[1]);
+        a.w = __float_as_uint(p.o[2]);
+        b.x = p.v[0];
+        b.y = p.v[1];
+        b.z = p.v[2];
+        b.w = __uint_as_float(p.id);
+    }
+    static __device__ __forceinline__ void stage_load(const uint4 *, const float4 *B, size_t i, float v[3],
+                                                      uint32_t &id) {
+        const float4 b = B[i];
+        v[0] = b.x;
+        v[1] = b.y;
+        v[2] = b.z;
+        id = __float_as_uint(b.w);
+    }
+
+    // r += w*tau in voxel units, carrying whole voxels into the index.
+    static __device__ __forceinline__ void advance(int c[3], float o[3], const float w[3], float tau) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            float x = fmaf(w[d], tau, o[d]);
+            if (x >= 1.0f || x < 0.0f) {
+                float f = floorf(x);
+                c[d] += (int)f;
+                x -= f;
+                if (x >= 1.0f) x = one_minus_ulp();
+            }
+            o[d] = x;
+        }
+    }
+
+    // Grid::get_time_until_collision (dsmc/grid.h:82-137) in voxel units: the
+    // earliest positive crossing of a face of voxel cb whose hit point lies on
+    // that face (bounds inclusive), faces in the reference's order
+    // x-, x+, y-, y+, z-, z+; 0 below 1e-5, else minus 1e-7.
+    static __device__ __forceinline__ float facet_time(const float d[3], const float w[3], int &axis, int &side) {
+        float best = 1e9f;
+        axis = -1;
+        side = 0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const float t = ((float)s - d[a]) / w[a];
+                if (!(t > 0.0f && t < best)) continue;
+                const int b1 = (a + 1) % 3, b2 = (a + 2) % 3;
+                const float h1 = fmaf(w[b1], t, d[b1]);
+                const float h2 = fmaf(w[b2], t, d[b2]);
+                // fp32 hit points on an edge can round just outside the face
+                const float eps = 1e-6f;
+                if (h1 >= -eps && h1 <= 1.0f + eps && h2 >= -eps && h2 <= 1.0f + eps) {
+                    best = t;
+                    axis = a;
+                    side = s;
+                }
+            }
+        }
+        if (axis < 0) return -1.0f;
+        return best < 1e-5f ? 0.0f : best - 1e-7f;
+    }
+
+    // System::find_position (dsmc/system.cpp:384-396): uniform in the box until
+    // the voxel is empty.
+    static __device__ bool reseed(const SysDev &g, Particle &p, DrawStream &rs) {
+        for (int tries = 0; tries < 100000; ++tries) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                const float x = rs.uniform32() * (float)g.n[d];
+                int c = (int)x;
+                if (c > g.n[d] - 1) c = g.n[d] - 1;
+                float o = x - (float)c;
+                if (o >= 1.0f) o = one_minus_ulp();
+                p.c[d] = c;
+                p.o[d] = o;
+            }
+            if (voxel_type(g, p.c[0], p.c[1], p.c[2]) < DSMC_VOX_WALL) return true;
+        }
+        return false;
+    }
+
+    // ColliderThermal::collide (dsmc/colliderthermal.cpp:13-46).
+    static __device__ __forceinline__ void reflect(const SysDev &g, uint32_t vlin, float v[3], DrawStream &rs) {
+        const float s = g.wall_s_f;
+        const float vn = s * sqrtf(-2.0f * logf(rs.uniform32()));
+        float u = rs.uniform32();
+        float c = rs.uniform32();
+        const float g1 = sqrtf(-2.0f * logf(1.0f - u)) * cosf(6.283185307f * c);
+        u = rs.uniform32();
+        c = rs.uniform32();
+        const float g2 = sqrtf(-2.0f * logf(1.0f - u)) * cosf(6.283185307f * c);
+        const float vt1 = s * g1, vt2 = s * g2;
+        const float *n = g.nrm + 3 * (size_t)vlin;
+        const float *a = g.t1 + 3 * (size_t)vlin;
+        const float *b = g.t2 + 3 * (size_t)vlin;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) v[d] = vn * __ldg(n + d) + vt1 * __ldg(a + d) + vt2 * __ldg(b + d);
+    }
+
+    // MoleculeMover::move_molecule (dsmc/moleculemover.cpp:50-126) with its
+    // recursion unrolled into a loop, then the periodic wrap.
+    //
+    // In the reference every "move back by tau" of the facet loop
+    // (dsmc/moleculemover.cpp:95-108) returns the particle to the position it
+    // had at the start of the sub-step (the bisection's halvings and the
+    // facet move are undone exactly in exact arithmetic).  In fp32 offsets
+    // that subtraction drifts by an ulp, which is more than the 1e-7 time
+    // units the reference leaves before a face for slow particles, so the
+    // sub-step's start position is kept and restored instead.
+    static __device__ void move(const SysDev &g, Particle &p, uint32_t step, MoveTally &t) {
+        DrawStream rs;
+        rs.init(g.seed, p.id, step, DSMC_TAG_MOVE);
+        float w[3] = {p.v[0] * g.inv_vox_f[0], p.v[1] * g.inv_vox_f[1], p.v[2] * g.inv_vox_f[2]};
+        float dt = g.dt_f;
+        for (int depth = 0;; ++depth) {
+            if (voxel_type(g, p.c[0], p.c[1], p.c[2]) != DSMC_VOX_EMPTY) {
+                ++t.reseeds;
+                if (!reseed(g, p, rs)) t.err |= DSMC_EBIT_RESEED;
+                break;
+            }
+            const int c0[3] = {p.c[0], p.c[1], p.c[2]};
+            const float o0[3] = {p.o[0], p.o[1], p.o[2]};
+            float tau = dt;
+            advance(p.c, p.o, w, tau);
+            int vt = voxel_type(g, p.c[0], p.c[1], p.c[2]);
+            if (vt == DSMC_VOX_EMPTY) break;
+            // Bisect back out of solid (wall) voxels until a boundary voxel.
+            bool stop = false, again = false;
+            int count = 0;
+            while (vt != DSMC_VOX_BOUNDARY) {
+                if (++count > 100) {
+                    ++t.reseeds;
+                    if (!reseed(g, p, rs)) t.err |= DSMC_EBIT_RESEED;
+                    stop = true;
+                    break;
+                }
+                if (vt == DSMC_VOX_WALL) {
+                    tau *= 0.5f;
+                    advance(p.c, p.o, w, -tau);
+                    vt = voxel_type(g, p.c[0], p.c[1], p.c[2]);
+                } else {
+                    dt -= tau;
+                    again = dt > 1e-5f && depth < 10;
+                    stop = !again;
+                    break;
+                }
+            }
+            if (stop) break;
+            if (again) continue;
+            // Back off and stop just short of the first boundary voxel's face.
+            int cb[3] = {p.c[0], p.c[1], p.c[2]};
+            count = 0;
+            while (vt == DSMC_VOX_BOUNDARY) {
+                if (++count > 100) {
+                    ++t.reseeds;
+                    if (!reseed(g, p, rs)) t.err |= DSMC_EBIT_RESEED;
+                    stop = true;
+                    break;
+                }
+                cb[0] = p.c[0];
+                cb[1] = p.c[1];
+                cb[2] = p.c[2];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    p.c[a] = c0[a];
+                    p.o[a] = o0[a];
+                }
+                float d[3];
+                bool outside = false;
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    d[a] = (float)(p.c[a] - cb[a]) + p.o[a];
+                    outside |= (d[a] < 0.0f) | (d[a] >= 1.0f);
+                }
+                int axis, side;
+                const float tf = facet_time(d, w, axis, side);
+                if (tf < 0.0f) {
+                    t.err |= DSMC_EBIT_FACET;
+                    ++t.reseeds;
+                    if (!reseed(g, p, rs)) t.err |= DSMC_EBIT_RESEED;
+                    stop = true;
+                    break;
+                }
+                tau = tf;
+                advance(p.c, p.o, w, tau);
+                // fp32 offsets can round onto the face the fp64 reference stops
+                // 1e-7 time units short of; put the particle back outside.
+                if (outside && tau > 0.0f && p.c[0] == cb[0] && p.c[1] == cb[1] && p.c[2] == cb[2]) {
+                    if (side == 0) {
+                        p.c[axis] = cb[axis] - 1;
+                        p.o[axis] = one_minus_ulp();
+                    } else {
+                        p.c[axis] = cb[axis] + 1;
+                        p.o[axis] = 0.0f;
+                    }
+                }
+                vt = voxel_type(g, p.c[0], p.c[1], p.c[2]);
+            }
+            if (stop) break;
+            dt -= tau;
+            reflect(g, voxel_linear(g, cb[0], cb[1], cb[2]), p.v, rs);
+            ++t.wall_hits;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) w[d] = p.v[d] * g.inv_vox_f[d];
+            if (!(dt > 1e-5f && depth < 10)) break;
+        }
+        // Periodic wrap, one box length at most, counting net crossings.
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (p.c[d] >= g.n[d]) {
+                p.c[d] -= g.n[d];
+                ++t.cross[d];
+            } else if (p.c[d] < 0) {
+                p.c[d] += g.n[d];
+                --t.cross[d];
+            }
+            if (!(p.o[d] >= 0.0f && p.o[d] < 1.0f) || !isfinite(p.v[d]) || p.c[d] < 0 || p.c[d] >= g.n[d]) {
+                t.err |= DSMC_EBIT_NAN;
+                p.c[d] = min(max(p.c[d], 0), g.n[d] - 1);
+                p.o[d] = 0.5f;
+            }
+        }
+    }
+
+    // Cell of the particle: whole voxels per cell, so cell = voxel / vpc.
+    static __device__ __forceinline__ int cell_global(const SysDev &g, const Particle &p) {
+        int ci[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            int c = __float2int_rz(((float)p.c[d] + 0.5f) * g.inv_vpc[d]);
+            ci[d] = min(c, g.cells[d] - 1);
+        }
+        return (ci[0] * g.cells[1] + ci[1]) * g.cells[2] + ci[2];
+    }
+
+    static __device__ __forceinline__ void accelerate(const SysDev &g, Particle &p) {
+        if (g.flow_dir >= 0) p.v[g.flow_dir] += g.accel_dt_f;
+    }
+};
+
+// ============================================================================
+// fp64 reference arithmetic: absolute fp64 positions as in System::r
+// (dsmc/system.h:74), the reference's float-rounded index constants.
+// ============================================================================
+struct Vec3d {
+    double x, y, z;
+};
+__device__ __forceinline__ Vec3d v3(double x, double y, double z) {
+    Vec3d r;
+    r.x = x;
+    r.y = y;
+    r.z = z;
+    return r;
+}
+__device__ __forceinline__ Vec3d v3sub(const Vec3d &a, const Vec3d &b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ Vec3d v3add(const Vec3d &a, const Vec3d &b) { return v3(b.x + a.x, b.y + a.y, b.z + a.z); }
+__device__ __forceinline__ Vec3d v3scale(const Vec3d &a, double s) { return v3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ double v3dot(const Vec3d &a, const Vec3d &o) { return a.x * o.x + a.y * o.y + a.z * o.z; }
+// CVector::cross (dsmc/cvector.h:148-150): this x o
+__device__ __forceinline__ Vec3d v3cross(const Vec3d &t, const Vec3d &o) {
+    return v3(o.y * t.z - o.z * t.y, o.z * t.x - o.x * t.z, o.x * t.y - o.y * t.x);
+}
+// same_side / is_point_within_square (dsmc/grid.h:21-41)
+__device__ __forceinline__ bool same_side(const Vec3d &p1, const Vec3d &p2, const Vec3d &a, const Vec3d &b) {
+    const Vec3d ba = v3sub(b, a);
+    const Vec3d cp1 = v3cross(ba, v3sub(p1, a));
+    const Vec3d cp2 = v3cross(ba, v3sub(p2, a));
+    return v3dot(cp1, cp2) >= 0;
+}
+__device__ __forceinline__ bool within_square(const Vec3d &p1, const Vec3d &p2, const Vec3d &p3, const Vec3d &p4,
+                                              const Vec3d &pt) {
+    const Vec3d c = v3scale(v3add(v3add(v3add(p1, p2), p3), p4), 0.25);
+    return same_side(pt, c, p1, p2) && same_side(pt, c, p2, p3) && same_side(pt, c, p3, p4) &&
+           same_side(pt, c, p4, p1);
+}
+
+struct Fp64 {
+    typedef double real;
+    typedef double4 RecA;
+    typedef double4 RecB;
+
+    struct Particle {
+        double r[3];
+        double v[3];
+        uint32_t id;
+    };
+
+    static __device__ __forceinline__ void unpack(const double4 &a, const double4 &b, Particle &p) {
+        p.r[0] = a.x;
+        p.r[1] = a.y;
+        p.r[2] = a.z;
+        p.id = (uint32_t)a.w;
+        p.v[0] = b.x;
+        p.v[1] = b.y;
+        p.v[2] = b.z;
+    }
+    static __device__ __forceinline__ void pack(const Particle &p, double4 &a, double4 &b) {
+        a.x = p.r[0];
+        a.y = p.r[1];
+        a.z = p.r[2];
+        a.w = (double)p.id;
+        b.x = p.v[0];
+        b.y = p.v[1];
+        b.z = p.v[2];
+        b.w = 0.0;
+    }
+    static __device__ __forceinline__ void stage_load(const double4 *A, const double4 *B, size_t i, double v[3],
+                                                      uint32_t &id) {
+        const double4 b = B[i];
+        v[0] = b.x;
+        v[1] = b.y;
+        v[2] = b.z;
+        id = (uint32_t)A[i].w;
+    }
+
+    // Grid::get_index_of_voxel (dsmc/grid.h:139-145): i = int(r*float(n/L) +
+    // float(halo offset)) in the 3x halo grid; returned here relative to the
+    // box (halo offset subtracted, may lie in [-n, 2n)).
+    static __device__ __forceinline__ void voxel_of(const SysDev &g, const double r[3], int u[3]) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) u[d] = (int)(r[d] * g.ref_scale[d] + g.ref_shift[d]) - g.n[d];
+    }
+    static __device__ __forceinline__ int type_at(const SysDev &g, const double r[3], int u[3]) {
+        voxel_of(g, r, u);
+        return voxel_type(g, u[0], u[1], u[2]);
+    }
+    static __device__ __forceinline__ void do_move(double r[3], const double v[3], double tau) {
+#pragma unroll
+        for (int d = 0; d < 3; ++d) r[d] += v[d] * tau;
+    }
+
+    // Grid::get_time_until_collision (dsmc/grid.h:82-137), operation by operation.
+    static __device__ double facet_time(const SysDev &g, const double r[3], const double v[3], const int b[3],
+                                        bool &found) {
+        const Vec3d R = v3(r[0] - 0.0, r[1] - 0.0, r[2] - 0.0);
+        const Vec3d V = v3(v[0], v[1], v[2]);
+        const double hx = g.vox_len[0], hy = g.vox_len[1], hz = g.vox_len[2];
+        const int i = b[0], j = b[1], k = b[2];
+        Vec3d P[8];
+        P[0] = v3(i * hx, j * hy, k * hz);
+        P[1] = v3((i + 1) * hx, j * hy, k * hz);
+        P[2] = v3(i * hx, j * hy, (k + 1) * hz);
+        P[3] = v3((i + 1) * hx, j * hy, (k + 1) * hz);
+        P[4] = v3(i * hx, (j + 1) * hy, k * hz);
+        P[5] = v3((i + 1) * hx, (j + 1) * hy, k * hz);
+        P[6] = v3(i * hx, (j + 1) * hy, (k + 1) * hz);
+        P[7] = v3((i + 1) * hx, (j + 1) * hy, (k + 1) * hz);
+        const Vec3d N[6] = {v3(-1, 0, 0), v3(1, 0, 0), v3(0, -1, 0), v3(0, 1, 0), v3(0, 0, -1), v3(0, 0, 1)};
+        const int plane_point[6] = {2, 1, 0, 4, 0, 2};
+        const int sq[6][4] = {{4, 0, 2, 6}, {1, 5, 7, 3}, {0, 1, 3, 2}, {5, 4, 6, 7}, {4, 5, 1, 0}, {2, 3, 7, 6}};
+        double best = 1e9;
+        found = false;
+        for (int f = 0; f < 6; ++f) {
+            const double tf = v3dot(v3sub(P[plane_point[f]], R), N[f]) / v3dot(V, N[f]);
+            const bool hit = within_square(P[sq[f][0]], P[sq[f][1]], P[sq[f][2]], P[sq[f][3]], v3add(R, v3scale(V, tf)));
+            if (tf > 0 && tf < best && hit && !isnan(tf)) {
+                best = tf;
+                found = true;
+            }
+        }
+        if (best < 1e-5) return 0;
+        return best - 1e-7;
+    }
+
+    // System::find_position (dsmc/system.cpp:384-396) with Grid::get_voxel(r, n)
+    // (dsmc/grid.cpp:63-69): all-double index arithmetic.
+    static __device__ bool reseed(const SysDev &g, Particle &p, DrawStream &rs) {
+        for (int tries = 0; tries < 100000; ++tries) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) p.r[d] = 0.0 + g.L[d] * rs.uniform64();
+            int u[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d)
+                u[d] = (int)((p.r[d] - 0.0) * g.invL[d] * (double)g.n[d] + (double)g.n[d]) - g.n[d];
+            if (voxel_type(g, u[0], u[1], u[2]) < DSMC_VOX_WALL) return true;
+        }
+        return false;
+    }
+
+    // ColliderThermal::collide (dsmc/colliderthermal.cpp:13-46).
+    static __device__ __forceinline__ void reflect(const SysDev &g, uint32_t vlin, double v[3], DrawStream &rs) {
+        const double s = g.wall_s;
+        const double vn = s * sqrt(-2 * log(rs.uniform64()));
+        double u = rs.uniform64();
+        double c = rs.uniform64();
+        const double g1 = sqrt(-2.0 * log(1.0 - u)) * cos(6.283185307 * c);
+        u = rs.uniform64();
+        c = rs.uniform64();
+        const double g2 = sqrt(-2.0 * log(1.0 - u)) * cos(6.283185307 * c);
+        const double vt1 = s * g1, vt2 = s * g2;
+        const float *n = g.nrm + 3 * (size_t)vlin;
+        const float *a = g.t1 + 3 * (size_t)vlin;
+        const float *b = g.t2 + 3 * (size_t)vlin;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const float nf = __ldg(n + d), af = __ldg(a + d), bf = __ldg(b + d);
+            v[d] = vn * nf + vt1 * af + vt2 * bf;
+        }
+    }
+
+    static __device__ void move(const SysDev &g, Particle &p, uint32_t step, MoveTally &t) {
+        DrawStream rs;
+        rs.init(g.seed, p.id, step, DSMC_TAG_MOVE);
+        double dt = g.dt;
+        int u[3];
+        for (int depth = 0;; ++depth) {
+            double tau = dt;
+            if (type_at(g, p.r, u) != DSMC_VOX_EMPTY) {
+                ++t.reseeds;
+                if (!reseed(g, p, rs)) t.err |= DSMC_EBIT_RESEED;
+                break;
+            }
+            do_move(p.r, p.v, tau);
+            int vt = type_at(g, p.r, u);
+            if (vt < DSMC_VOX_WALL) break;
+            bool stop = false, again = false;
+            int count = 0;
+            while (vt != DSMC_VOX_BOUNDARY) {
+                if (++count > 100) {
+                    ++t.reseeds;
+                    if (!reseed(g, p, rs)) t.err |= DSMC_EBIT_RESEED;
+                    stop = true;
+                    break;
+                }
+                if (vt == DSMC_VOX_WALL) {
+                    tau /= 2;
+                    do_move(p.r, p.v, -tau);
+                    vt = type_at(g, p.r, u);
+                } else {
+                    dt -= tau;
+                    again = dt > 1e-5 && depth < 10;
+                    stop = !again;
+                    break;
+                }
+            }
+            if (stop) break;
+            if (again) continue;
+            int b[3] = {u[0], u[1], u[2]};
+            count = 0;
+            while (vt == DSMC_VOX_BOUNDARY) {
+                if (++count > 100) {
+                    ++t.reseeds;
+                    if (!reseed(g, p, rs)) t.err |= DSMC_EBIT_RESEED;
+                    stop = true;
+                    break;
+                }
+                b[0] = u[0];
+                b[1] = u[1];
+                b[2] = u[2];
+                do_move(p.r, p.v, -tau);
+                bool found;
+                tau = facet_time(g, p.r, p.v, b, found);
+                if (!found) {
+                    t.err |= DSMC_EBIT_FACET;
+                    ++t.reseeds;
+                    if (!reseed(g, p, rs)) t.err |= DSMC_EBIT_RESEED;
+                    stop = true;
+                    break;
+                }
+                do_move(p.r, p.v, tau);
+                vt = type_at(g, p.r, u);
+            }
+            if (stop) break;
+            dt -= tau;
+            reflect(g, voxel_linear(g, b[0], b[1], b[2]), p.v, rs);
+            ++t.wall_hits;
+            if (!(dt > 1e-5 && depth < 10)) break;
+        }
+        // MoleculeMover::apply_periodic_boundary_conditions (dsmc/moleculemover.h:29-38)
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            if (p.r[d] >= g.L[d]) {
+                p.r[d] -= g.L[d];
+                ++t.cross[d];
+            } else if (p.r[d] < 0) {
+                p.r[d] += g.L[d];
+                --t.cross[d];
+            }
+            if (!isfinite(p.r[d]) || !isfinite(p.v[d])) t.err |= DSMC_EBIT_NAN;
+        }
+    }
+
+    // System::cell_index_from_position (dsmc/system.h:122-132).
+    static __device__ __forceinline__ int cell_global(const SysDev &g, const Particle &p) {
+        int ci[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            int c = (int)(p.r[d] * g.invL[d] * g.cells[d]);
+            ci[d] = min(max(c, 0), g.cells[d] - 1);
+        }
+        return (ci[0] * g.cells[1] + ci[1]) * g.cells[2] + ci[2];
+    }
+
+    static __device__ __forceinline__ void accelerate(const SysDev &g, Particle &p) {
+        if (g.flow_dir >= 0) p.v[g.flow_dir] += g.accel_dt;
+    }
+};
+
+// ============================================================================
+// The cell pass.
+// ============================================================================
+template <class Prec> struct WarpStage {
+    typedef typename Prec::real real;
+    real *vx, *vy, *vz;
+    uint32_t *id;
+    uint16_t *perm;
+    static __host__ __device__ size_t bytes(int cap) {
+        size_t b = (size_t)cap * (3 * sizeof(real) + sizeof(uint32_t) + sizeof(uint16_t));
+        return (b + 15) & ~(size_t)15;
+    }
+    __device__ void bind(unsigned char *base, int cap) {
+        vx = reinterpret_cast<real *>(base);
+        vy = vx + cap;
+        vz = vy + cap;
+        id = reinterpret_cast<uint32_t *>(vz + cap);
+        perm = reinterpret_cast<uint16_t *>(id + cap);
+    }
+};
+
+// Cell::prepare + Cell::collide + Cell::collide_molecules (dsmc/cell.cpp:42-111)
+// on one cell staged in shared memory, members in id order.  Run by one lane.
+template <class Prec>
+__device__ void ntc_collide(const SysDev &g, int cell_global_index, uint32_t step, int n, double coeff,
+                            double &vr_max, double &rest, WarpStage<Prec> &st, unsigned long long &collisions,
+                            unsigned long long &candidates) {
+    typedef typename Prec::real real;
+    const double select = coeff * n * (n - 1) * vr_max + rest;
+    const int pairs = (int)round(select);
+    rest = select - pairs;
+    if (n < 2) return;
+    DrawStream rs;
+    rs.init(g.seed, (uint32_t)cell_global_index, step, DSMC_TAG_COLLIDE);
+    double crm = vr_max;
+    const real vmax = (real)vr_max;
+    for (int isel = 0; isel < pairs; ++isel) {
+        const real ua = rs.template uniform<real>();
+        int ip0 = min((int)(ua * (real)n), n - 1);
+        const real ub = rs.template uniform<real>();
+        const int ip1 = ((int)((real)(ip0 + 1) + ub * (real)(n - 1))) % n;
+        const int s0 = st.perm[ip0], s1 = st.perm[ip1];
+        const real dx = st.vx[s0] - st.vx[s1], dy = st.vy[s0] - st.vy[s1], dz = st.vz[s0] - st.vz[s1];
+        const real vrel = sqrt(dx * dx + dy * dy + dz * dz);
+        if ((double)vrel > crm) crm = (double)vrel;
+        const real uc = rs.template uniform<real>();
+        if (vrel > uc * vmax) {
+            ++collisions;
+            const real cmx = (real)0.5 * (st.vx[s0] + st.vx[s1]);
+            const real cmy = (real)0.5 * (st.vy[s0] + st.vy[s1]);
+            const real cmz = (real)0.5 * (st.vz[s0] + st.vz[s1]);
+            const real cos_th = (real)1.0 - (real)2.0 * rs.template uniform<real>();
+            const real sin_th = sqrt((real)1.0 - cos_th * cos_th);
+            const real phi = (real)(2 * 3.14159265358979323846) * rs.template uniform<real>();
+            const real rx = vrel * cos_th;
+            const real ry = vrel * sin_th * cos(phi);
+            const real rz = vrel * sin_th * sin(phi);
+            st.vx[s0] = cmx + (real)0.5 * rx;
+            st.vy[s0] = cmy + (real)0.5 * ry;
+            st.vz[s0] = cmz + (real)0.5 * rz;
+            st.vx[s1] = cmx - (real)0.5 * rx;
+            st.vy[s1] = cmy - (real)0.5 * ry;
+            st.vz[s1] = cmz - (real)0.5 * rz;
+        }
+    }
+    candidates += (unsigned long long)pairs;
+    vr_max = crm;
+}
+
+struct WarpTally {
+    unsigned long long collisions, candidates, wall_hits, reseeds, moved;
+    long long cross[3];
+    unsigned err;
+    int sys;
+};
+
+__device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+__device__ __forceinline__ long long warp_sum_i64(long long x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+__device__ __forceinline__ double warp_sum_f64(double x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+__device__ __forceinline__ void flush_tally(const PassParams &P, WarpTally &w, int lane) {
+    // All lanes call; per-lane partial counts are summed, lane 0 publishes.
+    const unsigned long long wh = warp_sum_u64(w.wall_hits);
+    const unsigned long long rs = warp_sum_u64(w.reseeds);
+    const unsigned long long mv = warp_sum_u64(w.moved);
+    long long cr[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) cr[d] = warp_sum_i64(w.cross[d]);
+    unsigned err = __reduce_or_sync(0xffffffffu, w.err);
+    if (lane == 0 && w.sys >= 0) {
+        SysTally &T = P.tally[w.sys];
+        if (w.collisions) atomicAdd(&T.collisions, w.collisions);
+        if (w.candidates) atomicAdd(&T.candidates, w.candidates);
+        if (wh) atomicAdd(&T.wall_hits, wh);
+        if (rs) atomicAdd(&T.reseeds, rs);
+        if (mv) atomicAdd(&T.particle_steps, mv);
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (cr[d]) atomicAdd((unsigned long long *)&T.count_periodic[d], (unsigned long long)cr[d]);
+        if (err) atomicOr(&P.status->error, err);
+    }
+    w.collisions = w.candidates = w.wall_hits = w.reseeds = w.moved = 0;
+    w.cross[0] = w.cross[1] = w.cross[2] = 0;
+    w.err = 0;
+}
+
+template <class Prec, int MODE>
+__global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
+    typedef typename Prec::real real;
+    typedef typename Prec::RecA RecA;
+    typedef typename Prec::RecB RecB;
+    typedef typename Prec::Particle Particle;
+    extern __shared__ __align__(16) unsigned char smem[];
+
+    const int lane = threadIdx.x & 31;
+    const int warp_in_block = threadIdx.x >> 5;
+    const int warps_per_block = blockDim.x >> 5;
+    const volatile Status *vs = P.status;
+    if (vs->halted) return;
+    const uint32_t step = vs->step;
+    const uint32_t move_step = step + 1;
+
+    WarpStage<Prec> st;
+    st.bind(smem + (size_t)warp_in_block * WarpStage<Prec>::bytes(P.smem_cap), P.smem_cap);
+
+    const RecA *Ain = reinterpret_cast<const RecA *>(P.parts.A[P.cur]);
+    const RecB *Bin = reinterpret_cast<const RecB *>(P.parts.B[P.cur]);
+    RecA *Aout = reinterpret_cast<RecA *>(P.parts.A[P.cur ^ 1]);
+    RecB *Bout = reinterpret_cast<RecB *>(P.parts.B[P.cur ^ 1]);
+    RecA *Aio = reinterpret_cast<RecA *>(P.parts.A[P.cur]);
+    RecB *Bio = reinterpret_cast<RecB *>(P.parts.B[P.cur]);
+    unsigned *cnt_in = P.cells.count[P.cur];
+    unsigned *cnt_out = P.cells.count[P.cur ^ 1];
+
+    WarpTally wt;
+    wt.collisions = wt.candidates = wt.wall_hits = wt.reseeds = wt.moved = 0;
+    wt.cross[0] = wt.cross[1] = wt.cross[2] = 0;
+    wt.err = 0;
+    wt.sys = -1;
+
+    const int C = P.cells.num_cells;
+    const int stride = gridDim.x * warps_per_block;
+    for (int a = blockIdx.x * warps_per_block + warp_in_block; a < C; a += stride) {
+        const int sys = P.cells.sys[a];
+        if (sys != wt.sys) {
+            if (wt.sys >= 0) flush_tally(P, wt, lane);
+            wt.sys = sys;
+        }
+        const SysDev &g = P.sys[sys];
+        int n = (int)min(cnt_in[a], P.cells.cap[a]);
+        const unsigned base = P.cells.base[a];
+        if (n > P.smem_cap) {
+            wt.err |= DSMC_EBIT_SMEM;
+            n = P.smem_cap;
+        }
+        const bool collide = P.do_collide && MODE != MODE_SORT;
+        bool sample = P.do_sample && MODE != MODE_SORT && g.sample_interval > 0 && step > 0 &&
+                      (step % (uint32_t)g.sample_interval) == 0 && step >= (uint32_t)g.sample_begin;
+        const bool need_order = collide || sample;
+
+        // Stage velocities (and ids) in shared memory.
+        if (MODE != MODE_SORT) {
+            for (int s = lane; s < n; s += 32) {
+                real v[3];
+                uint32_t id;
+                Prec::stage_load(Ain, Bin, base + s, v, id);
+                st.vx[s] = v[0];
+                st.vy[s] = v[1];
+                st.vz[s] = v[2];
+                st.id[s] = id;
+            }
+            __syncwarp();
+        }
+        if (need_order) {
+            // Members in id order: rank = number of smaller ids.
+            for (int s = lane; s < n; s += 32) {
+                const uint32_t mine = st.id[s];
+                int rank = 0;
+                for (int q = 0; q < n; ++q) rank += st.id[q] < mine;
+                st.perm[rank] = (uint16_t)s;
+            }
+            __syncwarp();
+        }
+        if (collide) {
+            if (lane == 0) {
+                double vr = P.cells.vr_max[a], rest = P.cells.rest[a];
+                ntc_collide<Prec>(g, P.cells.global[a], step, n, P.cells.coeff[a], vr, rest, st, wt.collisions,
+                                  wt.candidates);
+                P.cells.vr_max[a] = vr;
+                P.cells.rest[a] = rest;
+            }
+            __syncwarp();
+        }
+        if (sample) {
+            double m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int r = lane; r < n; r += 32) {
+                const int s = st.perm[r];
+                const double x = (double)st.vx[s], y = (double)st.vy[s], z = (double)st.vz[s];
+                m[0] += 1.0;
+                m[1] += x;
+                m[2] += y;
+                m[3] += z;
+                m[4] += x * x;
+                m[5] += y * y;
+                m[6] += z * z;
+            }
+#pragma unroll
+            for (int q = 0; q < 7; ++q) m[q] = warp_sum_f64(m[q]);
+            if (lane == 0) {
+                double *M = P.cells.mom + 8 * (size_t)a;
+#pragma unroll
+                for (int q = 0; q < 7; ++q) M[q] += m[q];
+                M[7] += m[4] + m[5] + m[6];
+                if (a == g.active_begin) atomicAdd(&P.tally[sys].samples, 1ull);
+            }
+        }
+        if (MODE == MODE_FUSED || MODE == MODE_SORT) {
+            if (lane == 0) cnt_in[a] = 0;
+        }
+
+        // Move (or pass through) and place every particle.
+        const int chunks = (n + 31) >> 5;
+        for (int ch = 0; ch < chunks; ++ch) {
+            const int s = ch * 32 + lane;
+            const bool valid = s < n;
+            Particle p;
+            unsigned key = 0xffffffffu;
+            if (valid) {
+                RecA ra = Ain[base + s];
+                RecB rb = Bin[base + s];
+                Prec::unpack(ra, rb, p);
+                if (MODE != MODE_SORT) {
+                    p.v[0] = st.vx[s];
+                    p.v[1] = st.vy[s];
+                    p.v[2] = st.vz[s];
+                }
+                if (MODE == MODE_SORT) {
+                    key = P.cells.key[base + s];
+                } else if (P.do_move) {
+                    Prec::accelerate(g, p);
+                    MoveTally mt;
+                    mt.wall_hits = mt.reseeds = 0;
+                    mt.cross[0] = mt.cross[1] = mt.cross[2] = 0;
+                    mt.err = 0;
+                    Prec::move(g, p, move_step, mt);
+                    wt.wall_hits += mt.wall_hits;
+                    wt.reseeds += mt.reseeds;
+                    wt.cross[0] += mt.cross[0];
+                    wt.cross[1] += mt.cross[1];
+                    wt.cross[2] += mt.cross[2];
+                    wt.err |= mt.err;
+                    wt.moved += 1;
+                    const int cg = Prec::cell_global(g, p);
+                    const int ac = __ldg(g.cell_map + cg);
+                    if (ac < 0) {
+                        wt.err |= DSMC_EBIT_CELL;
+                        key = (unsigned)a;
+                    } else {
+                        key = (unsigned)ac;
+                    }
+                } else {
+                    key = (unsigned)a;
+                }
+            }
+            if (MODE == MODE_INPLACE) {
+                if (valid) {
+                    RecA ra;
+                    RecB rb;
+                    Prec::pack(p, ra, rb);
+                    if (P.do_move) {
+                        Aio[base + s] = ra;
+                        P.cells.key[base + s] = key;
+                    }
+                    if (P.do_move || collide) Bio[base + s] = rb;
+                }
+            } else {
+                // Warp-aggregated counting-sort insert into the new cell's slots.
+                const unsigned peers = __match_any_sync(0xffffffffu, key);
+                const int leader = __ffs(peers) - 1;
+                const unsigned lower = peers & ((1u << lane) - 1u);
+                unsigned slot0 = 0;
+                if (valid && lane == leader) slot0 = atomicAdd(&cnt_out[key], (unsigned)__popc(peers));
+                slot0 = __shfl_sync(0xffffffffu, slot0, leader);
+                if (valid) {
+                    const unsigned slot = slot0 + (unsigned)__popc(lower);
+                    RecA ra;
+                    RecB rb;
+                    Prec::pack(p, ra, rb);
+                    if (slot < P.cells.cap[key]) {
+                        const unsigned dst = P.cells.base[key] + slot;
+                        Aout[dst] = ra;
+                        Bout[dst] = rb;
+                    } else {
+                        const unsigned si = atomicAdd(&P.status->spill, 1u);
+                        if (si < P.parts.spill_cap) {
+                            SpillRec &sr = P.parts.spill[si];
+                            if (sizeof(real) == 8) {
+                                sr.ra = *reinterpret_cast<const double4 *>(&ra);
+                                sr.rb = *reinterpret_cast<const double4 *>(&rb);
+                            } else {
+                                sr.a = *reinterpret_cast<const uint4 *>(&ra);
+                                sr.b = *reinterpret_cast<const uint4 *>(&rb);
+                            }
+                            sr.cell = (int)key;
+                        } else {
+                            wt.err |= DSMC_EBIT_SPILL_FULL;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (wt.sys >= 0) flush_tally(P, wt, lane);
+
+    // End of pass: the last block to finish advances the step and halts the
+    // pipeline if anything spilled or failed.
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned done = atomicAdd(&P.status->blocks_done, 1u);
+        if (done == gridDim.x - 1) {
+            __threadfence();
+            if (P.advance_step) atomicAdd(&P.status->step, 1u);
+            if (atomicAdd(&P.status->spill, 0u) != 0u || (atomicAdd(&P.status->error, 0u) & DSMC_EBIT_FATAL) != 0u)
+                atomicExch(&P.status->halted, 1u);
+            atomicExch(&P.status->blocks_done, 0u);
+        }
+    }
+}
+
+}  // namespace dsmc

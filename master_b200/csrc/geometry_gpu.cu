@@ -1,0 +1,224 @@
+// Geometry preprocessing on the GPU: surface normals, tangent frames and
+// boundary typing of a voxel mask, byte-identical to the CPU path
+// (dsmc_geometry_finish, which follows ComplexGeometry::calculate_normals,
+// calculate_tangents and find_boundary_points, dsmc/complexgeometry.cpp:928-1063).
+//
+// The reference sweeps voxels in index order and empties, in place, solid
+// voxels that have no normal but an empty neighbour, so a voxel can see
+// removals made earlier in the sweep.  The GPU evaluates every voxel against
+// the unmodified mask (one thread per voxel); the host then replays, in sweep
+// order, only the voxels whose window can contain an earlier removal: the
+// removal candidates and, transitively, the later voxels around each actual
+// removal.  Every other voxel's window is unchanged at its turn in the sweep,
+// so its GPU result is the sequential one.
+//
+// Tangent seeds come from one sequential ran1(-1) stream (three draws per
+// voxel), drawn on the host; the Gram-Schmidt frame is built on the GPU.
+// Built with -fmad=false: every float/double operation rounds as on the host.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+#include <queue>
+#include <vector>
+
+#include "dsmc_b200.h"
+#include "dsmc_internal.h"
+#include "dsmc_layout.h"
+
+namespace dsmc {
+namespace {
+
+struct Dims {
+    int X, Y, Z, avg;
+};
+
+__host__ __device__ inline uint64_t lin(const Dims &d, int i, int j, int k) {
+    return ((uint64_t)((i + d.X) % d.X) * d.Y + (uint64_t)((j + d.Y) % d.Y)) * d.Z + (uint64_t)((k + d.Z) % d.Z);
+}
+
+// One voxel of calculate_normals against mask m: writes the normal and
+// returns whether the voxel is emptied.
+__host__ __device__ inline bool normal_of(const Dims &d, const uint8_t *m, int i, int j, int k, float out[3]) {
+    bool any_solid = false, all_solid = true;
+    float n0 = 0.f, n1 = 0.f, n2 = 0.f;
+    for (int di = -1; di <= 1; ++di)
+        for (int dj = -1; dj <= 1; ++dj)
+            for (int dk = -1; dk <= 1; ++dk) {
+                const int s = m[lin(d, i + di, j + dj, k + dk)];
+                if (s > 0) any_solid = true;
+                if (s == 0) all_solid = false;
+                n0 -= s * di;
+                n1 -= s * dj;
+                n2 -= s * dk;
+            }
+    const double norm_sq = n0 * n0 + n1 * n1 + n2 * n2;
+    if (norm_sq > 0) {
+        n0 = n1 = n2 = 0.f;
+        for (int di = -d.avg; di <= d.avg; ++di)
+            for (int dj = -d.avg; dj <= d.avg; ++dj)
+                for (int dk = -d.avg; dk <= d.avg; ++dk) {
+                    const int s = m[lin(d, i + di, j + dj, k + dk)];
+                    n0 -= s * di;
+                    n1 -= s * dj;
+                    n2 -= s * dk;
+                }
+    }
+    const double norm = (double)sqrtf(n0 * n0 + n1 * n1 + n2 * n2);
+    bool emptied = false;
+    if (norm > 0) {
+        n0 = (float)(n0 / norm);
+        n1 = (float)(n1 / norm);
+        n2 = (float)(n2 / norm);
+    } else if (!any_solid || !all_solid) {
+        emptied = true;
+    }
+    out[0] = n0;
+    out[1] = n1;
+    out[2] = n2;
+    return emptied;
+}
+
+__global__ void k_normals(Dims d, const uint8_t *mask, float *nrm, uint8_t *cand) {
+    const uint64_t V = (uint64_t)d.X * d.Y * d.Z;
+    for (uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; idx < V;
+         idx += (uint64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(idx % d.Z);
+        const int j = (int)((idx / d.Z) % d.Y);
+        const int i = (int)(idx / ((uint64_t)d.Y * d.Z));
+        float n[3];
+        const bool emptied = normal_of(d, mask, i, j, k, n);
+        nrm[3 * idx] = n[0];
+        nrm[3 * idx + 1] = n[1];
+        nrm[3 * idx + 2] = n[2];
+        // only a solid voxel changes when emptied
+        cand[idx] = emptied && mask[idx] != 0;
+    }
+}
+
+__global__ void k_frames(uint64_t V, const float *nrm, const float *seed, float *t1, float *t2, uint8_t *vox) {
+    for (uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; idx < V;
+         idx += (uint64_t)gridDim.x * blockDim.x) {
+        const float n0 = nrm[3 * idx], n1 = nrm[3 * idx + 1], n2 = nrm[3 * idx + 2];
+        float a0 = seed[3 * idx], a1 = seed[3 * idx + 1], a2 = seed[3 * idx + 2];
+        const double dot = n0 * a0 + n1 * a1 + n2 * a2;
+        a0 = (float)(a0 - n0 * dot);
+        a1 = (float)(a1 - n1 * dot);
+        a2 = (float)(a2 - n2 * dot);
+        double norm = (double)sqrtf(a0 * a0 + a1 * a1 + a2 * a2);
+        if (norm > 0) {
+            a0 = (float)(a0 / norm);
+            a1 = (float)(a1 / norm);
+            a2 = (float)(a2 / norm);
+        }
+        float b0 = a1 * n2 - a2 * n1;
+        float b1 = a2 * n0 - a0 * n2;
+        float b2 = a0 * n1 - a1 * n0;
+        norm = (double)sqrtf(b0 * b0 + b1 * b1 + b2 * b2);
+        if (norm > 0) {
+            b0 = (float)(b0 / norm);
+            b1 = (float)(b1 / norm);
+            b2 = (float)(b2 / norm);
+        }
+        t1[3 * idx] = a0;
+        t1[3 * idx + 1] = a1;
+        t1[3 * idx + 2] = a2;
+        t2[3 * idx] = b0;
+        t2[3 * idx + 1] = b1;
+        t2[3 * idx + 2] = b2;
+        const double nn = n0 * n0 + n1 * n1 + n2 * n2;
+        if (vox[idx] > 0 && nn > 0) vox[idx] = DSMC_VOX_BOUNDARY;
+    }
+}
+
+}  // namespace
+}  // namespace dsmc
+
+using namespace dsmc;
+
+extern "C" int dsmc_geometry_finish_gpu(int device_id, uint32_t nx, uint32_t ny, uint32_t nz, int avg, uint8_t *vox,
+                                        float *nrm, float *t1, float *t2) {
+    if (!vox || !nrm || !t1 || !t2 || nx == 0 || ny == 0 || nz == 0 || avg < 0) return DSMC_ERR_ARG;
+    if (cudaSetDevice(device_id) != cudaSuccess) {
+        set_thread_error("no CUDA device for geometry preprocessing");
+        return DSMC_ERR_NO_DEVICE;
+    }
+    const Dims d = {(int)nx, (int)ny, (int)nz, avg};
+    const uint64_t V = (uint64_t)nx * ny * nz;
+    uint8_t *dmask = nullptr, *dcand = nullptr;
+    float *dn = nullptr, *dseed = nullptr, *dt1 = nullptr, *dt2 = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(dmask);
+        cudaFree(dcand);
+        cudaFree(dn);
+        cudaFree(dseed);
+        cudaFree(dt1);
+        cudaFree(dt2);
+    };
+    auto cuda_err = [&](cudaError_t e) {
+        cleanup();
+        set_thread_error(std::string("geometry on the GPU: ") + cudaGetErrorString(e));
+        return DSMC_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&dmask, V)) || (e = cudaMalloc(&dcand, V)) || (e = cudaMalloc(&dn, 12 * V)))
+        return cuda_err(e);
+    if ((e = cudaMemcpy(dmask, vox, V, cudaMemcpyHostToDevice))) return cuda_err(e);
+    const int block = 256;
+    const int grid = (int)std::min<uint64_t>((V + block - 1) / block, 148 * 64);
+    k_normals<<<grid, block>>>(d, dmask, dn, dcand);
+    if ((e = cudaGetLastError())) return cuda_err(e);
+    std::vector<uint8_t> cand(V);
+    if ((e = cudaMemcpy(nrm, dn, 12 * V, cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(cand.data(), dcand, V, cudaMemcpyDeviceToHost)))
+        return cuda_err(e);
+    // Sequential replay of the voxels a removal can reach, in sweep order.
+    std::priority_queue<uint64_t, std::vector<uint64_t>, std::greater<uint64_t>> dirty;
+    std::vector<uint8_t> queued(V, 0);
+    for (uint64_t idx = 0; idx < V; ++idx)
+        if (cand[idx]) {
+            dirty.push(idx);
+            queued[idx] = 1;
+        }
+    const int reach = std::max(1, avg);
+    while (!dirty.empty()) {
+        const uint64_t idx = dirty.top();
+        dirty.pop();
+        const int k = (int)(idx % nz), j = (int)((idx / nz) % ny), i = (int)(idx / ((uint64_t)ny * nz));
+        float n[3];
+        const bool emptied = normal_of(d, vox, i, j, k, n);
+        nrm[3 * idx] = n[0];
+        nrm[3 * idx + 1] = n[1];
+        nrm[3 * idx + 2] = n[2];
+        if (emptied && vox[idx] != 0) {
+            vox[idx] = 0;
+            for (int di = -reach; di <= reach; ++di)
+                for (int dj = -reach; dj <= reach; ++dj)
+                    for (int dk = -reach; dk <= reach; ++dk) {
+                        const uint64_t q = lin(d, i + di, j + dj, k + dk);
+                        if (q > idx && !queued[q]) {
+                            queued[q] = 1;
+                            dirty.push(q);
+                        }
+                    }
+        }
+    }
+    // Tangent seeds: ran1(-1), three per voxel in index order.
+    std::vector<float> seed(3 * V);
+    Ran1 rnd(-1);
+    for (uint64_t q = 0; q < 3 * V; ++q) seed[q] = (float)rnd.next();
+    if ((e = cudaMalloc(&dseed, 12 * V)) || (e = cudaMalloc(&dt1, 12 * V)) || (e = cudaMalloc(&dt2, 12 * V)))
+        return cuda_err(e);
+    if ((e = cudaMemcpy(dn, nrm, 12 * V, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(dseed, seed.data(), 12 * V, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(dmask, vox, V, cudaMemcpyHostToDevice)))
+        return cuda_err(e);
+    k_frames<<<grid, block>>>(V, dn, dseed, dt1, dt2, dmask);
+    if ((e = cudaGetLastError())) return cuda_err(e);
+    if ((e = cudaMemcpy(t1, dt1, 12 * V, cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(t2, dt2, 12 * V, cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(vox, dmask, V, cudaMemcpyDeviceToHost)))
+        return cuda_err(e);
+    cleanup();
+    return DSMC_OK;
+}

@@ -1,0 +1,40 @@
+// Launchers of the DSMC kernels, one set per precision policy
+// (namespaces dsmc::split32 and dsmc::fp64).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "dsmc_layout.h"
+
+namespace dsmc {
+
+#define DSMC_DECLARE_LAUNCHERS(NS)                                                                              \
+    namespace NS {                                                                                              \
+    cudaError_t launch_pass(int mode, const PassParams &P, int grid, int block, cudaStream_t st);               \
+    int pass_blocks_per_sm(int mode, int block, int smem_cap);                                                  \
+    size_t record_bytes();                                                                                      \
+    cudaError_t launch_from_fp64(const SysDev *sys, int s, const double *r, const double *v, uint32_t id_base, \
+                                 long long n, void *A, void *B, int *key, unsigned *hist, unsigned *err,        \
+                                 cudaStream_t st);                                                              \
+    cudaError_t launch_init(const SysDev *sys, int s, double sqrt_t_over_m, long long n, void *A, void *B,     \
+                            int *key, unsigned *hist, unsigned *err, cudaStream_t st);                          \
+    cudaError_t launch_gather(const CellArrays &cells, const ParticleArrays &parts, int cur, int c0, int c1,   \
+                              unsigned nspill, void *A, void *B, int *key, unsigned *hist,                      \
+                              unsigned long long *cursor, unsigned long long limit, unsigned *err,               \
+                              cudaStream_t st);                                                                  \
+    cudaError_t launch_insert(const CellArrays &cells, const ParticleArrays &parts, int cur, long long n,      \
+                              const void *A, const void *B, const int *key, unsigned *err, cudaStream_t st);    \
+    cudaError_t launch_to_fp64(const SysDev *sys, int s, const CellArrays &cells, const ParticleArrays &parts, \
+                               int cur, uint32_t id_base, long long cap, double *r, double *v, int *cell,      \
+                               unsigned *err, cudaStream_t st);                                                 \
+    cudaError_t launch_cell_energy(const CellArrays &cells, const ParticleArrays &parts, int cur, int c0, int c1,  \
+                                   double *out, cudaStream_t st);                                               \
+    }
+
+DSMC_DECLARE_LAUNCHERS(split32)
+DSMC_DECLARE_LAUNCHERS(fp64)
+
+// Pass modes (engine.cuh PassMode).
+enum { PASS_FUSED = 0, PASS_INPLACE = 1, PASS_SORT = 2 };
+
+}  // namespace dsmc
