@@ -289,7 +289,8 @@ def main():
         "clocks": clocks,
         "device_status": {"error_bits": err, "spill": spill},
         "physics": {"temperature_K": tal.temperature, "collisions": tal.collisions,
-                    "wall_collisions": tal.wall_collisions, "reseeds": tal.reseeds},
+                    "wall_collisions": tal.wall_collisions, "reseeds": tal.reseeds,
+                    "stranded": tal.stranded},
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

@@ -146,6 +146,16 @@ int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t
 /* Same, reading s->world/0000.bin. */
 int dsmc_system_add_world(dsmc_ctx *ctx, const dsmc_settings *s, int *sys_id);
 
+/* The active cells of a voxel grid as System::setup_cells builds them
+ * (dsmc/system.cpp:432-490): numbered in order of first touch by a k-outer,
+ * i-inner voxel sweep, cells without empty voxels dropped; per cell its
+ * global index (i*cy*cz + j*cz + k), empty and total voxel counts, volume
+ * (Cell::update_volume, dsmc/cell.cpp:27-40) and NTC coefficient.  Host only.
+ * cap: capacity of the output arrays (any may be NULL); *num_cells is set. */
+int dsmc_cells_layout(const dsmc_settings *s, uint32_t nx, uint32_t ny, uint32_t nz, const uint8_t *voxels,
+                      int cap, int32_t *global_index, int32_t *pixels, int32_t *total_pixels, double *volume,
+                      double *coeff, int *num_cells);
+
 typedef struct dsmc_system_info {
     int64_t num_particles;
     int num_cells_total;
@@ -202,6 +212,7 @@ typedef struct dsmc_tallies {
     double temperature;         /* current, K (MeasureTemperature) */
     double flux;                /* F_N*count_periodic[flow]/(t - t0) (MeasureNumberFlowRate) */
     double time;                /* t, reduced */
+    uint64_t stranded;          /* moves that ended in a cell with no free volume (re-seeded next step) */
 } dsmc_tallies;
 int dsmc_tallies_get(dsmc_ctx *ctx, int sys_id, dsmc_tallies *t);
 int dsmc_tallies_reset(dsmc_ctx *ctx, int sys_id);
@@ -212,6 +223,12 @@ int dsmc_tallies_reset(dsmc_ctx *ctx, int sys_id);
 int dsmc_cells_get(dsmc_ctx *ctx, int sys_id, int cap, int32_t *global_index, int32_t *count,
                    double *vr_max, double *rest, double *moments, double *volume, int *num_cells);
 int dsmc_cells_set_state(dsmc_ctx *ctx, int sys_id, const double *vr_max, const double *rest);
+
+/* Slot capacity policy of the cell-sorted particle buffers: a cell gets
+ * ceil(factor * max(expected, present) + pad) slots (default 2.0, 24).  An
+ * overflow never loses particles: they spill to an overflow list, the
+ * pipeline stops after that step and the host re-lays the buffers out. */
+int dsmc_ctx_set_capacity(dsmc_ctx *ctx, double factor, int pad);
 
 /* Reads the status of the last pass: bit flags of device-side errors. */
 int dsmc_device_status(dsmc_ctx *ctx, uint32_t *error_bits, uint32_t *spill);

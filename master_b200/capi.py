@@ -35,7 +35,8 @@ EXPORTED = [
     "dsmc_system_add_world", "dsmc_system_info_get", "dsmc_particles_init", "dsmc_particles_set",
     "dsmc_particles_count", "dsmc_particles_get", "dsmc_step", "dsmc_stage_move", "dsmc_stage_sort",
     "dsmc_stage_collide", "dsmc_stage_sample", "dsmc_tallies_get", "dsmc_tallies_reset", "dsmc_cells_get",
-    "dsmc_cells_set_state", "dsmc_device_status", "dsmc_stream", "dsmc_counters_get",
+    "dsmc_cells_set_state", "dsmc_device_status", "dsmc_stream", "dsmc_counters_get", "dsmc_cells_layout",
+    "dsmc_ctx_set_capacity",
 ]
 
 
@@ -84,7 +85,7 @@ class Tallies(C.Structure):
     _fields_ = [("step", C.c_uint64), ("collisions", C.c_uint64), ("wall_collisions", C.c_uint64),
                 ("reseeds", C.c_uint64), ("particle_steps", C.c_uint64), ("count_periodic", C.c_int64 * 3),
                 ("samples", C.c_uint64), ("candidates", C.c_uint64), ("kinetic_energy", C.c_double),
-                ("temperature", C.c_double), ("flux", C.c_double), ("time", C.c_double)]
+                ("temperature", C.c_double), ("flux", C.c_double), ("time", C.c_double), ("stranded", C.c_uint64)]
 
 
 _lib = None
@@ -138,6 +139,9 @@ def load() -> C.CDLL:
         "dsmc_device_status": [_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)],
         "dsmc_stream": [_P],
         "dsmc_counters_get": [_P, C.c_int, C.POINTER(C.c_int64)],
+        "dsmc_ctx_set_capacity": [_P, C.c_double, C.c_int],
+        "dsmc_cells_layout": [C.POINTER(Settings), C.c_uint32, C.c_uint32, C.c_uint32, _U8, C.c_int, _I32, _I32,
+                              _I32, _D, _D, C.POINTER(C.c_int)],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)

@@ -82,10 +82,11 @@ struct dsmc_ctx {
     DevBuf<Status> status;
     // cells (all systems)
     int num_cells = 0;
-    DevBuf<int> cell_sys, cell_global;
-    DevBuf<unsigned> cell_base, cell_cap, count0, count1, key;
-    DevBuf<double> vr_max, rest, coeff, mom;
-    std::vector<unsigned> h_base, h_cap;
+    DevBuf<int4> meta;
+    DevBuf<double4> state;
+    DevBuf<unsigned> count0, count1, key;
+    DevBuf<double> mom;
+    std::vector<int4> h_meta;   // {base, cap, global, sys}
     size_t slots = 0;
     int smem_cap = 32;
     // particles
@@ -105,6 +106,10 @@ struct dsmc_ctx {
     // launch shape of the cell pass
     int block = 256;
     int grid = 0;
+    int fused_grid = 0;     // pipelined split-precision pass; 0 = not usable
+    bool use_pipelined = true;
+    double cap_factor = 2.0;
+    int cap_pad = 24;
 
     size_t rec_half() const { return precision == DSMC_PREC_FP64 ? 32 : 16; }
 };
@@ -132,15 +137,10 @@ bool is_fp64(const dsmc_ctx *ctx) { return ctx->precision == DSMC_PREC_FP64; }
 CellArrays cell_arrays(dsmc_ctx *ctx) {
     CellArrays c;
     c.num_cells = ctx->num_cells;
-    c.sys = ctx->cell_sys.p;
-    c.global = ctx->cell_global.p;
-    c.base = ctx->cell_base.p;
-    c.cap = ctx->cell_cap.p;
+    c.meta = ctx->meta.p;
+    c.state = ctx->state.p;
     c.count[0] = ctx->count0.p;
     c.count[1] = ctx->count1.p;
-    c.vr_max = ctx->vr_max.p;
-    c.rest = ctx->rest.p;
-    c.coeff = ctx->coeff.p;
     c.mom = ctx->mom.p;
     c.key = ctx->key.p;
     return c;
@@ -184,8 +184,6 @@ int relayout(dsmc_ctx *ctx, long long total) {
     // Capacity per cell: twice the larger of the expected and the present
     // occupancy plus 24 slots, a multiple of 4 (Poisson tails beyond it are
     // below 1e-12 per cell and step; an overflow spills and the host repacks).
-    ctx->h_base.assign(C, 0);
-    ctx->h_cap.assign(C, 0);
     size_t slots = 0;
     unsigned maxcap = 4;
     for (auto &sp : ctx->systems) {
@@ -196,15 +194,15 @@ int relayout(dsmc_ctx *ctx, long long total) {
         for (int a = s.active_begin; a < s.active_end; ++a) {
             const double expect = total_pixels > 0 ? nsys * s.pixels[a - s.active_begin] / total_pixels : 0;
             const double want = std::max(expect, (double)counts[a]);
-            unsigned cap = (unsigned)std::ceil(2.0 * want + 24.0);
-            cap = (cap + 3u) & ~3u;
-            ctx->h_base[a] = (unsigned)slots;
-            ctx->h_cap[a] = cap;
+            unsigned cap = (unsigned)std::ceil(ctx->cap_factor * want + ctx->cap_pad);
+            if (cap < 1) cap = 1;
+            ctx->h_meta[a].x = (int)slots;
+            ctx->h_meta[a].y = (int)cap;
             slots += cap;
             maxcap = std::max(maxcap, cap);
         }
     }
-    if (slots >= (size_t)0xffffffffu) return fail(ctx, DSMC_ERR_CAPACITY, "more than 2^32 particle slots");
+    if (slots >= (size_t)0x7fffffffu) return fail(ctx, DSMC_ERR_CAPACITY, "more than 2^31 particle slots");
     if (maxcap > 4096) return fail(ctx, DSMC_ERR_CAPACITY, "a cell needs more than 4096 slots");
     ctx->smem_cap = (int)((maxcap + 31u) & ~31u);
     ctx->slots = slots;
@@ -214,11 +212,9 @@ int relayout(dsmc_ctx *ctx, long long total) {
     CK(ctx->B0.ensure(slots * half));
     CK(ctx->B1.ensure(slots * half));
     CK(ctx->key.ensure(slots));
-    CK(ctx->cell_base.ensure(C));
-    CK(ctx->cell_cap.ensure(C));
+    CK(ctx->meta.ensure(std::max(C, 1)));
     if (C) {
-        CK(cudaMemcpyAsync(ctx->cell_base.p, ctx->h_base.data(), C * sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemcpyAsync(ctx->cell_cap.p, ctx->h_cap.data(), C * sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->meta.p, ctx->h_meta.data(), C * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaMemsetAsync(ctx->count0.p, 0, C * sizeof(unsigned), ctx->stream));
         CK(cudaMemsetAsync(ctx->count1.p, 0, C * sizeof(unsigned), ctx->stream));
     }
@@ -243,6 +239,11 @@ int relayout(dsmc_ctx *ctx, long long total) {
     is_fp64(ctx) ? fp64::pass_blocks_per_sm(PASS_SORT, ctx->block, ctx->smem_cap)
                  : split32::pass_blocks_per_sm(PASS_SORT, ctx->block, ctx->smem_cap);
     ctx->grid = bps * ctx->num_sms;
+    ctx->fused_grid = 0;
+    if (!is_fp64(ctx) && split32::fused_capacity(ctx->smem_cap) > 0) {
+        const int fb = split32::fused_blocks_per_sm(ctx->smem_cap);
+        ctx->fused_grid = fb * ctx->num_sms;
+    }
     Status st;
     cudaError_t e;
     st = read_status(ctx, &e);
@@ -309,8 +310,12 @@ int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, 
     P.do_sample = do_sample;
     P.smem_cap = ctx->smem_cap;
     P.advance_step = advance;
-    cudaError_t e = is_fp64(ctx) ? fp64::launch_pass(mode, P, ctx->grid, ctx->block, ctx->stream)
-                                 : split32::launch_pass(mode, P, ctx->grid, ctx->block, ctx->stream);
+    cudaError_t e;
+    if (mode == PASS_FUSED && ctx->use_pipelined && ctx->fused_grid > 0)
+        e = split32::launch_fused(P, ctx->fused_grid, ctx->stream);
+    else
+        e = is_fp64(ctx) ? fp64::launch_pass(mode, P, ctx->grid, ctx->block, ctx->stream)
+                         : split32::launch_pass(mode, P, ctx->grid, ctx->block, ctx->stream);
     CK(e);
     return DSMC_OK;
 }
@@ -350,11 +355,11 @@ int rebuild_cells(dsmc_ctx *ctx) {
     // Keep the cell state and tallies of the systems already present: a new
     // system's cells are appended after theirs.
     const int C_old = ctx->num_cells;
-    std::vector<double> old_vr(C_old), old_rest(C_old), old_mom(8 * (size_t)C_old);
+    std::vector<double4> old_state(C_old);
+    std::vector<double> old_mom(8 * (size_t)C_old);
     std::vector<SysTally> old_tally(ctx->systems.size() > 0 ? ctx->systems.size() - 1 : 0);
     if (C_old > 0) {
-        CK(cudaMemcpyAsync(old_vr.data(), ctx->vr_max.p, C_old * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(old_rest.data(), ctx->rest.p, C_old * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(old_state.data(), ctx->state.p, C_old * sizeof(double4), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaMemcpyAsync(old_mom.data(), ctx->mom.p, 8 * C_old * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     }
     if (!old_tally.empty())
@@ -364,17 +369,17 @@ int rebuild_cells(dsmc_ctx *ctx) {
     // Concatenate the active cells of all systems.
     int C = 0;
     for (auto &s : ctx->systems) C += (int)s->cell_global.size();
-    std::vector<int> sys(C), glob(C);
-    std::vector<double> vr(C), rest(C, 0.0), coeff(C);
+    ctx->h_meta.assign(C, int4{0, 0, 0, 0});
+    std::vector<double4> state(C);
     int a = 0;
     for (size_t si = 0; si < ctx->systems.size(); ++si) {
         SysHost &s = *ctx->systems[si];
         s.active_begin = a;
         for (size_t c = 0; c < s.cell_global.size(); ++c, ++a) {
-            sys[a] = (int)si;
-            glob[a] = s.cell_global[c];
-            vr[a] = s.vr_max0;
-            coeff[a] = s.coeff[c];
+            ctx->h_meta[a].z = s.cell_global[c];
+            ctx->h_meta[a].w = (int)si;
+            // Cell::vr_max starts at 3*sqrt(T) (dsmc/system.cpp:451,477)
+            state[a] = double4{s.vr_max0, 0.0, s.coeff[c], 0.0};
         }
         s.active_end = a;
         s.dev.active_begin = s.active_begin;
@@ -389,29 +394,21 @@ int rebuild_cells(dsmc_ctx *ctx) {
     }
     ctx->num_cells = C;
     const size_t Cn = std::max(C, 1);
-    CK(ctx->cell_sys.alloc(Cn));
-    CK(ctx->cell_global.alloc(Cn));
+    CK(ctx->meta.alloc(Cn));
+    CK(ctx->state.alloc(Cn));
     CK(ctx->count0.alloc(Cn));
     CK(ctx->count1.alloc(Cn));
-    CK(ctx->vr_max.alloc(Cn));
-    CK(ctx->rest.alloc(Cn));
-    CK(ctx->coeff.alloc(Cn));
     CK(ctx->mom.alloc(8 * Cn));
     CK(ctx->hist.alloc(Cn));
     if (C) {
-        CK(cudaMemcpyAsync(ctx->cell_sys.p, sys.data(), C * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemcpyAsync(ctx->cell_global.p, glob.data(), C * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemcpyAsync(ctx->vr_max.p, vr.data(), C * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemcpyAsync(ctx->rest.p, rest.data(), C * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemcpyAsync(ctx->coeff.p, coeff.data(), C * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        if (C_old > 0 && C_old <= C)
+            for (int q = 0; q < C_old; ++q) state[q] = old_state[q];
+        CK(cudaMemcpyAsync(ctx->state.p, state.data(), C * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaMemsetAsync(ctx->mom.p, 0, 8 * C * sizeof(double), ctx->stream));
         CK(cudaMemsetAsync(ctx->count0.p, 0, C * sizeof(unsigned), ctx->stream));
         CK(cudaMemsetAsync(ctx->count1.p, 0, C * sizeof(unsigned), ctx->stream));
-        if (C_old > 0 && C_old <= C) {
-            CK(cudaMemcpyAsync(ctx->vr_max.p, old_vr.data(), C_old * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-            CK(cudaMemcpyAsync(ctx->rest.p, old_rest.data(), C_old * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        if (C_old > 0 && C_old <= C)
             CK(cudaMemcpyAsync(ctx->mom.p, old_mom.data(), 8 * C_old * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-        }
     }
     CK(ctx->tally.alloc(std::max<size_t>(ctx->systems.size(), 1)));
     CK(cudaMemsetAsync(ctx->tally.p, 0, std::max<size_t>(ctx->systems.size(), 1) * sizeof(SysTally), ctx->stream));
@@ -517,43 +514,20 @@ int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t
     volume = volume / 1 * h->porosity;
     h->volume = volume;
     h->expected = (int64_t)(density * volume / h->atoms_per_molecule);
-    // System::setup_cells (dsmc/system.cpp:432-490): cells numbered in order
-    // of first touch by a k-outer, i-inner voxel sweep; cells with no empty
-    // voxel are dropped.
-    const int cx = s->cells_x, cy = s->cells_y, cz = s->cells_z;
-    const int ncells = cx * cy * cz;
-    std::vector<int> first(ncells, -1), tot, pix, order;
-    for (uint32_t k = 0; k < nz; ++k) {
-        const int c_z = (int)((float)k / nz * cz);
-        for (uint32_t j = 0; j < ny; ++j) {
-            const int c_y = (int)((float)j / ny * cy);
-            for (uint32_t i = 0; i < nx; ++i) {
-                const int c_x = (int)((float)i / nx * cx);
-                const int ci = c_x * cy * cz + c_y * cz + c_z;
-                if (first[ci] < 0) {
-                    first[ci] = (int)order.size();
-                    order.push_back(ci);
-                    tot.push_back(0);
-                    pix.push_back(0);
-                }
-                tot[first[ci]]++;
-                pix[first[ci]] += voxels[((uint64_t)i * ny + j) * nz + k] < DSMC_VOX_WALL;
-            }
-        }
-    }
-    h->cell_map.assign(ncells, -1);
-    const double system_volume = L[0] * L[1] * L[2];
-    for (size_t c = 0; c < order.size(); ++c) {
-        if (pix[c] == 0) continue;
-        // Cell::update_volume (dsmc/cell.cpp:27-40)
-        const double vol = system_volume / (ncells) * (float)pix[c] / tot[c];
-        const double coeff = 0.5 * h->atoms_per_molecule * M_PI * s->diam * s->diam * s->dt / vol;
-        h->cell_map[order[c]] = (int)h->cell_global.size();
-        h->cell_global.push_back(order[c]);
-        h->pixels.push_back(pix[c]);
-        h->total_pixels.push_back(tot[c]);
-        h->volume_cell.push_back(vol);
-        h->coeff.push_back(coeff);
+    {
+        int nc = 0;
+        int rc2 = dsmc_cells_layout(s, nx, ny, nz, voxels, 0, nullptr, nullptr, nullptr, nullptr, nullptr, &nc);
+        if (rc2) return fail(ctx, rc2, thread_error());
+        h->cell_global.resize(nc);
+        h->pixels.resize(nc);
+        h->total_pixels.resize(nc);
+        h->volume_cell.resize(nc);
+        h->coeff.resize(nc);
+        rc2 = dsmc_cells_layout(s, nx, ny, nz, voxels, nc, h->cell_global.data(), h->pixels.data(),
+                                h->total_pixels.data(), h->volume_cell.data(), h->coeff.data(), &nc);
+        if (rc2) return fail(ctx, rc2, thread_error());
+        h->cell_map.assign(s->cells_x * s->cells_y * s->cells_z, -1);
+        for (int c = 0; c < nc; ++c) h->cell_map[h->cell_global[c]] = c;
     }
     // Device geometry.
     CK(h->vox.alloc(V));
@@ -614,6 +588,55 @@ int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t
         CK(cudaMemcpyAsync(ctx->hist.p, hc.data(), hc.size() * sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
     }
     return relayout(ctx, staged);
+}
+
+int dsmc_cells_layout(const dsmc_settings *s, uint32_t nx, uint32_t ny, uint32_t nz, const uint8_t *voxels, int cap,
+                      int32_t *global_index, int32_t *pixels, int32_t *total_pixels, double *volume, double *coeff,
+                      int *num_cells) {
+    if (!s || !voxels || !num_cells || nx == 0 || ny == 0 || nz == 0) return DSMC_ERR_ARG;
+    const int cx = s->cells_x, cy = s->cells_y, cz = s->cells_z;
+    if (cx <= 0 || cy <= 0 || cz <= 0) return fail(nullptr, DSMC_ERR_CONFIG, "cells must be > 0");
+    // System::setup_cells (dsmc/system.cpp:432-490): cells numbered in order of
+    // first touch by a k-outer, i-inner voxel sweep; cells with no empty voxel
+    // are dropped.
+    const int ncells = cx * cy * cz;
+    std::vector<int> first(ncells, -1), tot, pix, order;
+    for (uint32_t k = 0; k < nz; ++k) {
+        const int c_z = (int)((float)k / nz * cz);
+        for (uint32_t j = 0; j < ny; ++j) {
+            const int c_y = (int)((float)j / ny * cy);
+            for (uint32_t i = 0; i < nx; ++i) {
+                const int c_x = (int)((float)i / nx * cx);
+                const int ci = c_x * cy * cz + c_y * cz + c_z;
+                if (first[ci] < 0) {
+                    first[ci] = (int)order.size();
+                    order.push_back(ci);
+                    tot.push_back(0);
+                    pix.push_back(0);
+                }
+                tot[first[ci]]++;
+                pix[first[ci]] += voxels[((uint64_t)i * ny + j) * nz + k] < DSMC_VOX_WALL;
+            }
+        }
+    }
+    const double system_volume = s->Lx * s->Ly * s->Lz;
+    const double apm = s->atoms_per_molecule;
+    int n = 0;
+    for (size_t c = 0; c < order.size(); ++c) {
+        if (pix[c] == 0) continue;
+        if (n < cap) {
+            // Cell::update_volume (dsmc/cell.cpp:27-40)
+            const double vol = system_volume / (ncells) * (float)pix[c] / tot[c];
+            if (global_index) global_index[n] = order[c];
+            if (pixels) pixels[n] = pix[c];
+            if (total_pixels) total_pixels[n] = tot[c];
+            if (volume) volume[n] = vol;
+            if (coeff) coeff[n] = 0.5 * apm * M_PI * s->diam * s->diam * s->dt / vol;
+        }
+        ++n;
+    }
+    *num_cells = n;
+    return DSMC_OK;
 }
 
 int dsmc_system_add_world(dsmc_ctx *ctx, const dsmc_settings *s, int *sys_id) {
@@ -844,6 +867,7 @@ int dsmc_tallies_get(dsmc_ctx *ctx, int sys_id, dsmc_tallies *t) {
     for (int a = 0; a < 3; ++a) t->count_periodic[a] = T.count_periodic[a];
     t->samples = T.samples;
     t->candidates = T.candidates;
+    t->stranded = T.stranded;
     t->time = st.step * h.settings.dt;
     // MeasureEnergy / MeasureTemperature (dsmc/statisticalproperty.cpp:21-71)
     // from the current velocities, summed per cell and then in cell order.
@@ -906,12 +930,17 @@ int dsmc_cells_get(dsmc_ctx *ctx, int sys_id, int cap, int32_t *global_index, in
         unsigned *cp = ctx->cur ? ctx->count1.p : ctx->count0.p;
         CK(cudaMemcpyAsync(count, cp + a0, C * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     }
-    if (vr_max) CK(cudaMemcpyAsync(vr_max, ctx->vr_max.p + a0, C * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    if (rest) CK(cudaMemcpyAsync(rest, ctx->rest.p + a0, C * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<double4> st(C);
+    if (vr_max || rest)
+        CK(cudaMemcpyAsync(st.data(), ctx->state.p + a0, C * sizeof(double4), cudaMemcpyDeviceToHost, ctx->stream));
     if (moments)
         CK(cudaMemcpyAsync(moments, ctx->mom.p + 8 * (size_t)a0, 8 * (size_t)C * sizeof(double), cudaMemcpyDeviceToHost,
                            ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    for (int q = 0; q < C; ++q) {
+        if (vr_max) vr_max[q] = st[q].x;
+        if (rest) rest[q] = st[q].y;
+    }
     return DSMC_OK;
 }
 
@@ -923,13 +952,26 @@ int dsmc_cells_set_state(dsmc_ctx *ctx, int sys_id, const double *vr_max, const 
     SysHost &h = *ctx->systems[sys_id];
     const int C = h.active_end - h.active_begin;
     if (C == 0) return DSMC_OK;
-    if (vr_max) CK(cudaMemcpyAsync(ctx->vr_max.p + h.active_begin, vr_max, C * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    if (rest) CK(cudaMemcpyAsync(ctx->rest.p + h.active_begin, rest, C * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<double4> st(C);
+    CK(cudaMemcpyAsync(st.data(), ctx->state.p + h.active_begin, C * sizeof(double4), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (int q = 0; q < C; ++q) {
+        if (vr_max) st[q].x = vr_max[q];
+        if (rest) st[q].y = rest[q];
+    }
+    CK(cudaMemcpyAsync(ctx->state.p + h.active_begin, st.data(), C * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return DSMC_OK;
 }
 
 void *dsmc_stream(dsmc_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int dsmc_ctx_set_capacity(dsmc_ctx *ctx, double factor, int pad) {
+    if (!ctx || !(factor >= 1.0) || pad < 0) return DSMC_ERR_ARG;
+    ctx->cap_factor = factor;
+    ctx->cap_pad = pad;
+    return DSMC_OK;
+}
 
 int dsmc_counters_get(dsmc_ctx *ctx, int sys_id, int64_t out[8]) {
     if (!ctx || !out || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;

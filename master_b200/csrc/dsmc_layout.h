@@ -35,8 +35,13 @@
 #define DSMC_EBIT_SPILL_FULL 8u  // the overflow list itself overflowed
 #define DSMC_EBIT_SMEM 16u       // a cell held more particles than the staging buffer
 #define DSMC_EBIT_NAN 32u        // non-finite position or velocity
-// bits that stop the pipeline (a failed facet search re-seeds the particle and goes on)
-#define DSMC_EBIT_FATAL (DSMC_EBIT_CELL | DSMC_EBIT_RESEED | DSMC_EBIT_SPILL_FULL | DSMC_EBIT_SMEM | DSMC_EBIT_NAN)
+#define DSMC_EBIT_TIMEOUT 128u   // a bounded wait on a bulk copy ran out
+#define DSMC_EBIT_STRANDED 64u   // a move ended inside solid whose cell has no free volume; the
+                                 // particle stays in its previous cell and is re-seeded next step
+// bits that stop the pipeline (a failed facet search or a stranded particle is
+// re-seeded, counted, and the pipeline goes on)
+#define DSMC_EBIT_FATAL \
+    (DSMC_EBIT_CELL | DSMC_EBIT_RESEED | DSMC_EBIT_SPILL_FULL | DSMC_EBIT_SMEM | DSMC_EBIT_NAN | DSMC_EBIT_TIMEOUT)
 
 #define DSMC_VOX_PACK(i, j, k) ((uint32_t)(i) | ((uint32_t)(j) << 11) | ((uint32_t)(k) << 22))
 #define DSMC_VOX_I(p) ((int)((p)&0x7FFu))
@@ -83,6 +88,7 @@ struct SysTally {
     long long count_periodic[3];   // net boundary crossings (dsmc/moleculemover.h:29-38)
     unsigned long long samples;    // sampled steps folded into the cell moments
     unsigned long long candidates;
+    unsigned long long stranded;   // moves that ended inside solid cells (see DSMC_EBIT_STRANDED)
 };
 
 struct Status {
@@ -105,14 +111,13 @@ struct SpillRec {
 
 struct CellArrays {
     int num_cells;             // total active cells over all systems
-    const int *sys;            // system of each active cell
-    const int *global;         // the reference's cell index (dsmc/system.h:130-132)
-    const unsigned *base;      // first slot
-    const unsigned *cap;       // slots
+    const int4 *meta;          // {first slot, slots, the reference's cell index
+                               //  (dsmc/system.h:130-132), system}, fixed between relayouts
+    double4 *state;            // {vr_max, selection remainder, coefficient, 0} in fp64:
+                               //  (sigma*c_r)_max bookkeeping and NTC remainder
+                               //  (dsmc/cell.cpp:42-111), 0.5 F_N pi d^2 dt / V_cell
+                               //  (dsmc/cell.cpp:27-40)
     unsigned *count[2];        // occupancy per buffer
-    double *vr_max;            // (sigma*c_r)_max bookkeeping, fp64 (dsmc/cell.cpp:75-111)
-    double *rest;              // selection remainder (dsmc/cell.cpp:42-51)
-    const double *coeff;       // 0.5 F_N pi d^2 dt / V_cell (dsmc/cell.cpp:27-40)
     double *mom;               // 8 fp64 per cell: n, sum v (3), sum v^2 (3), sum |v|^2
     unsigned *key;             // per slot: new active cell after a stand-alone move stage
 };

@@ -58,18 +58,23 @@ struct Split32 {
     typedef uint4 RecA;
     typedef float4 RecB;
 
+    // flag: the particle's voxel is not empty (kept in the sign bit of ox,
+    // which is otherwise always clear), so the move needs no lookup to know
+    // the start voxel's type.
     struct Particle {
         int c[3];
         float o[3];
         float v[3];
         uint32_t id;
+        uint32_t flag;
     };
 
     static __device__ __forceinline__ void unpack(const uint4 &a, const float4 &b, Particle &p) {
         p.c[0] = DSMC_VOX_I(a.x);
         p.c[1] = DSMC_VOX_J(a.x);
         p.c[2] = DSMC_VOX_K(a.x);
-        p.o[0] = __uint_as_float(a.y);
+        p.flag = a.y >> 31;
+        p.o[0] = __uint_as_float(a.y & 0x7fffffffu);
         p.o[1] = __uint_as_float(a.z);
         p.o[2] = __uint_as_float(a.w);
         p.v[0] = b.x;
@@ -79,7 +84,7 @@ struct Split32 {
     }
     static __device__ __forceinline__ void pack(const Particle &p, uint4 &a, float4 &b) {
         a.x = DSMC_VOX_PACK(p.c[0], p.c[1], p.c[2]);
-        a.y = __float_as_uint(p.o[0]);
+        a.y = __float_as_uint(p.o[0]) | (p.flag << 31);
         a.z = __float_as_uint(p.o[1]);
         a.w = __float_as_uint(p.o[2]);
         b.x = p.v[0];
@@ -188,15 +193,17 @@ struct Split32 {
     // that subtraction drifts by an ulp, which is more than the 1e-7 time
     // units the reference leaves before a face for slow particles, so the
     // sub-step's start position is kept and restored instead.
-    static __device__ void move(const SysDev &g, Particle &p, uint32_t step, MoveTally &t) {
+    static __device__ __noinline__ void move_general(const SysDev &g, Particle &p, uint32_t step, MoveTally &t) {
         DrawStream rs;
         rs.init(g.seed, p.id, step, DSMC_TAG_MOVE);
         float w[3] = {p.v[0] * g.inv_vox_f[0], p.v[1] * g.inv_vox_f[1], p.v[2] * g.inv_vox_f[2]};
         float dt = g.dt_f;
+        int here = p.flag ? DSMC_VOX_WALL : DSMC_VOX_EMPTY;  // (non-)emptiness of the current voxel
         for (int depth = 0;; ++depth) {
-            if (voxel_type(g, p.c[0], p.c[1], p.c[2]) != DSMC_VOX_EMPTY) {
+            if (here != DSMC_VOX_EMPTY) {
                 ++t.reseeds;
                 if (!reseed(g, p, rs)) t.err |= DSMC_EBIT_RESEED;
+                here = DSMC_VOX_EMPTY;
                 break;
             }
             const int c0[3] = {p.c[0], p.c[1], p.c[2]};
@@ -267,17 +274,23 @@ struct Split32 {
                 // fp32 offsets can round onto the face the fp64 reference stops
                 // 1e-7 time units short of; put the particle back outside.
                 if (outside && tau > 0.0f && p.c[0] == cb[0] && p.c[1] == cb[1] && p.c[2] == cb[2]) {
-                    if (side == 0) {
-                        p.c[axis] = cb[axis] - 1;
-                        p.o[axis] = one_minus_ulp();
+                    const int out = side == 0 ? cb[axis] - 1 : cb[axis] + 1;
+                    const float oo = side == 0 ? one_minus_ulp() : 0.0f;
+                    if (axis == 0) {
+                        p.c[0] = out;
+                        p.o[0] = oo;
+                    } else if (axis == 1) {
+                        p.c[1] = out;
+                        p.o[1] = oo;
                     } else {
-                        p.c[axis] = cb[axis] + 1;
-                        p.o[axis] = 0.0f;
+                        p.c[2] = out;
+                        p.o[2] = oo;
                     }
                 }
                 vt = voxel_type(g, p.c[0], p.c[1], p.c[2]);
             }
             if (stop) break;
+            here = vt;
             dt -= tau;
             reflect(g, voxel_linear(g, cb[0], cb[1], cb[2]), p.v, rs);
             ++t.wall_hits;
@@ -285,6 +298,7 @@ struct Split32 {
             for (int d = 0; d < 3; ++d) w[d] = p.v[d] * g.inv_vox_f[d];
             if (!(dt > 1e-5f && depth < 10)) break;
         }
+        p.flag = here != DSMC_VOX_EMPTY;
         // Periodic wrap, one box length at most, counting net crossings.
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
@@ -301,6 +315,31 @@ struct Split32 {
                 p.o[d] = 0.5f;
             }
         }
+    }
+
+    // The whole move.  A particle whose full-dt flight stays inside its
+    // (empty) voxel needs no lookup at all: that is the reference's outcome
+    // too (r += v*dt lands in an empty voxel, dt = 0; dsmc/moleculemover.cpp:
+    // 74-77,122).  Everything else takes the general path.
+    // Returns true when the particle left its voxel.
+    static __device__ __forceinline__ bool move(const SysDev &g, Particle &p, uint32_t step, MoveTally &t) {
+        if (!p.flag) {
+            float x[3];
+            bool stay = true;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                x[d] = fmaf(p.v[d] * g.inv_vox_f[d], g.dt_f, p.o[d]);
+                stay &= (x[d] >= 0.0f) & (x[d] < 1.0f);
+            }
+            if (stay) {
+                p.o[0] = x[0];
+                p.o[1] = x[1];
+                p.o[2] = x[2];
+                return false;
+            }
+        }
+        move_general(g, p, step, t);
+        return true;
     }
 
     // Cell of the particle: whole voxels per cell, so cell = voxel / vpc.
@@ -479,7 +518,7 @@ struct Fp64 {
         }
     }
 
-    static __device__ void move(const SysDev &g, Particle &p, uint32_t step, MoveTally &t) {
+    static __device__ bool move(const SysDev &g, Particle &p, uint32_t step, MoveTally &t) {
         DrawStream rs;
         rs.init(g.seed, p.id, step, DSMC_TAG_MOVE);
         double dt = g.dt;
@@ -559,6 +598,7 @@ struct Fp64 {
             }
             if (!isfinite(p.r[d]) || !isfinite(p.v[d])) t.err |= DSMC_EBIT_NAN;
         }
+        return true;
     }
 
     // System::cell_index_from_position (dsmc/system.h:122-132).
@@ -598,56 +638,140 @@ template <class Prec> struct WarpStage {
     }
 };
 
-// Cell::prepare + Cell::collide + Cell::collide_molecules (dsmc/cell.cpp:42-111)
-// on one cell staged in shared memory, members in id order.  Run by one lane.
-template <class Prec>
-__device__ void ntc_collide(const SysDev &g, int cell_global_index, uint32_t step, int n, double coeff,
-                            double &vr_max, double &rest, WarpStage<Prec> &st, unsigned long long &collisions,
-                            unsigned long long &candidates) {
-    typedef typename Prec::real real;
-    const double select = coeff * n * (n - 1) * vr_max + rest;
+// ---- NTC arithmetic shared by every collide path ----------------------------
+// Rounding is spelled out (no contraction) so that the fused pass and the
+// stand-alone collide stage produce bit-identical velocities, and the fp64
+// bookkeeping rounds as the reference's does.
+
+// Cell::prepare (dsmc/cell.cpp:42-51): pairs = round(coeff N (N-1) vr_max + rest).
+__device__ __forceinline__ int ntc_select(double coeff, int n, double vr_max, double &rest) {
+    const double select = __dadd_rn(__dmul_rn(__dmul_rn(__dmul_rn(coeff, (double)n), (double)(n - 1)), vr_max), rest);
     const int pairs = (int)round(select);
-    rest = select - pairs;
-    if (n < 2) return;
+    rest = __dsub_rn(select, (double)pairs);
+    return pairs;
+}
+
+// candidate pair (dsmc/cell.cpp:80-82): ip0 = int(U N), ip1 = int(ip0 + 1 + U (N-1)) % N
+__device__ __forceinline__ void ntc_pick(float ua, float ub, int n, int &ip0, int &ip1) {
+    ip0 = min((int)__fmul_rn(ua, (float)n), n - 1);
+    ip1 = ((int)__fadd_rn((float)(ip0 + 1), __fmul_rn(ub, (float)(n - 1)))) % n;
+}
+__device__ __forceinline__ void ntc_pick(double ua, double ub, int n, int &ip0, int &ip1) {
+    ip0 = min((int)__dmul_rn(ua, (double)n), n - 1);
+    ip1 = ((int)__dadd_rn((double)(ip0 + 1), __dmul_rn(ub, (double)(n - 1)))) % n;
+}
+
+__device__ __forceinline__ float rel_speed(float dx, float dy, float dz) {
+    return __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
+}
+__device__ __forceinline__ double rel_speed(double dx, double dy, double dz) {
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+}
+
+// Cell::collide_molecules (dsmc/cell.cpp:53-73): isotropic post-collision
+// relative velocity about the centre of mass.
+__device__ __forceinline__ void ntc_scatter(float &ax, float &ay, float &az, float &bx, float &by, float &bz,
+                                            float vrel, float u_cos, float u_phi) {
+    const float cmx = __fmul_rn(0.5f, __fadd_rn(ax, bx));
+    const float cmy = __fmul_rn(0.5f, __fadd_rn(ay, by));
+    const float cmz = __fmul_rn(0.5f, __fadd_rn(az, bz));
+    const float cos_th = __fsub_rn(1.0f, __fmul_rn(2.0f, u_cos));
+    const float sin_th = __fsqrt_rn(__fsub_rn(1.0f, __fmul_rn(cos_th, cos_th)));
+    const float phi = __fmul_rn(6.2831853071795864769f, u_phi);
+    float sp, cp;
+    sincosf(phi, &sp, &cp);
+    const float rx = __fmul_rn(vrel, cos_th);
+    const float ry = __fmul_rn(__fmul_rn(vrel, sin_th), cp);
+    const float rz = __fmul_rn(__fmul_rn(vrel, sin_th), sp);
+    ax = __fadd_rn(cmx, __fmul_rn(0.5f, rx));
+    ay = __fadd_rn(cmy, __fmul_rn(0.5f, ry));
+    az = __fadd_rn(cmz, __fmul_rn(0.5f, rz));
+    bx = __fsub_rn(cmx, __fmul_rn(0.5f, rx));
+    by = __fsub_rn(cmy, __fmul_rn(0.5f, ry));
+    bz = __fsub_rn(cmz, __fmul_rn(0.5f, rz));
+}
+__device__ __forceinline__ void ntc_scatter(double &ax, double &ay, double &az, double &bx, double &by, double &bz,
+                                            double vrel, double u_cos, double u_phi) {
+    const double cmx = 0.5 * (ax + bx), cmy = 0.5 * (ay + by), cmz = 0.5 * (az + bz);
+    const double cos_th = 1.0 - 2.0 * u_cos;
+    const double sin_th = sqrt(1.0 - cos_th * cos_th);
+    const double phi = 2 * 3.14159265358979323846 * u_phi;
+    const double rx = vrel * cos_th;
+    const double ry = vrel * sin_th * cos(phi);
+    const double rz = vrel * sin_th * sin(phi);
+    ax = cmx + 0.5 * rx;
+    ay = cmy + 0.5 * ry;
+    az = cmz + 0.5 * rz;
+    bx = cmx - 0.5 * rx;
+    by = cmy - 0.5 * ry;
+    bz = cmz - 0.5 * rz;
+}
+
+// Cell::collide (dsmc/cell.cpp:75-111) over the members in id order, on
+// velocities staged in shared memory.  Run by one lane.  Draws: stream
+// (cell, step, collide), three per candidate and two more per collision.
+template <class real, class Vel>
+__device__ void ntc_run(uint64_t seed, int cell_global_index, uint32_t step, int n, int pairs, double &vr_max,
+                        Vel vel, const uint16_t *perm, unsigned long long &collisions) {
     DrawStream rs;
-    rs.init(g.seed, (uint32_t)cell_global_index, step, DSMC_TAG_COLLIDE);
+    rs.init(seed, (uint32_t)cell_global_index, step, DSMC_TAG_COLLIDE);
     double crm = vr_max;
     const real vmax = (real)vr_max;
     for (int isel = 0; isel < pairs; ++isel) {
         const real ua = rs.template uniform<real>();
-        int ip0 = min((int)(ua * (real)n), n - 1);
         const real ub = rs.template uniform<real>();
-        const int ip1 = ((int)((real)(ip0 + 1) + ub * (real)(n - 1))) % n;
-        const int s0 = st.perm[ip0], s1 = st.perm[ip1];
-        const real dx = st.vx[s0] - st.vx[s1], dy = st.vy[s0] - st.vy[s1], dz = st.vz[s0] - st.vz[s1];
-        const real vrel = sqrt(dx * dx + dy * dy + dz * dz);
+        int ip0, ip1;
+        ntc_pick(ua, ub, n, ip0, ip1);
+        const int s0 = perm[ip0], s1 = perm[ip1];
+        real ax, ay, az, bx, by, bz;
+        vel.get(s0, ax, ay, az);
+        vel.get(s1, bx, by, bz);
+        const real vrel = rel_speed(ax - bx, ay - by, az - bz);
         if ((double)vrel > crm) crm = (double)vrel;
         const real uc = rs.template uniform<real>();
         if (vrel > uc * vmax) {
             ++collisions;
-            const real cmx = (real)0.5 * (st.vx[s0] + st.vx[s1]);
-            const real cmy = (real)0.5 * (st.vy[s0] + st.vy[s1]);
-            const real cmz = (real)0.5 * (st.vz[s0] + st.vz[s1]);
-            const real cos_th = (real)1.0 - (real)2.0 * rs.template uniform<real>();
-            const real sin_th = sqrt((real)1.0 - cos_th * cos_th);
-            const real phi = (real)(2 * 3.14159265358979323846) * rs.template uniform<real>();
-            const real rx = vrel * cos_th;
-            const real ry = vrel * sin_th * cos(phi);
-            const real rz = vrel * sin_th * sin(phi);
-            st.vx[s0] = cmx + (real)0.5 * rx;
-            st.vy[s0] = cmy + (real)0.5 * ry;
-            st.vz[s0] = cmz + (real)0.5 * rz;
-            st.vx[s1] = cmx - (real)0.5 * rx;
-            st.vy[s1] = cmy - (real)0.5 * ry;
-            st.vz[s1] = cmz - (real)0.5 * rz;
+            const real u_cos = rs.template uniform<real>();
+            const real u_phi = rs.template uniform<real>();
+            ntc_scatter(ax, ay, az, bx, by, bz, vrel, u_cos, u_phi);
+            vel.set(s0, ax, ay, az);
+            vel.set(s1, bx, by, bz);
         }
     }
-    candidates += (unsigned long long)pairs;
     vr_max = crm;
 }
 
+template <class Prec> struct StageVel {
+    typedef typename Prec::real real;
+    real *vx, *vy, *vz;
+    __device__ void get(int s, real &x, real &y, real &z) const {
+        x = vx[s];
+        y = vy[s];
+        z = vz[s];
+    }
+    __device__ void set(int s, real x, real y, real z) const {
+        vx[s] = x;
+        vy[s] = y;
+        vz[s] = z;
+    }
+};
+
+template <class Prec>
+__device__ void ntc_collide(const SysDev &g, int cell_global_index, uint32_t step, int n, double coeff,
+                            double &vr_max, double &rest, WarpStage<Prec> &st, unsigned long long &collisions,
+                            unsigned long long &candidates) {
+    const int pairs = ntc_select(coeff, n, vr_max, rest);
+    if (n < 2 || pairs <= 0) return;
+    StageVel<Prec> vel;
+    vel.vx = st.vx;
+    vel.vy = st.vy;
+    vel.vz = st.vz;
+    ntc_run<typename Prec::real>(g.seed, cell_global_index, step, n, pairs, vr_max, vel, st.perm, collisions);
+    candidates += (unsigned long long)pairs;
+}
+
 struct WarpTally {
-    unsigned long long collisions, candidates, wall_hits, reseeds, moved;
+    unsigned long long collisions, candidates, wall_hits, reseeds, moved, stranded;
     long long cross[3];
     unsigned err;
     int sys;
@@ -674,6 +798,7 @@ __device__ __forceinline__ void flush_tally(const PassParams &P, WarpTally &w, i
     const unsigned long long wh = warp_sum_u64(w.wall_hits);
     const unsigned long long rs = warp_sum_u64(w.reseeds);
     const unsigned long long mv = warp_sum_u64(w.moved);
+    const unsigned long long sd = warp_sum_u64(w.stranded);
     long long cr[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) cr[d] = warp_sum_i64(w.cross[d]);
@@ -685,12 +810,13 @@ __device__ __forceinline__ void flush_tally(const PassParams &P, WarpTally &w, i
         if (wh) atomicAdd(&T.wall_hits, wh);
         if (rs) atomicAdd(&T.reseeds, rs);
         if (mv) atomicAdd(&T.particle_steps, mv);
+        if (sd) atomicAdd(&T.stranded, sd);
 #pragma unroll
         for (int d = 0; d < 3; ++d)
             if (cr[d]) atomicAdd((unsigned long long *)&T.count_periodic[d], (unsigned long long)cr[d]);
         if (err) atomicOr(&P.status->error, err);
     }
-    w.collisions = w.candidates = w.wall_hits = w.reseeds = w.moved = 0;
+    w.collisions = w.candidates = w.wall_hits = w.reseeds = w.moved = w.stranded = 0;
     w.cross[0] = w.cross[1] = w.cross[2] = 0;
     w.err = 0;
 }
@@ -724,7 +850,7 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
     unsigned *cnt_out = P.cells.count[P.cur ^ 1];
 
     WarpTally wt;
-    wt.collisions = wt.candidates = wt.wall_hits = wt.reseeds = wt.moved = 0;
+    wt.collisions = wt.candidates = wt.wall_hits = wt.reseeds = wt.moved = wt.stranded = 0;
     wt.cross[0] = wt.cross[1] = wt.cross[2] = 0;
     wt.err = 0;
     wt.sys = -1;
@@ -732,14 +858,15 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
     const int C = P.cells.num_cells;
     const int stride = gridDim.x * warps_per_block;
     for (int a = blockIdx.x * warps_per_block + warp_in_block; a < C; a += stride) {
-        const int sys = P.cells.sys[a];
+        const int4 meta = P.cells.meta[a];
+        const int sys = meta.w;
         if (sys != wt.sys) {
             if (wt.sys >= 0) flush_tally(P, wt, lane);
             wt.sys = sys;
         }
         const SysDev &g = P.sys[sys];
-        int n = (int)min(cnt_in[a], P.cells.cap[a]);
-        const unsigned base = P.cells.base[a];
+        int n = (int)min(cnt_in[a], (unsigned)meta.y);
+        const unsigned base = (unsigned)meta.x;
         if (n > P.smem_cap) {
             wt.err |= DSMC_EBIT_SMEM;
             n = P.smem_cap;
@@ -774,11 +901,9 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
         }
         if (collide) {
             if (lane == 0) {
-                double vr = P.cells.vr_max[a], rest = P.cells.rest[a];
-                ntc_collide<Prec>(g, P.cells.global[a], step, n, P.cells.coeff[a], vr, rest, st, wt.collisions,
-                                  wt.candidates);
-                P.cells.vr_max[a] = vr;
-                P.cells.rest[a] = rest;
+                double4 cs = P.cells.state[a];
+                ntc_collide<Prec>(g, meta.z, step, n, cs.z, cs.x, cs.y, st, wt.collisions, wt.candidates);
+                P.cells.state[a] = cs;
             }
             __syncwarp();
         }
@@ -833,7 +958,7 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
                     mt.wall_hits = mt.reseeds = 0;
                     mt.cross[0] = mt.cross[1] = mt.cross[2] = 0;
                     mt.err = 0;
-                    Prec::move(g, p, move_step, mt);
+                    const bool left_voxel = Prec::move(g, p, move_step, mt);
                     wt.wall_hits += mt.wall_hits;
                     wt.reseeds += mt.reseeds;
                     wt.cross[0] += mt.cross[0];
@@ -841,10 +966,13 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
                     wt.cross[2] += mt.cross[2];
                     wt.err |= mt.err;
                     wt.moved += 1;
-                    const int cg = Prec::cell_global(g, p);
-                    const int ac = __ldg(g.cell_map + cg);
+                    const int ac = left_voxel ? __ldg(g.cell_map + Prec::cell_global(g, p)) : a;
                     if (ac < 0) {
-                        wt.err |= DSMC_EBIT_CELL;
+                        // The reference aborts here (dsmc/system.h:134-142); the
+                        // particle sits in solid and its next move re-seeds it
+                        // (dsmc/moleculemover.cpp:57-60), so keep it in this cell.
+                        wt.err |= DSMC_EBIT_STRANDED;
+                        ++wt.stranded;
                         key = (unsigned)a;
                     } else {
                         key = (unsigned)ac;
@@ -877,8 +1005,9 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
                     RecA ra;
                     RecB rb;
                     Prec::pack(p, ra, rb);
-                    if (slot < P.cells.cap[key]) {
-                        const unsigned dst = P.cells.base[key] + slot;
+                    const int4 km = key == (unsigned)a ? meta : P.cells.meta[key];
+                    if (slot < (unsigned)km.y) {
+                        const unsigned dst = (unsigned)km.x + slot;
                         Aout[dst] = ra;
                         Bout[dst] = rb;
                     } else {

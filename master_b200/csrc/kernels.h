@@ -34,6 +34,13 @@ namespace dsmc {
 DSMC_DECLARE_LAUNCHERS(split32)
 DSMC_DECLARE_LAUNCHERS(fp64)
 
+namespace split32 {
+// the bulk-copy pipelined production pass (fused_split.cuh)
+int fused_capacity(int smem_cap);   // 0: no instantiation holds smem_cap
+int fused_blocks_per_sm(int smem_cap);
+cudaError_t launch_fused(const PassParams &P, int grid, cudaStream_t st);
+}  // namespace split32
+
 // Pass modes (engine.cuh PassMode).
 enum { PASS_FUSED = 0, PASS_INPLACE = 1, PASS_SORT = 2 };
 

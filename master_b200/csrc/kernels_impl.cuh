@@ -30,6 +30,7 @@ template <> struct Maker<Split32> {
             p.v[d] = (float)v[d];
         }
         p.id = id;
+        p.flag = voxel_type(g, p.c[0], p.c[1], p.c[2]) != DSMC_VOX_EMPTY;
     }
     static __device__ void position(const SysDev &g, const Split32::Particle &p, double r[3]) {
         for (int d = 0; d < 3; ++d) r[d] = ((double)p.c[d] + (double)p.o[d]) * g.vox_len[d];
@@ -115,7 +116,8 @@ __global__ void k_gather(const CellArrays cells, const ParticleArrays parts, int
     const RecA *Ain = reinterpret_cast<const RecA *>(parts.A[cur]);
     const RecB *Bin = reinterpret_cast<const RecB *>(parts.B[cur]);
     for (int a = c0 + warp; a < c1; a += nwarps) {
-        const unsigned n = min(cells.count[cur][a], cells.cap[a]);
+        const int4 m = cells.meta[a];
+        const unsigned n = min(cells.count[cur][a], (unsigned)m.y);
         unsigned long long at = 0;
         if (lane == 0 && n) at = atomicAdd(cursor, (unsigned long long)n);
         at = __shfl_sync(0xffffffffu, at, 0);
@@ -124,8 +126,8 @@ __global__ void k_gather(const CellArrays cells, const ParticleArrays parts, int
             continue;
         }
         for (unsigned s = lane; s < n; s += 32) {
-            A[at + s] = Ain[cells.base[a] + s];
-            B[at + s] = Bin[cells.base[a] + s];
+            A[at + s] = Ain[m.x + s];
+            B[at + s] = Bin[m.x + s];
             key[at + s] = a;
         }
         if (lane == 0 && n) atomicAdd(&hist[a], n);
@@ -159,13 +161,14 @@ __global__ void k_insert(const CellArrays cells, const ParticleArrays parts, int
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const int a = key[i];
         if (a < 0) continue;
+        const int4 m = cells.meta[a];
         const unsigned slot = atomicAdd(&cells.count[cur][a], 1u);
-        if (slot >= cells.cap[a]) {
+        if (slot >= (unsigned)m.y) {
             atomicOr(err, DSMC_EBIT_SPILL_FULL);
             continue;
         }
-        Aout[cells.base[a] + slot] = A[i];
-        Bout[cells.base[a] + slot] = B[i];
+        Aout[m.x + slot] = A[i];
+        Bout[m.x + slot] = B[i];
     }
 }
 
@@ -179,10 +182,11 @@ __global__ void k_to_fp64(const SysDev *sys, int s, const CellArrays cells, cons
     const RecA *Ain = reinterpret_cast<const RecA *>(parts.A[cur]);
     const RecB *Bin = reinterpret_cast<const RecB *>(parts.B[cur]);
     for (int a = g.active_begin + warp; a < g.active_end; a += nwarps) {
-        const unsigned n = min(cells.count[cur][a], cells.cap[a]);
+        const int4 m = cells.meta[a];
+        const unsigned n = min(cells.count[cur][a], (unsigned)m.y);
         for (unsigned q = lane; q < n; q += 32) {
             Particle p;
-            Prec::unpack(Ain[cells.base[a] + q], Bin[cells.base[a] + q], p);
+            Prec::unpack(Ain[m.x + q], Bin[m.x + q], p);
             const long long i = (long long)p.id - (long long)id_base;
             if (i < 0 || i >= cap) {
                 atomicOr(err, DSMC_EBIT_CELL);
@@ -194,7 +198,7 @@ __global__ void k_to_fp64(const SysDev *sys, int s, const CellArrays cells, cons
                 r[3 * i + d] = rr[d];
                 v[3 * i + d] = (double)p.v[d];
             }
-            if (cell) cell[i] = cells.global[a];
+            if (cell) cell[i] = m.z;
         }
     }
 }
@@ -208,10 +212,11 @@ __global__ void k_cell_energy(const CellArrays cells, const ParticleArrays parts
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     const RecB *Bin = reinterpret_cast<const RecB *>(parts.B[cur]);
     for (int a = c0 + warp; a < c1; a += nwarps) {
-        const unsigned n = min(cells.count[cur][a], cells.cap[a]);
+        const int4 m = cells.meta[a];
+        const unsigned n = min(cells.count[cur][a], (unsigned)m.y);
         double e = 0;
         for (unsigned q = lane; q < n; q += 32) {
-            const RecB b = Bin[cells.base[a] + q];
+            const RecB b = Bin[m.x + q];
             const double x = (double)b.x, y = (double)b.y, z = (double)b.z;
             e += x * x + y * y + z * z;
         }

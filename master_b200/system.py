@@ -136,6 +136,23 @@ class Geometry:
         return float((self.voxels == 0).mean())
 
 
+def cells_layout(settings: Settings, geometry: Geometry) -> dict:
+    """System::setup_cells' active cells for a geometry (host only)."""
+    lib = capi.load()
+    nx, ny, nz = geometry.shape
+    n = C.c_int()
+    check(lib.dsmc_cells_layout(C.byref(settings.raw), nx, ny, nz, ptr(geometry.voxels, C.c_uint8), 0, None, None,
+                                None, None, None, C.byref(n)))
+    out = {k: np.empty(n.value, np.int32) for k in ("global_index", "pixels", "total_pixels")}
+    out["volume"] = np.empty(n.value)
+    out["coeff"] = np.empty(n.value)
+    check(lib.dsmc_cells_layout(C.byref(settings.raw), nx, ny, nz, ptr(geometry.voxels, C.c_uint8), n.value,
+                                ptr(out["global_index"], C.c_int32), ptr(out["pixels"], C.c_int32),
+                                ptr(out["total_pixels"], C.c_int32), ptr(out["volume"], C.c_double),
+                                ptr(out["coeff"], C.c_double), C.byref(n)))
+    return out
+
+
 class Context:
     """One GPU context holding any number of systems (geometry + gas)."""
 

@@ -22,6 +22,7 @@
  * index so the member order no longer depends on history.
  */
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -176,6 +177,28 @@ void refh_canonicalize_cells(void *h) {
         std::sort(c->molecules.begin(), c->molecules.begin() + c->num_molecules);
         for (int i = 0; i < c->num_molecules; ++i) s->molecule_index_in_cell[c->molecules[i]] = i;
     }
+}
+
+/* System::setup_molecules (dsmc/system.cpp:398-430) with one draw stream per
+ * particle (id n, step 0, init tag): three next_gauss velocities times
+ * sqrt(T/m), then the reference's own find_position. */
+int refh_init_particles(void *h, uint64_t seed, long n) {
+    System *s = sys_of(h);
+    if (n > s->MAX_MOLECULE_NUM) return -1;
+    for (Cell *c : s->active_cells) c->num_molecules = 0;
+    s->num_molecules_local = n;
+    s->num_molecules_global = n;
+    const double sqrt_temp_over_mass = std::sqrt(s->temperature / s->settings->mass);
+    for (long i = 0; i < n; ++i) {
+        tape_select(seed, (uint32_t)i, 0u, 3u);
+        s->v[3 * i + 0] = s->rnd->next_gauss() * sqrt_temp_over_mass;
+        s->v[3 * i + 1] = s->rnd->next_gauss() * sqrt_temp_over_mass;
+        s->v[3 * i + 2] = s->rnd->next_gauss() * sqrt_temp_over_mass;
+        s->find_position((int)i);
+        Cell *c = s->cell_that_should_contain_molecule((int)i);
+        c->add_molecule((int)i, s->molecule_index_in_cell, s->molecule_cell_index);
+    }
+    return 0;
 }
 
 void refh_accelerate(void *h) { sys_of(h)->accelerate(); }

@@ -88,6 +88,7 @@ class RefSystem:
         L.refh_set_particles.argtypes = [C.c_void_p, C.c_long, _D, _D]
         L.refh_get_particles.argtypes = [C.c_void_p, _D, _D, _I]
         L.refh_move.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32]
+        L.refh_init_particles.argtypes = [C.c_void_p, C.c_uint64, C.c_long]
         L.refh_collide.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32]
         L.refh_counters.argtypes = [C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_ulong), C.POINTER(C.c_ulong)]
         L.refh_cell_info.argtypes = [C.c_void_p, _I, _I, _I, _D, _D, _D, _D, _I]
@@ -148,6 +149,10 @@ class RefSystem:
         buf = np.empty(4096, np.int32)
         n = self.lib.refh_cell_members(self.h, cell, _p(buf, C.c_int), buf.size)
         return buf[:n].copy()
+
+    def init_particles(self, seed: int, n: int) -> None:
+        if self.lib.refh_init_particles(self.h, seed, n):
+            raise RuntimeError("too many particles for max_molecules_per_node")
 
     def accelerate(self):
         self.lib.refh_accelerate(self.h)
