@@ -36,12 +36,14 @@
 #define DSMC_EBIT_SMEM 16u       // a cell held more particles than the staging buffer
 #define DSMC_EBIT_NAN 32u        // non-finite position or velocity
 #define DSMC_EBIT_TIMEOUT 128u   // a bounded wait on a bulk copy ran out
+#define DSMC_EBIT_ALIGN 256u     // a bulk copy operand was not 16-byte aligned (copy skipped)
 #define DSMC_EBIT_STRANDED 64u   // a move ended inside solid whose cell has no free volume; the
                                  // particle stays in its previous cell and is re-seeded next step
 // bits that stop the pipeline (a failed facet search or a stranded particle is
 // re-seeded, counted, and the pipeline goes on)
 #define DSMC_EBIT_FATAL \
-    (DSMC_EBIT_CELL | DSMC_EBIT_RESEED | DSMC_EBIT_SPILL_FULL | DSMC_EBIT_SMEM | DSMC_EBIT_NAN | DSMC_EBIT_TIMEOUT)
+    (DSMC_EBIT_CELL | DSMC_EBIT_RESEED | DSMC_EBIT_SPILL_FULL | DSMC_EBIT_SMEM | DSMC_EBIT_NAN | DSMC_EBIT_TIMEOUT | \
+     DSMC_EBIT_ALIGN)
 
 #define DSMC_VOX_PACK(i, j, k) ((uint32_t)(i) | ((uint32_t)(j) << 11) | ((uint32_t)(k) << 22))
 #define DSMC_VOX_I(p) ((int)((p)&0x7FFu))

@@ -25,13 +25,15 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 __device__ __forceinline__ void mbar_arrive_expect(uint64_t *bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
-// global -> shared bulk copy (16-byte aligned addresses, size a multiple of 16)
+// global -> shared bulk copy into this CTA's own shared memory (16-byte
+// aligned addresses, size a multiple of 16; no cluster is involved).
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+    asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                      smem_u32(dst)),
                  "l"(src), "r"(bytes), "r"(smem_u32(bar))
                  : "memory");
 }
+__device__ __forceinline__ bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
@@ -320,11 +322,21 @@ __global__ void __launch_bounds__(256, 3) fused_split_kernel(PassParams P) {
         W.meta[stage] = m_pf;
         W.n[stage] = (int)n_pf;
         const uint32_t bytes = n_pf * 16u;
+        const void *srcA = Ain + m_pf.x, *srcB = Bin + m_pf.x, *srcS = P.cells.state + cell;
+        // every operand is 16-byte aligned by construction; a violation is
+        // recorded and the transfer skipped rather than issued
+        if (!aligned16(srcA) || !aligned16(srcB) || !aligned16(srcS) || !aligned16(&W.A[stage][0]) ||
+            !aligned16(&W.B[stage][0]) || !aligned16(&W.cs[stage])) {
+            atomicOr(&P.status->error, DSMC_EBIT_ALIGN);
+            W.n[stage] = 0;
+            mbar_arrive_expect(&W.bar[stage], 0u);
+            return;
+        }
         mbar_arrive_expect(&W.bar[stage], 2u * bytes + (uint32_t)sizeof(double4));
-        bulk_g2s(&W.cs[stage], P.cells.state + cell, (uint32_t)sizeof(double4), &W.bar[stage]);
+        bulk_g2s(&W.cs[stage], srcS, (uint32_t)sizeof(double4), &W.bar[stage]);
         if (n_pf) {
-            bulk_g2s(&W.A[stage][0], Ain + m_pf.x, bytes, &W.bar[stage]);
-            bulk_g2s(&W.B[stage][0], Bin + m_pf.x, bytes, &W.bar[stage]);
+            bulk_g2s(&W.A[stage][0], srcA, bytes, &W.bar[stage]);
+            bulk_g2s(&W.B[stage][0], srcB, bytes, &W.bar[stage]);
         }
     };
     load_meta(a);
@@ -449,7 +461,8 @@ __global__ void __launch_bounds__(256, 3) fused_split_kernel(PassParams P) {
                 if (lane == 0) W.qn += __popc(slow);
                 __syncwarp();
             }
-            insert(sink, p, valid && stay, (unsigned)a, lane, a, m, t.err);
+            const bool place = valid && stay;
+            insert(sink, p, place, place ? (unsigned)a : 0xffffffffu, lane, a, m, t.err);
         }
         __syncwarp();
     }

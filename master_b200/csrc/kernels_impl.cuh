@@ -246,16 +246,21 @@ cudaError_t launch_pass(int mode, const PassParams &P, int grid, int block, cuda
 
 int pass_blocks_per_sm(int mode, int block, int smem_cap) {
     const size_t smem = stage_bytes(smem_cap) * (block / 32);
+    // the opt-in limit is a property of the function, shared by every
+    // context: raise it to the device maximum, never lower it
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     int nb = 0;
     cudaError_t e;
     if (mode == MODE_FUSED) {
-        cudaFuncSetAttribute(pass_kernel<Prec, MODE_FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(pass_kernel<Prec, MODE_FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pass_kernel<Prec, MODE_FUSED>, block, smem);
     } else if (mode == MODE_INPLACE) {
-        cudaFuncSetAttribute(pass_kernel<Prec, MODE_INPLACE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(pass_kernel<Prec, MODE_INPLACE>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pass_kernel<Prec, MODE_INPLACE>, block, smem);
     } else {
-        cudaFuncSetAttribute(pass_kernel<Prec, MODE_SORT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(pass_kernel<Prec, MODE_SORT>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pass_kernel<Prec, MODE_SORT>, block, smem);
     }
     return e == cudaSuccess ? nb : 0;

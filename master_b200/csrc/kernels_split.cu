@@ -17,7 +17,12 @@ template <int CAP> static cudaError_t launch_fused_cap(const PassParams &P, int 
 }
 template <int CAP> static int fused_cap_blocks() {
     const size_t smem = fused::fused_smem_bytes<CAP>(8);
-    cudaFuncSetAttribute(fused::fused_split_kernel<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the opt-in limit is a property of the function, shared by every
+    // context: raise it to the device maximum, never lower it
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncSetAttribute(fused::fused_split_kernel<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fused::fused_split_kernel<CAP>, 256, smem) != cudaSuccess)
         return 0;
