@@ -288,6 +288,7 @@ def main():
         "gpu_launches": args.steps,
         "clocks": clocks,
         "device_status": {"error_bits": err, "spill": spill},
+        "pass": system.ctx.pass_info(),
         "physics": {"temperature_K": tal.temperature, "collisions": tal.collisions,
                     "wall_collisions": tal.wall_collisions, "reseeds": tal.reseeds,
                     "stranded": tal.stranded},

@@ -230,6 +230,11 @@ int dsmc_cells_set_state(dsmc_ctx *ctx, int sys_id, const double *vr_max, const 
  * pipeline stops after that step and the host re-lays the buffers out. */
 int dsmc_ctx_set_capacity(dsmc_ctx *ctx, double factor, int pad);
 
+/* Launch shape of the timestep pass: pipelined = 1 when the bulk-copy
+ * pipelined split-precision kernel runs dsmc_step (0: the generic cell pass,
+ * e.g. fp64 contexts), its grid and block, and the per-warp staging capacity. */
+int dsmc_pass_info(dsmc_ctx *ctx, int *pipelined, int *grid, int *block, int *stage_capacity);
+
 /* Reads the status of the last pass: bit flags of device-side errors. */
 int dsmc_device_status(dsmc_ctx *ctx, uint32_t *error_bits, uint32_t *spill);
 

@@ -234,10 +234,11 @@ int relayout(dsmc_ctx *ctx, long long total) {
     const int bps = is_fp64(ctx) ? fp64::pass_blocks_per_sm(PASS_FUSED, ctx->block, ctx->smem_cap)
                                  : split32::pass_blocks_per_sm(PASS_FUSED, ctx->block, ctx->smem_cap);
     if (bps <= 0) return fail(ctx, DSMC_ERR_CUDA, "cell pass cannot be resident (shared memory)");
-    is_fp64(ctx) ? fp64::pass_blocks_per_sm(PASS_INPLACE, ctx->block, ctx->smem_cap)
-                 : split32::pass_blocks_per_sm(PASS_INPLACE, ctx->block, ctx->smem_cap);
-    is_fp64(ctx) ? fp64::pass_blocks_per_sm(PASS_SORT, ctx->block, ctx->smem_cap)
-                 : split32::pass_blocks_per_sm(PASS_SORT, ctx->block, ctx->smem_cap);
+    const int bps_in = is_fp64(ctx) ? fp64::pass_blocks_per_sm(PASS_INPLACE, ctx->block, ctx->smem_cap)
+                                    : split32::pass_blocks_per_sm(PASS_INPLACE, ctx->block, ctx->smem_cap);
+    const int bps_so = is_fp64(ctx) ? fp64::pass_blocks_per_sm(PASS_SORT, ctx->block, ctx->smem_cap)
+                                    : split32::pass_blocks_per_sm(PASS_SORT, ctx->block, ctx->smem_cap);
+    if (bps_in <= 0 || bps_so <= 0) return fail(ctx, DSMC_ERR_CUDA, "stage passes cannot be resident (shared memory)");
     ctx->grid = bps * ctx->num_sms;
     ctx->fused_grid = 0;
     if (!is_fp64(ctx) && split32::fused_capacity(ctx->smem_cap) > 0) {
@@ -986,6 +987,16 @@ int dsmc_counters_get(dsmc_ctx *ctx, int sys_id, int64_t out[8]) {
     out[5] = T.count_periodic[1];
     out[6] = T.count_periodic[2];
     out[7] = (int64_t)T.samples;
+    return DSMC_OK;
+}
+
+int dsmc_pass_info(dsmc_ctx *ctx, int *pipelined, int *grid, int *block, int *stage_capacity) {
+    if (!ctx) return DSMC_ERR_ARG;
+    const bool pipe = ctx->use_pipelined && ctx->fused_grid > 0;
+    if (pipelined) *pipelined = pipe ? 1 : 0;
+    if (grid) *grid = pipe ? ctx->fused_grid : ctx->grid;
+    if (block) *block = ctx->block;
+    if (stage_capacity) *stage_capacity = pipe ? split32::fused_capacity(ctx->smem_cap) : ctx->smem_cap;
     return DSMC_OK;
 }
 

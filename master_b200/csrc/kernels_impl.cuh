@@ -244,26 +244,28 @@ cudaError_t launch_pass(int mode, const PassParams &P, int grid, int block, cuda
     return cudaGetLastError();
 }
 
-int pass_blocks_per_sm(int mode, int block, int smem_cap) {
-    const size_t smem = stage_bytes(smem_cap) * (block / 32);
+template <class K> static int blocks_per_sm(K kernel, int block, size_t smem) {
     // the opt-in limit is a property of the function, shared by every
     // context: raise it to the device maximum, never lower it
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) return 0;
+    if (smem + fa.sharedSizeBytes > (size_t)optin) return 0;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes) !=
+        cudaSuccess)
+        return 0;
     int nb = 0;
-    cudaError_t e;
-    if (mode == MODE_FUSED) {
-        cudaFuncSetAttribute(pass_kernel<Prec, MODE_FUSED>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pass_kernel<Prec, MODE_FUSED>, block, smem);
-    } else if (mode == MODE_INPLACE) {
-        cudaFuncSetAttribute(pass_kernel<Prec, MODE_INPLACE>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pass_kernel<Prec, MODE_INPLACE>, block, smem);
-    } else {
-        cudaFuncSetAttribute(pass_kernel<Prec, MODE_SORT>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pass_kernel<Prec, MODE_SORT>, block, smem);
-    }
-    return e == cudaSuccess ? nb : 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, block, smem) != cudaSuccess) return 0;
+    return nb;
+}
+
+int pass_blocks_per_sm(int mode, int block, int smem_cap) {
+    const size_t smem = stage_bytes(smem_cap) * (block / 32);
+    if (mode == MODE_FUSED) return blocks_per_sm(pass_kernel<Prec, MODE_FUSED>, block, smem);
+    if (mode == MODE_INPLACE) return blocks_per_sm(pass_kernel<Prec, MODE_INPLACE>, block, smem);
+    return blocks_per_sm(pass_kernel<Prec, MODE_SORT>, block, smem);
 }
 
 size_t record_bytes() { return sizeof(RecA) + sizeof(RecB); }

@@ -22,7 +22,12 @@ template <int CAP> static int fused_cap_blocks() {
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    cudaFuncSetAttribute(fused::fused_split_kernel<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, fused::fused_split_kernel<CAP>) != cudaSuccess) return 0;
+    if (smem + fa.sharedSizeBytes > (size_t)optin) return 0;
+    if (cudaFuncSetAttribute(fused::fused_split_kernel<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             optin - (int)fa.sharedSizeBytes) != cudaSuccess)
+        return 0;
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fused::fused_split_kernel<CAP>, 256, smem) != cudaSuccess)
         return 0;

@@ -192,6 +192,11 @@ class Context:
     def sync(self):
         self.check(self.lib.dsmc_sync(self.handle))
 
+    def pass_info(self) -> dict:
+        vals = [C.c_int() for _ in range(4)]
+        self.check(self.lib.dsmc_pass_info(self.handle, *(C.byref(v) for v in vals)))
+        return dict(zip(("pipelined", "grid", "block", "stage_capacity"), (v.value for v in vals)))
+
     def device_status(self):
         e, s = C.c_uint32(), C.c_uint32()
         self.check(self.lib.dsmc_device_status(self.handle, C.byref(e), C.byref(s)))

@@ -150,6 +150,7 @@ def test_fused_pass_equals_stage_calls(case):
     stand-alone stage kernels give bit-identical trajectories."""
     A, z, meta = run_pair(case)
     B, _, _ = run_pair(case)
+    assert A.ctx.pass_info()["pipelined"] == 1
     K = 6
     A.step(K)
     for _ in range(K):
@@ -172,6 +173,7 @@ def test_overflow_spills_and_repacks_without_loss():
     host repack must give the same trajectories as ample capacity."""
     A, z, meta = run_pair("small_dt5")
     B, _, _ = run_pair("small_dt5", capacity=(1.0, 0))
+    assert A.ctx.pass_info()["pipelined"] == 1 and B.ctx.pass_info()["pipelined"] == 1
     A.step(5)
     B.step(5)
     ra, va = A.get_particles()
@@ -205,3 +207,30 @@ def test_geometry_gpu_matches_cpu():
                                                       ptr(b.tangents2, C.c_float)))
     for k in ("voxels", "normals", "tangents1", "tangents2"):
         assert np.array_equal(getattr(a, k), getattr(b, k)), k
+
+
+def test_fused_equals_stages_dense_cells():
+    """~40 particles per cell: the pipelined pass with a 128-particle staging
+    capacity (above the default 48 KB shared-memory window) against the
+    stage kernels."""
+    from master_b200 import workloads
+    w = workloads.Workload("dense32", n=32, radius_voxels=3, porosity=0.5, geometry_seed=3, cells=16,
+                           atoms_per_molecule=workloads.simulators_per_cell_weight(2.5e24, 0.1, 2, 40))
+    s = w.settings(rng_seed=99, statistics_interval=1)
+    g = w.geometry()
+    A = System(s, g)
+    B = System(s, g)
+    info = A.ctx.pass_info()
+    assert info["pipelined"] == 1 and info["stage_capacity"] >= 128
+    A.step(4)
+    for _ in range(4):
+        B.accelerate_and_move()
+        B.update_molecule_cells()
+        B.collide()
+        B.sample()
+    ra, va = A.get_particles()
+    rb, vb = B.get_particles()
+    assert np.array_equal(ra, rb) and np.array_equal(va, vb)
+    ma, mb = A.cells()["moments"], B.cells()["moments"]
+    assert np.allclose(ma, mb, rtol=1e-12, atol=1e-12)
+    assert A.tallies().samples == B.tallies().samples == 4
