@@ -36,7 +36,7 @@ EXPORTED = [
     "dsmc_particles_count", "dsmc_particles_get", "dsmc_step", "dsmc_stage_move", "dsmc_stage_sort",
     "dsmc_stage_collide", "dsmc_stage_sample", "dsmc_tallies_get", "dsmc_tallies_reset", "dsmc_cells_get",
     "dsmc_cells_set_state", "dsmc_device_status", "dsmc_stream", "dsmc_counters_get", "dsmc_cells_layout",
-    "dsmc_ctx_set_capacity", "dsmc_pass_info",
+    "dsmc_ctx_set_capacity", "dsmc_pass_info", "dsmc_geometry_finish_gpu_noalloc",
 ]
 
 
@@ -115,6 +115,8 @@ def load() -> C.CDLL:
         "dsmc_geometry_packed_spheres": [C.POINTER(SphereParams), _U8, _F, _F, _F, _F],
         "dsmc_geometry_finish": [C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, _U8, _F, _F, _F],
         "dsmc_geometry_finish_gpu": [C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, _U8, _F, _F, _F],
+        "dsmc_geometry_finish_gpu_noalloc": [C.c_int, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, _U8, _F, _F,
+                                             _F],
         "dsmc_ctx_create": [C.c_int, C.c_int, C.POINTER(_P)],
         "dsmc_ctx_destroy": [_P],
         "dsmc_last_error": [_P],

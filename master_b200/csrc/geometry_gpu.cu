@@ -19,7 +19,9 @@
 
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <queue>
+#include <string>
 #include <vector>
 
 #include "dsmc_b200.h"
@@ -220,5 +222,132 @@ extern "C" int dsmc_geometry_finish_gpu(int device_id, uint32_t nx, uint32_t ny,
         (e = cudaMemcpy(vox, dmask, V, cudaMemcpyDeviceToHost)))
         return cuda_err(e);
     cleanup();
+    return DSMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The same preprocessing for callers that cannot allocate device memory: a
+// caller that runs where a cudaMalloc is not allowed or not wanted (inside a
+// region whose device memory is fixed in advance, or where the implicit
+// device synchronisation of an allocation would stall other work) still needs
+// the stencil's device-side working buffers.  They live in this file-scope
+// array instead, sized for grids of up to kNoAllocMaxVoxels voxels (64^3;
+// 50 bytes per voxel, 13.1 MB that every GPU which loads this library keeps
+// until the process exits).
+//
+// The array's host-side name is only a stand-in for the device symbol: the
+// device address is looked up with cudaGetSymbolAddress once per device, on
+// that device's first call, and cached.  That first call should therefore
+// come before any stream capture.  Every call reuses the same array and
+// leaves its contents behind; each kernel here rewrites every element it
+// later reads, so nothing needs clearing between calls.  Calls that overlap
+// on the GPU (two host threads, same device) race on the array.
+namespace dsmc {
+namespace {
+constexpr uint64_t kNoAllocMaxVoxels = 64ull * 64ull * 64ull;
+constexpr uint64_t kNoAllocBytes = kNoAllocMaxVoxels * (2 + 4 * 12);
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) unsigned char g_geometry_scratch[kNoAllocBytes];
+
+std::mutex g_scratch_mutex;
+unsigned char *g_scratch_ptr[kNoAllocMaxDevices] = {};
+}  // namespace
+}  // namespace dsmc
+
+extern "C" int dsmc_geometry_finish_gpu_noalloc(int device_id, uint32_t nx, uint32_t ny, uint32_t nz, int avg,
+                                                uint8_t *vox, float *nrm, float *t1, float *t2) {
+    if (!vox || !nrm || !t1 || !t2 || nx == 0 || ny == 0 || nz == 0 || avg < 0) return DSMC_ERR_ARG;
+    const uint64_t V = (uint64_t)nx * ny * nz;
+    if (V > kNoAllocMaxVoxels) {
+        set_thread_error("dsmc_geometry_finish_gpu_noalloc: grid of " + std::to_string(V) +
+                         " voxels exceeds the fixed scratch for " + std::to_string(kNoAllocMaxVoxels) +
+                         " voxels (64^3); use dsmc_geometry_finish_gpu");
+        return DSMC_ERR_CAPACITY;
+    }
+    if (device_id < 0 || device_id >= kNoAllocMaxDevices || cudaSetDevice(device_id) != cudaSuccess) {
+        set_thread_error("no CUDA device for geometry preprocessing");
+        return DSMC_ERR_NO_DEVICE;
+    }
+    unsigned char *base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_scratch_mutex);
+        if (!g_scratch_ptr[device_id]) {
+            void *p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_geometry_scratch);
+            if (e != cudaSuccess) {
+                set_thread_error(std::string("dsmc_geometry_finish_gpu_noalloc: scratch address: ") +
+                                 cudaGetErrorString(e));
+                return DSMC_ERR_CUDA;
+            }
+            g_scratch_ptr[device_id] = static_cast<unsigned char *>(p);
+        }
+        base = g_scratch_ptr[device_id];
+    }
+    // layout: mask[V], cand[V], then normals, seeds, tangents1, tangents2
+    // (3 floats per voxel each), every part 16-byte aligned
+    uint8_t *dmask = base;
+    uint8_t *dcand = base + kNoAllocMaxVoxels;
+    float *dn = reinterpret_cast<float *>(base + 2 * kNoAllocMaxVoxels);
+    float *dseed = dn + 3 * kNoAllocMaxVoxels;
+    float *dt1 = dseed + 3 * kNoAllocMaxVoxels;
+    float *dt2 = dt1 + 3 * kNoAllocMaxVoxels;
+    auto cuda_err = [&](cudaError_t e) {
+        set_thread_error(std::string("geometry on the GPU (fixed scratch): ") + cudaGetErrorString(e));
+        return DSMC_ERR_CUDA;
+    };
+    const Dims d = {(int)nx, (int)ny, (int)nz, avg};
+    cudaError_t e;
+    if ((e = cudaMemcpy(dmask, vox, V, cudaMemcpyHostToDevice))) return cuda_err(e);
+    const int block = 256;
+    const int grid = (int)std::min<uint64_t>((V + block - 1) / block, 148 * 64);
+    k_normals<<<grid, block>>>(d, dmask, dn, dcand);
+    if ((e = cudaGetLastError())) return cuda_err(e);
+    std::vector<uint8_t> cand(V);
+    if ((e = cudaMemcpy(nrm, dn, 12 * V, cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(cand.data(), dcand, V, cudaMemcpyDeviceToHost)))
+        return cuda_err(e);
+    std::priority_queue<uint64_t, std::vector<uint64_t>, std::greater<uint64_t>> dirty;
+    std::vector<uint8_t> queued(V, 0);
+    for (uint64_t idx = 0; idx < V; ++idx)
+        if (cand[idx]) {
+            dirty.push(idx);
+            queued[idx] = 1;
+        }
+    const int reach = std::max(1, avg);
+    while (!dirty.empty()) {
+        const uint64_t idx = dirty.top();
+        dirty.pop();
+        const int k = (int)(idx % nz), j = (int)((idx / nz) % ny), i = (int)(idx / ((uint64_t)ny * nz));
+        float n[3];
+        const bool emptied = normal_of(d, vox, i, j, k, n);
+        nrm[3 * idx] = n[0];
+        nrm[3 * idx + 1] = n[1];
+        nrm[3 * idx + 2] = n[2];
+        if (emptied && vox[idx] != 0) {
+            vox[idx] = 0;
+            for (int di = -reach; di <= reach; ++di)
+                for (int dj = -reach; dj <= reach; ++dj)
+                    for (int dk = -reach; dk <= reach; ++dk) {
+                        const uint64_t q = lin(d, i + di, j + dj, k + dk);
+                        if (q > idx && !queued[q]) {
+                            queued[q] = 1;
+                            dirty.push(q);
+                        }
+                    }
+        }
+    }
+    std::vector<float> seed(3 * V);
+    Ran1 rnd(-1);
+    for (uint64_t q = 0; q < 3 * V; ++q) seed[q] = (float)rnd.next();
+    if ((e = cudaMemcpy(dn, nrm, 12 * V, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(dseed, seed.data(), 12 * V, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(dmask, vox, V, cudaMemcpyHostToDevice)))
+        return cuda_err(e);
+    k_frames<<<grid, block>>>(V, dn, dseed, dt1, dt2, dmask);
+    if ((e = cudaGetLastError())) return cuda_err(e);
+    if ((e = cudaMemcpy(t1, dt1, 12 * V, cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(t2, dt2, 12 * V, cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(vox, dmask, V, cudaMemcpyDeviceToHost)))
+        return cuda_err(e);
     return DSMC_OK;
 }
