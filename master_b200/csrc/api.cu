@@ -84,7 +84,7 @@ struct dsmc_ctx {
     int num_cells = 0;
     DevBuf<int4> meta;
     DevBuf<double4> state;
-    DevBuf<unsigned> count0, count1, key;
+    DevBuf<unsigned> bot[3], top[3], key;  // occupancy sets, rotating per re-binning pass
     DevBuf<double> mom;
     std::vector<int4> h_meta;   // {base, cap, global, sys}
     size_t slots = 0;
@@ -94,6 +94,7 @@ struct dsmc_ctx {
     DevBuf<SpillRec> spill;
     unsigned spill_cap = 1u << 16;
     int cur = 0;
+    int cphase = 0;           // occupancy set the next pass reads
     bool pending = false;     // the last step's collide/sample has not run yet
     bool keys_valid = false;  // a stand-alone move stage left new cell keys
     // staging
@@ -139,8 +140,10 @@ CellArrays cell_arrays(dsmc_ctx *ctx) {
     c.num_cells = ctx->num_cells;
     c.meta = ctx->meta.p;
     c.state = ctx->state.p;
-    c.count[0] = ctx->count0.p;
-    c.count[1] = ctx->count1.p;
+    for (int q = 0; q < 3; ++q) {
+        c.bot[q] = ctx->bot[q].p;
+        c.top[q] = ctx->top[q].p;
+    }
     c.mom = ctx->mom.p;
     c.key = ctx->key.p;
     return c;
@@ -215,18 +218,21 @@ int relayout(dsmc_ctx *ctx, long long total) {
     CK(ctx->meta.ensure(std::max(C, 1)));
     if (C) {
         CK(cudaMemcpyAsync(ctx->meta.p, ctx->h_meta.data(), C * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemsetAsync(ctx->count0.p, 0, C * sizeof(unsigned), ctx->stream));
-        CK(cudaMemsetAsync(ctx->count1.p, 0, C * sizeof(unsigned), ctx->stream));
+        for (int q = 0; q < 3; ++q) {
+            CK(cudaMemsetAsync(ctx->bot[q].p, 0, C * sizeof(unsigned), ctx->stream));
+            CK(cudaMemsetAsync(ctx->top[q].p, 0, C * sizeof(unsigned), ctx->stream));
+        }
     }
     ctx->cur = 0;
+    ctx->cphase = 0;
     CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(unsigned) * 2, ctx->stream));  // error, spill
     unsigned zero = 0;
     CK(cudaMemcpyAsync(&ctx->status.p->halted, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
     if (total > 0) {
         cudaError_t e = is_fp64(ctx)
-                            ? fp64::launch_insert(cell_arrays(ctx), particle_arrays(ctx), 0, total, ctx->fA.p,
+                            ? fp64::launch_insert(cell_arrays(ctx), particle_arrays(ctx), 0, 0, total, ctx->fA.p,
                                                   ctx->fB.p, ctx->fkey.p, &ctx->status.p->error, ctx->stream)
-                            : split32::launch_insert(cell_arrays(ctx), particle_arrays(ctx), 0, total, ctx->fA.p,
+                            : split32::launch_insert(cell_arrays(ctx), particle_arrays(ctx), 0, 0, total, ctx->fA.p,
                                                      ctx->fB.p, ctx->fkey.p, &ctx->status.p->error, ctx->stream);
         CK(e);
     }
@@ -277,11 +283,12 @@ int stage_present(dsmc_ctx *ctx, long long extra, int skip, long long *staged) {
             if ((int)s == skip) continue;
             SysHost &h = *ctx->systems[s];
             if (h.active_end <= h.active_begin) continue;
-            e = is_fp64(ctx) ? fp64::launch_gather(cell_arrays(ctx), particle_arrays(ctx), ctx->cur, h.active_begin,
+            e = is_fp64(ctx) ? fp64::launch_gather(cell_arrays(ctx), particle_arrays(ctx), ctx->cur, ctx->cphase,
+                                                   h.active_begin,
                                                    h.active_end, std::min(st.spill, ctx->spill_cap), ctx->fA.p,
                                                    ctx->fB.p, ctx->fkey.p, ctx->hist.p, ctx->cursor.p,
                                                    (unsigned long long)total, &ctx->status.p->error, ctx->stream)
-                             : split32::launch_gather(cell_arrays(ctx), particle_arrays(ctx), ctx->cur,
+                             : split32::launch_gather(cell_arrays(ctx), particle_arrays(ctx), ctx->cur, ctx->cphase,
                                                       h.active_begin, h.active_end, std::min(st.spill, ctx->spill_cap),
                                                       ctx->fA.p, ctx->fB.p, ctx->fkey.p, ctx->hist.p, ctx->cursor.p,
                                                       (unsigned long long)total, &ctx->status.p->error, ctx->stream);
@@ -306,29 +313,38 @@ int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, 
     P.cells = cell_arrays(ctx);
     P.parts = particle_arrays(ctx);
     P.cur = ctx->cur;
+    P.cin = ctx->cphase;
+    P.cout = (ctx->cphase + 1) % 3;
+    P.cclear = (ctx->cphase + 2) % 3;
     P.do_collide = do_collide;
     P.do_move = do_move;
     P.do_sample = do_sample;
     P.smem_cap = ctx->smem_cap;
     P.advance_step = advance;
     cudaError_t e;
-    if (mode == PASS_FUSED && ctx->use_pipelined && ctx->fused_grid > 0)
+    if (mode == PASS_FUSED && ctx->use_pipelined && ctx->fused_grid > 0) {
+        P.top_only = 0;
         e = split32::launch_fused(P, ctx->fused_grid, ctx->stream);
-    else
+    } else {
+        P.top_only = 1;
         e = is_fp64(ctx) ? fp64::launch_pass(mode, P, ctx->grid, ctx->block, ctx->stream)
                          : split32::launch_pass(mode, P, ctx->grid, ctx->block, ctx->stream);
+    }
     CK(e);
+    // a re-binning pass rotates the occupancy sets
+    if (mode != PASS_INPLACE) ctx->cphase = (ctx->cphase + 1) % 3;
     return DSMC_OK;
 }
 
 // After a batch of passes: find how many ran, fix the buffer parity, and
 // repack if one of them spilled.
-int settle(dsmc_ctx *ctx, unsigned step_before, int cur_before, int *ran) {
+int settle(dsmc_ctx *ctx, unsigned step_before, int cur_before, int cphase_before, int *ran) {
     cudaError_t e;
     Status st = read_status(ctx, &e);
     CK(e);
     *ran = (int)(st.step - step_before);
     ctx->cur = cur_before ^ (*ran & 1);
+    ctx->cphase = (cphase_before + *ran) % 3;
     if (st.error & DSMC_EBIT_FATAL) {
         char buf[160];
         std::snprintf(buf, sizeof(buf), "device error bits 0x%x after step %u (1 cell, 4 reseed, 8 spill list, 16 "
@@ -397,8 +413,10 @@ int rebuild_cells(dsmc_ctx *ctx) {
     const size_t Cn = std::max(C, 1);
     CK(ctx->meta.alloc(Cn));
     CK(ctx->state.alloc(Cn));
-    CK(ctx->count0.alloc(Cn));
-    CK(ctx->count1.alloc(Cn));
+    for (int q = 0; q < 3; ++q) {
+        CK(ctx->bot[q].alloc(Cn));
+        CK(ctx->top[q].alloc(Cn));
+    }
     CK(ctx->mom.alloc(8 * Cn));
     CK(ctx->hist.alloc(Cn));
     if (C) {
@@ -406,8 +424,10 @@ int rebuild_cells(dsmc_ctx *ctx) {
             for (int q = 0; q < C_old; ++q) state[q] = old_state[q];
         CK(cudaMemcpyAsync(ctx->state.p, state.data(), C * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaMemsetAsync(ctx->mom.p, 0, 8 * C * sizeof(double), ctx->stream));
-        CK(cudaMemsetAsync(ctx->count0.p, 0, C * sizeof(unsigned), ctx->stream));
-        CK(cudaMemsetAsync(ctx->count1.p, 0, C * sizeof(unsigned), ctx->stream));
+        for (int q = 0; q < 3; ++q) {
+            CK(cudaMemsetAsync(ctx->bot[q].p, 0, C * sizeof(unsigned), ctx->stream));
+            CK(cudaMemsetAsync(ctx->top[q].p, 0, C * sizeof(unsigned), ctx->stream));
+        }
         if (C_old > 0 && C_old <= C)
             CK(cudaMemcpyAsync(ctx->mom.p, old_mom.data(), 8 * C_old * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     }
@@ -754,10 +774,10 @@ int dsmc_particles_get(dsmc_ctx *ctx, int sys_id, int64_t cap, double *r, double
     if (N == 0) return DSMC_OK;
     cudaError_t e = is_fp64(ctx)
                         ? fp64::launch_to_fp64(ctx->sys_dev.p, sys_id, cell_arrays(ctx), particle_arrays(ctx), ctx->cur,
-                                               0, N, ctx->io_r.p, ctx->io_v.p, ctx->io_cell.p, &ctx->status.p->error,
+                                               ctx->cphase, 0, N, ctx->io_r.p, ctx->io_v.p, ctx->io_cell.p, &ctx->status.p->error,
                                                ctx->stream)
                         : split32::launch_to_fp64(ctx->sys_dev.p, sys_id, cell_arrays(ctx), particle_arrays(ctx),
-                                                  ctx->cur, 0, N, ctx->io_r.p, ctx->io_v.p, ctx->io_cell.p,
+                                                  ctx->cur, ctx->cphase, 0, N, ctx->io_r.p, ctx->io_v.p, ctx->io_cell.p,
                                                   &ctx->status.p->error, ctx->stream);
     CK(e);
     CK(cudaMemcpyAsync(r, ctx->io_r.p, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -779,6 +799,7 @@ int dsmc_step(dsmc_ctx *ctx, int nsteps) {
         CK(e);
         const unsigned step0 = st.step;
         const int cur0 = ctx->cur;
+        const int cphase0 = ctx->cphase;
         const bool pending0 = ctx->pending;
         // One fused pass per step: collide + sample of the previous step's
         // cells, then accelerate + move + re-bin of this step.
@@ -789,7 +810,7 @@ int dsmc_step(dsmc_ctx *ctx, int nsteps) {
             ctx->cur ^= 1;
         }
         int ran = 0;
-        int rc = settle(ctx, step0, cur0, &ran);
+        int rc = settle(ctx, step0, cur0, cphase0, &ran);
         if (rc) return rc;
         if (ran <= 0) return fail(ctx, DSMC_ERR_STATE, "timestep pipeline made no progress");
         ctx->pending = true;
@@ -876,10 +897,11 @@ int dsmc_tallies_get(dsmc_ctx *ctx, int sys_id, dsmc_tallies *t) {
     if (C > 0 && ctx->A0.p) {
         DevBuf<double> ce;
         CK(ce.alloc(C));
-        e = is_fp64(ctx) ? fp64::launch_cell_energy(cell_arrays(ctx), particle_arrays(ctx), ctx->cur, h.active_begin,
+        e = is_fp64(ctx) ? fp64::launch_cell_energy(cell_arrays(ctx), particle_arrays(ctx), ctx->cur, ctx->cphase,
+                                                    h.active_begin,
                                                     h.active_end, ce.p, ctx->stream)
                          : split32::launch_cell_energy(cell_arrays(ctx), particle_arrays(ctx), ctx->cur,
-                                                       h.active_begin, h.active_end, ce.p, ctx->stream);
+                                                       ctx->cphase, h.active_begin, h.active_end, ce.p, ctx->stream);
         CK(e);
         std::vector<double> hc(C);
         CK(cudaMemcpyAsync(hc.data(), ce.p, C * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
@@ -927,9 +949,14 @@ int dsmc_cells_get(dsmc_ctx *ctx, int sys_id, int cap, int32_t *global_index, in
     const int a0 = h.active_begin;
     if (global_index) std::memcpy(global_index, h.cell_global.data(), C * sizeof(int32_t));
     if (volume) std::memcpy(volume, h.volume_cell.data(), C * sizeof(double));
+    std::vector<unsigned> nb, nt;
     if (count) {
-        unsigned *cp = ctx->cur ? ctx->count1.p : ctx->count0.p;
-        CK(cudaMemcpyAsync(count, cp + a0, C * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        nb.resize(C);
+        nt.resize(C);
+        CK(cudaMemcpyAsync(nb.data(), ctx->bot[ctx->cphase].p + a0, C * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+        CK(cudaMemcpyAsync(nt.data(), ctx->top[ctx->cphase].p + a0, C * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                           ctx->stream));
     }
     std::vector<double4> st(C);
     if (vr_max || rest)
@@ -941,6 +968,11 @@ int dsmc_cells_get(dsmc_ctx *ctx, int sys_id, int cap, int32_t *global_index, in
     for (int q = 0; q < C; ++q) {
         if (vr_max) vr_max[q] = st[q].x;
         if (rest) rest[q] = st[q].y;
+        if (count) {
+            const unsigned cap = (unsigned)ctx->h_meta[a0 + q].y;
+            const unsigned b = std::min(nb[q], cap);
+            count[q] = (int32_t)(b + std::min(nt[q], cap - b));
+        }
     }
     return DSMC_OK;
 }
@@ -995,7 +1027,7 @@ int dsmc_pass_info(dsmc_ctx *ctx, int *pipelined, int *grid, int *block, int *st
     const bool pipe = ctx->use_pipelined && ctx->fused_grid > 0;
     if (pipelined) *pipelined = pipe ? 1 : 0;
     if (grid) *grid = pipe ? ctx->fused_grid : ctx->grid;
-    if (block) *block = ctx->block;
+    if (block) *block = pipe ? split32::fused_block() : ctx->block;
     if (stage_capacity) *stage_capacity = pipe ? split32::fused_capacity(ctx->smem_cap) : ctx->smem_cap;
     return DSMC_OK;
 }

@@ -5,10 +5,16 @@
 // are concatenated into one cell range, and every kernel walks that range.
 //
 // Particles live in per-cell slot regions (a bucketed counting sort):
-//   active cell a owns slots [cell_base[a], cell_base[a] + cell_cap[a]) of
-//   each particle array, cell_count[b][a] of them occupied in buffer b.
-// Buffers b = 0/1 ping-pong: the fused pass reads buffer `cur` and inserts
+//   active cell a owns slots [base, base + cap) of each particle array
+//   (meta[a] = {base, cap, ...}); two segments of them are occupied:
+//   the bottom [base, base + bot) and the top [base + cap - top, base + cap).
+// Buffers b = 0/1 ping-pong: the fused pass reads buffer `cur` and places
 // every moved particle into its new cell's region of buffer `cur ^ 1`.
+// Particles that stay in their cell are written to the bottom by the warp
+// that owns the cell, without atomics; every other placement takes a top slot
+// with an atomic.  The occupancy counts rotate through three sets (in, out,
+// and the set the pass clears for the pass after next), so no count a pass
+// reads is written during it.
 //
 // Record formats (structure of arrays, 16-byte vectors):
 //   split precision:  A = uint4 {voxel (i | j<<11 | k<<22), ox, oy, oz (fp32 bits)}
@@ -51,6 +57,14 @@
 #define DSMC_VOX_K(p) ((int)((p) >> 22))
 
 namespace dsmc {
+
+// Slot address of the s-th occupied particle of a cell (bottom, then top).
+#ifdef __CUDACC__
+__host__ __device__
+#endif
+inline unsigned cell_slot(int base, int cap, unsigned bot, unsigned top, unsigned s) {
+    return s < bot ? (unsigned)base + s : (unsigned)(base + cap) - top + (s - bot);
+}
 
 struct SysDev {
     // voxel grid (no halo; periodic index wrap replaces the reference's 27x copy)
@@ -119,7 +133,8 @@ struct CellArrays {
                                //  (sigma*c_r)_max bookkeeping and NTC remainder
                                //  (dsmc/cell.cpp:42-111), 0.5 F_N pi d^2 dt / V_cell
                                //  (dsmc/cell.cpp:27-40)
-    unsigned *count[2];        // occupancy per buffer
+    unsigned *bot[3];          // bottom-segment occupancy, three rotating sets
+    unsigned *top[3];          // top-segment occupancy
     double *mom;               // 8 fp64 per cell: n, sum v (3), sum v^2 (3), sum |v|^2
     unsigned *key;             // per slot: new active cell after a stand-alone move stage
 };
@@ -138,6 +153,8 @@ struct PassParams {
     CellArrays cells;
     ParticleArrays parts;
     int cur;                   // buffer read this pass
+    int cin, cout, cclear;     // count sets: read, written, cleared this pass
+    int top_only;              // every placement takes a top slot (generic passes)
     int do_collide;            // collide the cells of the pass's input (step - 1's sort)
     int do_move;               // accelerate + move + re-bin (step)
     int do_sample;             // sample after the collide, on the reference's cadence

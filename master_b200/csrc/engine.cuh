@@ -354,7 +354,10 @@ struct Split32 {
     }
 
     static __device__ __forceinline__ void accelerate(const SysDev &g, Particle &p) {
-        if (g.flow_dir >= 0) p.v[g.flow_dir] += g.accel_dt_f;
+        // unrolled select: a runtime index into p.v would put the particle in local memory
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (d == g.flow_dir) p.v[d] += g.accel_dt_f;
     }
 };
 
@@ -613,7 +616,9 @@ struct Fp64 {
     }
 
     static __device__ __forceinline__ void accelerate(const SysDev &g, Particle &p) {
-        if (g.flow_dir >= 0) p.v[g.flow_dir] += g.accel_dt;
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (d == g.flow_dir) p.v[d] += g.accel_dt;
     }
 };
 
@@ -846,8 +851,9 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
     RecB *Bout = reinterpret_cast<RecB *>(P.parts.B[P.cur ^ 1]);
     RecA *Aio = reinterpret_cast<RecA *>(P.parts.A[P.cur]);
     RecB *Bio = reinterpret_cast<RecB *>(P.parts.B[P.cur]);
-    unsigned *cnt_in = P.cells.count[P.cur];
-    unsigned *cnt_out = P.cells.count[P.cur ^ 1];
+    const unsigned *bot_in = P.cells.bot[P.cin];
+    const unsigned *top_in = P.cells.top[P.cin];
+    unsigned *top_out = P.cells.top[P.cout];
 
     WarpTally wt;
     wt.collisions = wt.candidates = wt.wall_hits = wt.reseeds = wt.moved = wt.stranded = 0;
@@ -865,8 +871,9 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
             wt.sys = sys;
         }
         const SysDev &g = P.sys[sys];
-        int n = (int)min(cnt_in[a], (unsigned)meta.y);
-        const unsigned base = (unsigned)meta.x;
+        const unsigned nb = min(bot_in[a], (unsigned)meta.y);
+        const unsigned nt = min(top_in[a], (unsigned)meta.y - nb);
+        int n = (int)(nb + nt);
         if (n > P.smem_cap) {
             wt.err |= DSMC_EBIT_SMEM;
             n = P.smem_cap;
@@ -881,7 +888,7 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
             for (int s = lane; s < n; s += 32) {
                 real v[3];
                 uint32_t id;
-                Prec::stage_load(Ain, Bin, base + s, v, id);
+                Prec::stage_load(Ain, Bin, cell_slot(meta.x, meta.y, nb, nt, s), v, id);
                 st.vx[s] = v[0];
                 st.vy[s] = v[1];
                 st.vz[s] = v[2];
@@ -931,7 +938,11 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
             }
         }
         if (MODE == MODE_FUSED || MODE == MODE_SORT) {
-            if (lane == 0) cnt_in[a] = 0;
+            // this pass writes only top slots; clear the set the pass after next fills
+            if (lane == 0) {
+                P.cells.bot[P.cclear][a] = 0;
+                P.cells.top[P.cclear][a] = 0;
+            }
         }
 
         // Move (or pass through) and place every particle.
@@ -941,9 +952,10 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
             const bool valid = s < n;
             Particle p;
             unsigned key = 0xffffffffu;
+            const unsigned addr = cell_slot(meta.x, meta.y, nb, nt, (unsigned)s);
             if (valid) {
-                RecA ra = Ain[base + s];
-                RecB rb = Bin[base + s];
+                RecA ra = Ain[addr];
+                RecB rb = Bin[addr];
                 Prec::unpack(ra, rb, p);
                 if (MODE != MODE_SORT) {
                     p.v[0] = st.vx[s];
@@ -951,7 +963,7 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
                     p.v[2] = st.vz[s];
                 }
                 if (MODE == MODE_SORT) {
-                    key = P.cells.key[base + s];
+                    key = P.cells.key[addr];
                 } else if (P.do_move) {
                     Prec::accelerate(g, p);
                     MoveTally mt;
@@ -987,30 +999,37 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
                     RecB rb;
                     Prec::pack(p, ra, rb);
                     if (P.do_move) {
-                        Aio[base + s] = ra;
-                        P.cells.key[base + s] = key;
+                        Aio[addr] = ra;
+                        P.cells.key[addr] = key;
                     }
-                    if (P.do_move || collide) Bio[base + s] = rb;
+                    if (P.do_move || collide) Bio[addr] = rb;
                 }
             } else {
-                // Warp-aggregated counting-sort insert into the new cell's slots.
+                // Warp-aggregated counting-sort insert into the new cell's top slots.
                 const unsigned peers = __match_any_sync(0xffffffffu, key);
                 const int leader = __ffs(peers) - 1;
                 const unsigned lower = peers & ((1u << lane) - 1u);
                 unsigned slot0 = 0;
-                if (valid && lane == leader) slot0 = atomicAdd(&cnt_out[key], (unsigned)__popc(peers));
+                if (valid && lane == leader) slot0 = atomicAdd(&top_out[key], (unsigned)__popc(peers));
                 slot0 = __shfl_sync(0xffffffffu, slot0, leader);
+                bool spilled = false;
                 if (valid) {
-                    const unsigned slot = slot0 + (unsigned)__popc(lower);
+                    const unsigned k = slot0 + (unsigned)__popc(lower);
                     RecA ra;
                     RecB rb;
                     Prec::pack(p, ra, rb);
                     const int4 km = key == (unsigned)a ? meta : P.cells.meta[key];
-                    if (slot < (unsigned)km.y) {
-                        const unsigned dst = (unsigned)km.x + slot;
+                    // a top slot may not reach the slots the cell's owner can
+                    // fill from the bottom (at most its input occupancy)
+                    const unsigned room =
+                        P.top_only ? (unsigned)km.y
+                                   : (unsigned)km.y - min((unsigned)km.y, bot_in[key] + top_in[key]);
+                    if (k < room) {
+                        const unsigned dst = (unsigned)(km.x + km.y) - 1u - k;
                         Aout[dst] = ra;
                         Bout[dst] = rb;
                     } else {
+                        spilled = true;
                         const unsigned si = atomicAdd(&P.status->spill, 1u);
                         if (si < P.parts.spill_cap) {
                             SpillRec &sr = P.parts.spill[si];
@@ -1027,6 +1046,10 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
                         }
                     }
                 }
+                // spilled slots are given back, so the counter ends at the
+                // number of particles actually placed in the top segment
+                const unsigned over = __ballot_sync(0xffffffffu, spilled) & peers;
+                if (valid && lane == leader && over) atomicSub(&top_out[key], (unsigned)__popc(over));
             }
         }
     }

@@ -1,14 +1,18 @@
 // The production timestep pass for split-precision state: one kernel per
 // step that, for every active cell, collides (NTC) and samples the particles
 // the previous step sorted into it, then accelerates, moves and re-bins them
-// into the next buffer.  One warp per cell, persistent grid.
+// into the next buffer.  One warp per cell at a time, persistent grid.
 //
-// Memory pipeline: each warp double-buffers its cells in shared memory.  While
-// it works on cell k, the bulk-copy engine (cp.async.bulk, completion on an
-// mbarrier) brings cell k+1's particle records in; cell k+2's metadata is
-// loaded into registers at the same time.  Every wait on an mbarrier is
-// bounded: on expiry the warp records DSMC_EBIT_TIMEOUT, waits (bounded) for
-// its copies in flight and leaves the loop.  No cluster multicast is used.
+// Work layout: each warp owns chunks of 32 consecutive active cells (chunk c
+// goes to warp c mod total warps).  The per-cell bookkeeping of a chunk --
+// metadata, occupancy, the NTC selection count, the (sigma c_r)_max state and
+// the occupancy written for the next pass -- is done by lane i for cell i,
+// with coalesced loads and stores, two chunks ahead of the particle work.
+//
+// Memory pipeline: the particle records of the warp's next cells stream into
+// a per-warp shared-memory ring of R slots with per-lane 16-byte cp.async
+// copies, one commit group per cell, up to DEPTH cells ahead of the cell in
+// work.  Waits are cp.async.wait_group on the warp's own copies (no spin).
 #pragma once
 #include "engine.cuh"
 
@@ -17,40 +21,24 @@ namespace fused {
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-__device__ __forceinline__ void mbar_init(uint64_t *bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+// 16-byte global -> shared copy, cached in L2 only (both addresses 16-byte
+// aligned: slots are uint4/float4 records).
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void mbar_arrive_expect(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Waits until at most `pending` of this thread's newest commit groups are
+// still in flight (0 <= pending <= 4).
+__device__ __forceinline__ void cp_async_wait(int pending) {
+    switch (pending) {
+        case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+        case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+        case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+        case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+        default: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
+    }
 }
-// global -> shared bulk copy into this CTA's own shared memory (16-byte
-// aligned addresses, size a multiple of 16; no cluster is involved).
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile("cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-__device__ __forceinline__ bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait: false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    for (int i = 0; i < (1 << 22); ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
+constexpr int DEPTH = 4;  // cells staged ahead of the one in work
 
 struct SmemVel {
     float4 *b;
@@ -78,18 +66,31 @@ struct SlowRec {
 
 constexpr int QCAP = 32;
 
-template <int CAP> struct WarpSmem {
-    uint4 A[2][CAP];
-    float4 B[2][CAP];
-    double4 cs[2];       // cell state {vr_max, rest, coeff, 0}
-    int4 meta[2];        // cell metadata {base, cap, global, sys}
-    uint64_t bar[2];
-    int n[2];
-    int qn;
-    int pad;
-    unsigned wtally[8];  // wall hits, reseeds, crossings x3, stranded, error bits (drained particles)
+// Per-chunk cell table: entry i describes cell first + i of the chunk.
+struct CellTab {
+    int base[32];        // first slot
+    int cap[32];         // slots
+    unsigned nb[32];     // bottom-segment occupancy (input)
+    unsigned nt[32];     // top-segment occupancy (input)
+    int glob[32];        // the reference's cell index
+    int sys[32];
+    int pairs[32];       // NTC candidate pairs this step
+    double vr[32];       // (sigma c_r)_max
+    double rest[32];     // selection remainder after this step's selection
+    int first;           // first active cell of the chunk
+    int ncell;           // cells in the chunk; 0: no chunk
+};
+
+// Per-warp shared memory: particle ring, two chunk tables, the general-mover
+// queue and the collide permutation.
+template <int R> struct WarpSmem {
+    uint4 A[R];
+    float4 B[R];
+    CellTab tab[2];
     SlowRec q[QCAP];
-    uint16_t perm[CAP];
+    uint16_t perm[R];
+    int qn;
+    unsigned wtally[8];  // wall hits, reseeds, crossings x3, stranded, error bits (drained particles)
 };
 
 struct LaneTally {
@@ -107,7 +108,7 @@ __device__ __forceinline__ void lane_tally_reset(LaneTally &t) {
 
 __device__ __forceinline__ unsigned warp_sum_u32(unsigned x) { return __reduce_add_sync(0xffffffffu, x); }
 
-__device__ void flush_lane_tally(const PassParams &P, LaneTally &t, int lane) {
+__device__ __forceinline__ void flush_lane_tally(const PassParams &P, LaneTally &t, int lane) {
     const unsigned long long col = warp_sum_u32(t.collisions), cand = warp_sum_u32(t.candidates);
     const unsigned long long wh = warp_sum_u32(t.wall_hits), rs = warp_sum_u32(t.reseeds);
     const unsigned long long mv = warp_sum_u32(t.moved), sd = warp_sum_u32(t.stranded);
@@ -133,7 +134,7 @@ __device__ void flush_lane_tally(const PassParams &P, LaneTally &t, int lane) {
 
 // Folds the drained particles' counts (warp shared tally) into lane 0's
 // tally and publishes the warp's counts for its current system.
-template <int CAP> __device__ void flush_warp(const PassParams &P, WarpSmem<CAP> &W, LaneTally &t, int lane) {
+template <int R> __device__ __forceinline__ void flush_warp(const PassParams &P, WarpSmem<R> &W, LaneTally &t, int lane) {
     __syncwarp();
     if (lane == 0) {
         t.wall_hits += W.wtally[0];
@@ -150,54 +151,52 @@ template <int CAP> __device__ void flush_warp(const PassParams &P, WarpSmem<CAP>
     flush_lane_tally(P, t, lane);
 }
 
-// Output side of a pass: where a moved particle goes.
-struct Sink {
-    unsigned *cnt_out;
-    uint4 *Aout;
-    float4 *Bout;
-    const int4 *meta;
-    Status *status;
-    SpillRec *spill;
-    unsigned spill_cap;
-};
-
-// Places one particle per valid lane into its new cell of the output buffer
-// (warp-aggregated counting-sort insert; overflow goes to the spill list).
-__device__ __forceinline__ void insert(const Sink &k, const Split32::Particle &p, bool valid, unsigned key, int lane,
-                                       int home, const int4 &home_meta, unsigned &err) {
+// Places one particle per valid lane into a top slot of its new cell
+// (warp-aggregated atomics; a slot that could meet the owner's bottom
+// segment, i.e. within the cell's input occupancy, spills instead).
+__device__ __forceinline__ void insert_top(const PassParams &P, const Split32::Particle &p, bool valid,
+                                           unsigned key, int lane, unsigned &err) {
+    unsigned *top_out = P.cells.top[P.cout];
     const unsigned peers = __match_any_sync(0xffffffffu, key);
     const int leader = __ffs(peers) - 1;
     unsigned slot0 = 0;
-    if (valid && lane == leader) slot0 = atomicAdd(&k.cnt_out[key], (unsigned)__popc(peers));
+    if (valid && lane == leader) slot0 = atomicAdd(&top_out[key], (unsigned)__popc(peers));
     slot0 = __shfl_sync(0xffffffffu, slot0, leader);
-    if (!valid) return;
-    const unsigned slot = slot0 + (unsigned)__popc(peers & ((1u << lane) - 1u));
-    uint4 ra;
-    float4 rb;
-    Split32::pack(p, ra, rb);
-    const int4 km = key == (unsigned)home ? home_meta : k.meta[key];
-    if (slot < (unsigned)km.y) {
-        const unsigned dst = (unsigned)km.x + slot;
-        k.Aout[dst] = ra;
-        k.Bout[dst] = rb;
-    } else {
-        const unsigned si = atomicAdd(&k.status->spill, 1u);
-        if (si < k.spill_cap) {
-            SpillRec &sr = k.spill[si];
-            sr.a = ra;
-            sr.b = *reinterpret_cast<const uint4 *>(&rb);
-            sr.cell = (int)key;
+    bool spilled = false;
+    if (valid) {
+        const unsigned j = slot0 + (unsigned)__popc(peers & ((1u << lane) - 1u));
+        uint4 ra;
+        float4 rb;
+        Split32::pack(p, ra, rb);
+        const int4 km = P.cells.meta[key];
+        const unsigned room = (unsigned)km.y - min((unsigned)km.y, P.cells.bot[P.cin][key] + P.cells.top[P.cin][key]);
+        if (j < room) {
+            const unsigned dst = (unsigned)(km.x + km.y) - 1u - j;
+            reinterpret_cast<uint4 *>(P.parts.A[P.cur ^ 1])[dst] = ra;
+            reinterpret_cast<float4 *>(P.parts.B[P.cur ^ 1])[dst] = rb;
         } else {
-            err |= DSMC_EBIT_SPILL_FULL;
+            spilled = true;
+            const unsigned si = atomicAdd(&P.status->spill, 1u);
+            if (si < P.parts.spill_cap) {
+                SpillRec &sr = P.parts.spill[si];
+                sr.a = ra;
+                sr.b = *reinterpret_cast<const uint4 *>(&rb);
+                sr.cell = (int)key;
+            } else {
+                err |= DSMC_EBIT_SPILL_FULL;
+            }
         }
     }
+    // spilled slots are given back: the counter ends at the placed count
+    const unsigned over = __ballot_sync(0xffffffffu, spilled) & peers;
+    if (valid && lane == leader && over) atomicSub(&top_out[key], (unsigned)__popc(over));
 }
 
 // Runs the general mover on the queued particles, one per lane, and places
 // them; its counts go to the warp's shared tally.  All lanes call.
-__device__ __noinline__ void drain_queue(const SysDev *gp, SlowRec *q, int *qn_p, unsigned *wtally, int lane,
-                                         uint32_t move_step, Sink k) {
-    const SysDev &g = *gp;
+__device__ __noinline__ void drain_queue(const PassParams &P, int sys, SlowRec *q, int *qn_p, unsigned *wtally,
+                                         int lane, uint32_t move_step) {
+    const SysDev &g = P.sys[sys];
     const int qn = *qn_p;
     const bool valid = lane < qn;
     Split32::Particle p;
@@ -224,7 +223,7 @@ __device__ __noinline__ void drain_queue(const SysDev *gp, SlowRec *q, int *qn_p
         }
     }
     __syncwarp();
-    insert(k, p, valid, key, lane, -1, make_int4(0, 0, 0, 0), mt.err);
+    insert_top(P, p, valid, key, lane, mt.err);
     const unsigned wh = __reduce_add_sync(0xffffffffu, (unsigned)mt.wall_hits);
     const unsigned rs = __reduce_add_sync(0xffffffffu, (unsigned)mt.reseeds);
     const int c0 = __reduce_add_sync(0xffffffffu, mt.cross[0]);
@@ -245,147 +244,193 @@ __device__ __noinline__ void drain_queue(const SysDev *gp, SlowRec *q, int *qn_p
     __syncwarp();
 }
 
-// The NTC collide of one staged cell by lane 0 (ranks by the whole warp).
+// The NTC collide of one staged cell by lane 0.  The warp first ranks the
+// cell's particles by id (the cell-list order of the reference's canonical
+// member order); perm[rank] is the ring slot of that particle.
+template <int R>
 __device__ __noinline__ unsigned collide_cell(uint64_t seed, int cell_global, uint32_t step, int n, int pairs,
-                                              double *vr_max, float4 *SB, uint16_t *perm, int lane) {
+                                              double *vr_max, float4 *ring_b, int start, uint16_t *perm, int lane) {
     for (int q = lane; q < n; q += 32) {
-        const uint32_t mine = __float_as_uint(SB[q].w);
+        int sq = start + q;
+        if (sq >= R) sq -= R;
+        const uint32_t mine = __float_as_uint(ring_b[sq].w);
         int rank = 0;
-        for (int r = 0; r < n; ++r) rank += __float_as_uint(SB[r].w) < mine;
-        perm[rank] = (uint16_t)q;
+        int sr = start;
+        for (int r = 0; r < n; ++r) {
+            rank += __float_as_uint(ring_b[sr].w) < mine;
+            if (++sr == R) sr = 0;
+        }
+        perm[rank] = (uint16_t)sq;
     }
     __syncwarp();
     unsigned long long col = 0;
     if (lane == 0) {
         SmemVel vel;
-        vel.b = SB;
+        vel.b = ring_b;
         ntc_run<float>(seed, cell_global, step, n, pairs, *vr_max, vel, perm, col);
     }
     __syncwarp();
     return (unsigned)col;
 }
 
-template <int CAP>
-__global__ void __launch_bounds__(256, 3) fused_split_kernel(PassParams P) {
+constexpr int FUSED_WARPS = 4;  // warps per block of the pipelined pass
+
+template <int R>
+__global__ void __launch_bounds__(32 * FUSED_WARPS, 5) fused_split_kernel(const __grid_constant__ PassParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     typedef Split32::Particle Particle;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const int warps_per_block = blockDim.x >> 5;
     const volatile Status *vs = P.status;
     if (vs->halted) return;
     const uint32_t step = vs->step;
     const uint32_t move_step = step + 1;
 
-    WarpSmem<CAP> &W = reinterpret_cast<WarpSmem<CAP> *>(smem_raw)[wib];
-    if (lane == 0) {
-        mbar_init(&W.bar[0]);
-        mbar_init(&W.bar[1]);
-        W.qn = 0;
-        fence_mbar_init();
-    }
-    __syncwarp();
+    WarpSmem<R> &W = reinterpret_cast<WarpSmem<R> *>(smem_raw)[wib];
+    if (lane == 0) W.qn = 0;
+    if (lane < 8) W.wtally[lane] = 0;
 
     const uint4 *Ain = reinterpret_cast<const uint4 *>(P.parts.A[P.cur]);
     const float4 *Bin = reinterpret_cast<const float4 *>(P.parts.B[P.cur]);
-    unsigned *cnt_in = P.cells.count[P.cur];
-    Sink sink;
-    sink.cnt_out = P.cells.count[P.cur ^ 1];
-    sink.Aout = reinterpret_cast<uint4 *>(P.parts.A[P.cur ^ 1]);
-    sink.Bout = reinterpret_cast<float4 *>(P.parts.B[P.cur ^ 1]);
-    sink.meta = P.cells.meta;
-    sink.status = P.status;
-    sink.spill = P.parts.spill;
-    sink.spill_cap = P.parts.spill_cap;
-    if (lane < 8) W.wtally[lane] = 0;
+    uint4 *Aout = reinterpret_cast<uint4 *>(P.parts.A[P.cur ^ 1]);
+    float4 *Bout = reinterpret_cast<float4 *>(P.parts.B[P.cur ^ 1]);
 
     LaneTally t;
     lane_tally_reset(t);
     t.sys = -1;
 
     const int C = P.cells.num_cells;
-    const int stride = gridDim.x * warps_per_block;
-    int a = blockIdx.x * warps_per_block + wib;
+    const int nchunks = (C + 31) >> 5;
+    const int wstride = gridDim.x * FUSED_WARPS;
+    const int chunk0 = blockIdx.x * FUSED_WARPS + wib;
 
-    // Lane 0 stages a cell: metadata into shared memory, then one bulk copy
-    // each of its records and its fp64 state.
-    int4 m_pf = make_int4(0, 0, 0, 0);  // lane 0: metadata of the cell to issue next
-    unsigned n_pf = 0;
-    auto load_meta = [&](int cell) {
-        if (lane == 0 && cell < C) {
-            m_pf = P.cells.meta[cell];
-            n_pf = min(min(cnt_in[cell], (unsigned)m_pf.y), (unsigned)CAP);
+    // Lane i: cell i of chunk `ch` into table b, with this step's NTC
+    // selection (Cell::prepare, dsmc/cell.cpp:42-50).
+    auto load_tab = [&](int b, int ch) {
+        CellTab &T = W.tab[b];
+        const int first = ch * 32;
+        const int ncell = ch < nchunks ? min(32, C - first) : 0;
+        if (lane == 0) {
+            T.first = first;
+            T.ncell = ncell;
+        }
+        if (lane < ncell) {
+            const int a = first + lane;
+            const int4 m = P.cells.meta[a];
+            const unsigned nb = min(P.cells.bot[P.cin][a], (unsigned)m.y);
+            const unsigned nt = min(P.cells.top[P.cin][a], (unsigned)m.y - nb);
+            const double4 st = P.cells.state[a];
+            double rest = st.y;
+            int pairs = 0;
+            if (P.do_collide) {
+                pairs = ntc_select(st.z, (int)(nb + nt), st.x, rest);
+                if (nb + nt < 2) pairs = 0;
+            }
+            if (nb + nt > (unsigned)R) atomicOr(&P.status->error, DSMC_EBIT_SMEM);  // the host sizes R above every cap
+            T.base[lane] = m.x;
+            T.cap[lane] = m.y;
+            T.nb[lane] = nb;
+            T.nt[lane] = nt;
+            T.glob[lane] = m.z;
+            T.sys[lane] = m.w;
+            T.pairs[lane] = pairs;
+            T.vr[lane] = st.x;
+            T.rest[lane] = rest;
         }
     };
-    auto issue = [&](int stage, int cell) {
-        fence_proxy_async();
-        W.meta[stage] = m_pf;
-        W.n[stage] = (int)n_pf;
-        const uint32_t bytes = n_pf * 16u;
-        const void *srcA = Ain + m_pf.x, *srcB = Bin + m_pf.x, *srcS = P.cells.state + cell;
-        // every operand is 16-byte aligned by construction; a violation is
-        // recorded and the transfer skipped rather than issued
-        if (!aligned16(srcA) || !aligned16(srcB) || !aligned16(srcS) || !aligned16(&W.A[stage][0]) ||
-            !aligned16(&W.B[stage][0]) || !aligned16(&W.cs[stage])) {
-            atomicOr(&P.status->error, DSMC_EBIT_ALIGN);
-            W.n[stage] = 0;
-            mbar_arrive_expect(&W.bar[stage], 0u);
-            return;
-        }
-        mbar_arrive_expect(&W.bar[stage], 2u * bytes + (uint32_t)sizeof(double4));
-        bulk_g2s(&W.cs[stage], srcS, (uint32_t)sizeof(double4), &W.bar[stage]);
-        if (n_pf) {
-            bulk_g2s(&W.A[stage][0], srcA, bytes, &W.bar[stage]);
-            bulk_g2s(&W.B[stage][0], srcB, bytes, &W.bar[stage]);
+    // Lane i: occupancy and cell state of cell i of table b for the next pass.
+    auto write_tab = [&](int b, unsigned nfs) {
+        const CellTab &T = W.tab[b];
+        if (lane < T.ncell) {
+            const int a = T.first + lane;
+            P.cells.bot[P.cout][a] = nfs;
+            P.cells.bot[P.cclear][a] = 0;
+            P.cells.top[P.cclear][a] = 0;
+            if (P.do_collide) *reinterpret_cast<double2 *>(&P.cells.state[a]) = make_double2(T.vr[lane], T.rest[lane]);
         }
     };
-    load_meta(a);
-    if (lane == 0 && a < C) issue(0, a);
-    load_meta(a + stride);
 
-    uint32_t parity = 0;
-    bool ok = true;
-    for (int k = 0; a < C; a += stride, ++k) {
-        const int s = k & 1;
-        const int a_nxt = a + stride;
-        if (lane == 0 && a_nxt < C) issue(s ^ 1, a_nxt);
-        load_meta(a_nxt + stride);
+    load_tab(0, chunk0);
+    load_tab(1, chunk0 + wstride);
+    __syncwarp();
 
-        if (!mbar_wait(&W.bar[s], (parity >> s) & 1u)) {
-            ok = false;
-            break;
+    // ring (warp-uniform): slots [tail, tail + used) hold the staged cells,
+    // the cell in work first
+    int head = 0, tail = 0, used = 0;
+    int it = 0, ii = 0;     // next cell to stage: chunk ordinal, cell in chunk
+    int ct = 0, ci = 0;     // cell in work
+    int ahead = 0;          // cells staged, the one in work included
+    unsigned nfs_mine = 0;  // lane i: bottom occupancy written for cell i of the chunk in work
+
+    // Stage cells ahead while the ring has room (warp-uniform control flow:
+    // every lane commits one group per staged cell).
+    auto stage_ahead = [&]() {
+        // (it, ii) moves past a full chunk as soon as its last cell is
+        // staged, so ii >= ncell only past the warp's last cell
+        while (ahead <= DEPTH && it <= ct + 1) {
+            const CellTab &T = W.tab[it & 1];
+            if (ii >= T.ncell) return;
+            const unsigned nb = T.nb[ii], nt = T.nt[ii];
+            const int n = (int)min(nb + nt, (unsigned)R);
+            if (used + n > R) return;
+            const int base = T.base[ii];
+            const int top0 = base + T.cap[ii] - (int)nt;
+            for (int q = lane; q < n; q += 32) {
+                const int slot = q < (int)nb ? base + q : top0 + (q - (int)nb);
+                int r = head + q;
+                if (r >= R) r -= R;
+                cp_async16(&W.A[r], Ain + slot);
+                cp_async16(&W.B[r], Bin + slot);
+            }
+            cp_async_commit();
+            head += n;
+            if (head >= R) head -= R;
+            used += n;
+            ++ahead;
+            if (++ii == 32) {
+                ++it;
+                ii = 0;
+            }
         }
-        parity ^= 1u << s;
+    };
+
+    while (true) {
+        const CellTab &T = W.tab[ct & 1];
+        if (ci >= T.ncell) {
+            // chunk finished: publish its cells, load the chunk two ahead
+            if (T.ncell > 0) write_tab(ct & 1, nfs_mine);
+            if (T.ncell < 32) break;  // that was the warp's last chunk
+            __syncwarp();
+            load_tab(ct & 1, chunk0 + (ct + 2) * wstride);
+            __syncwarp();
+            ++ct;
+            ci = 0;
+            continue;
+        }
+        stage_ahead();  // the cell in work is staged once this returns
+        cp_async_wait(ahead - 1);
         __syncwarp();
-        const int4 m = W.meta[s];
-        const int n = W.n[s];
-        const int sys = m.w;
+
+        const int a = T.first + ci;
+        const int n = (int)min(T.nb[ci] + T.nt[ci], (unsigned)R);
+        const int base = T.base[ci];
+        const int sys = T.sys[ci];
+        const int pairs = T.pairs[ci];
         if (sys != t.sys) {
-            if (W.qn) drain_queue(P.sys + t.sys, W.q, &W.qn, W.wtally, lane, move_step, sink);
+            if (W.qn) drain_queue(P, t.sys, W.q, &W.qn, W.wtally, lane, move_step);
             if (t.sys >= 0) flush_warp(P, W, t, lane);
             t.sys = sys;
         }
         const SysDev &g = P.sys[sys];
-        uint4 *SA = W.A[s];
-        float4 *SB = W.B[s];
 
-        // ---- collide: Cell::prepare + Cell::collide (dsmc/cell.cpp:42-111)
-        if (P.do_collide) {
-            int pairs = 0;
+        // ---- collide: Cell::collide (dsmc/cell.cpp:52-111)
+        if (pairs > 0) {
+            const unsigned col = collide_cell<R>(g.seed, T.glob[ci], step, n, pairs, &W.tab[ct & 1].vr[ci], W.B,
+                                                 tail, W.perm, lane);
             if (lane == 0) {
-                double4 &cs = W.cs[s];
-                pairs = ntc_select(cs.z, n, cs.x, cs.y);
-                if (n < 2) pairs = 0;
+                t.collisions += col;
+                t.candidates += (unsigned)pairs;
             }
-            pairs = __shfl_sync(0xffffffffu, pairs, 0);
-            if (pairs > 0) {
-                const unsigned col = collide_cell(g.seed, m.z, step, n, pairs, &W.cs[s].x, SB, W.perm, lane);
-                if (lane == 0) {
-                    t.collisions += col;
-                    t.candidates += (unsigned)pairs;
-                }
-            }
-            if (lane == 0) P.cells.state[a] = W.cs[s];
         }
 
         // ---- sample: cell moments in fp64 on the reference's cadence
@@ -393,7 +438,9 @@ __global__ void __launch_bounds__(256, 3) fused_split_kernel(PassParams P) {
             step >= (uint32_t)g.sample_begin) {
             double m1[3] = {0, 0, 0}, m2[3] = {0, 0, 0};
             for (int q = lane; q < n; q += 32) {
-                const float4 b = SB[q];
+                int r = tail + q;
+                if (r >= R) r -= R;
+                const float4 b = W.B[r];
                 const double x = b.x, y = b.y, z = b.z;
                 m1[0] += x;
                 m1[1] += y;
@@ -420,17 +467,20 @@ __global__ void __launch_bounds__(256, 3) fused_split_kernel(PassParams P) {
                 if (a == g.active_begin) atomicAdd(&P.tally[sys].samples, 1ull);
             }
         }
-        if (lane == 0) cnt_in[a] = 0;
 
-        // ---- accelerate + move; particles that stay in their voxel are
-        // placed at once, the rest queue for the general mover
-        for (int ch = 0; ch * 32 < n; ++ch) {
-            const int q = ch * 32 + lane;
+        // ---- accelerate + move.  Particles that stay in their voxel keep
+        // their cell and go to its bottom segment, in order, without atomics;
+        // the rest queue for the general mover and a top slot.
+        unsigned n_fs = 0;
+        for (int c0 = 0; c0 < n; c0 += 32) {
+            const int q = c0 + lane;
             const bool valid = q < n;
             Particle p;
             bool stay = false;
             if (valid) {
-                Split32::unpack(SA[q], SB[q], p);
+                int r = tail + q;
+                if (r >= R) r -= R;
+                Split32::unpack(W.A[r], W.B[r], p);
                 Split32::accelerate(g, p);
                 if (!p.flag) {
                     float x[3];
@@ -446,33 +496,42 @@ __global__ void __launch_bounds__(256, 3) fused_split_kernel(PassParams P) {
                         p.o[2] = x[2];
                     }
                 }
-                t.moved += 1;
             }
+            const unsigned fast = __ballot_sync(0xffffffffu, valid && stay);
             const unsigned slow = __ballot_sync(0xffffffffu, valid && !stay);
+            if (valid && stay) {
+                const unsigned dst = (unsigned)base + n_fs + (unsigned)__popc(fast & ((1u << lane) - 1u));
+                uint4 ra;
+                float4 rb;
+                Split32::pack(p, ra, rb);
+                Aout[dst] = ra;
+                Bout[dst] = rb;
+            }
+            n_fs += (unsigned)__popc(fast);
             if (slow) {
-                if (W.qn + __popc(slow) > QCAP) drain_queue(&g, W.q, &W.qn, W.wtally, lane, move_step, sink);
+                if (W.qn + __popc(slow) > QCAP) drain_queue(P, sys, W.q, &W.qn, W.wtally, lane, move_step);
                 if (valid && !stay) {
-                    SlowRec &r = W.q[W.qn + __popc(slow & ((1u << lane) - 1u))];
-                    Split32::pack(p, r.a, r.b);
-                    r.cell = a;
-                    r.global = m.z;
+                    SlowRec &rec = W.q[W.qn + __popc(slow & ((1u << lane) - 1u))];
+                    Split32::pack(p, rec.a, rec.b);
+                    rec.cell = a;
+                    rec.global = T.glob[ci];
                 }
                 __syncwarp();
                 if (lane == 0) W.qn += __popc(slow);
                 __syncwarp();
             }
-            const bool place = valid && stay;
-            insert(sink, p, place, place ? (unsigned)a : 0xffffffffu, lane, a, m, t.err);
         }
+        if (lane == ci) nfs_mine = n_fs;
+        if (lane == 0) t.moved += (unsigned)n;
+        // free the cell's ring slots once every lane is done with them
         __syncwarp();
+        tail += n;
+        if (tail >= R) tail -= R;
+        used -= n;
+        --ahead;
+        ++ci;
     }
-    if (!ok) {
-        if (lane == 0) atomicOr(&P.status->error, DSMC_EBIT_TIMEOUT);
-        mbar_wait(&W.bar[0], parity & 1u);
-        mbar_wait(&W.bar[1], (parity >> 1) & 1u);
-    } else if (W.qn) {
-        drain_queue(P.sys + t.sys, W.q, &W.qn, W.wtally, lane, move_step, sink);
-    }
+    if (W.qn) drain_queue(P, t.sys, W.q, &W.qn, W.wtally, lane, move_step);
     if (t.sys >= 0) flush_warp(P, W, t, lane);
 
     __syncthreads();
@@ -489,7 +548,7 @@ __global__ void __launch_bounds__(256, 3) fused_split_kernel(PassParams P) {
     }
 }
 
-template <int CAP> size_t fused_smem_bytes(int warps) { return sizeof(WarpSmem<CAP>) * warps; }
+template <int R> size_t fused_smem_bytes() { return sizeof(WarpSmem<R>) * FUSED_WARPS; }
 
 }  // namespace fused
 }  // namespace dsmc

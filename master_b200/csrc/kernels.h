@@ -18,16 +18,18 @@ namespace dsmc {
                                  cudaStream_t st);                                                              \
     cudaError_t launch_init(const SysDev *sys, int s, double sqrt_t_over_m, long long n, void *A, void *B,     \
                             int *key, unsigned *hist, unsigned *err, cudaStream_t st);                          \
-    cudaError_t launch_gather(const CellArrays &cells, const ParticleArrays &parts, int cur, int c0, int c1,   \
+    cudaError_t launch_gather(const CellArrays &cells, const ParticleArrays &parts, int cur, int cin, int c0,   \
+                              int c1,                                                                           \
                               unsigned nspill, void *A, void *B, int *key, unsigned *hist,                      \
                               unsigned long long *cursor, unsigned long long limit, unsigned *err,               \
                               cudaStream_t st);                                                                  \
-    cudaError_t launch_insert(const CellArrays &cells, const ParticleArrays &parts, int cur, long long n,      \
+    cudaError_t launch_insert(const CellArrays &cells, const ParticleArrays &parts, int cur, int cin, long long n, \
                               const void *A, const void *B, const int *key, unsigned *err, cudaStream_t st);    \
     cudaError_t launch_to_fp64(const SysDev *sys, int s, const CellArrays &cells, const ParticleArrays &parts, \
-                               int cur, uint32_t id_base, long long cap, double *r, double *v, int *cell,      \
+                               int cur, int cin, uint32_t id_base, long long cap, double *r, double *v, int *cell, \
                                unsigned *err, cudaStream_t st);                                                 \
-    cudaError_t launch_cell_energy(const CellArrays &cells, const ParticleArrays &parts, int cur, int c0, int c1,  \
+    cudaError_t launch_cell_energy(const CellArrays &cells, const ParticleArrays &parts, int cur, int cin, int c0,  \
+                                   int c1,                                                                      \
                                    double *out, cudaStream_t st);                                               \
     }
 
@@ -36,7 +38,8 @@ DSMC_DECLARE_LAUNCHERS(fp64)
 
 namespace split32 {
 // the bulk-copy pipelined production pass (fused_split.cuh)
-int fused_capacity(int smem_cap);   // 0: no instantiation holds smem_cap
+int fused_capacity(int smem_cap);   // ring slots per warp; 0: no instantiation holds smem_cap
+int fused_block();                  // threads per block of the pipelined pass
 int fused_blocks_per_sm(int smem_cap);
 cudaError_t launch_fused(const PassParams &P, int grid, cudaStream_t st);
 }  // namespace split32

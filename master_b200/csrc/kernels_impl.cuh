@@ -107,7 +107,7 @@ __global__ void k_init(const SysDev *sys, int s, double sqrt_t_over_m, long long
 }
 
 // Slots of buffer `cur` (cells [c0, c1)) and the overflow list -> flat records.
-__global__ void k_gather(const CellArrays cells, const ParticleArrays parts, int cur, int c0, int c1,
+__global__ void k_gather(const CellArrays cells, const ParticleArrays parts, int cur, int cin, int c0, int c1,
                          unsigned nspill, RecA *A, RecB *B, int *key, unsigned *hist, unsigned long long *cursor,
                          unsigned long long limit, unsigned *err) {
     const int lane = threadIdx.x & 31;
@@ -117,7 +117,9 @@ __global__ void k_gather(const CellArrays cells, const ParticleArrays parts, int
     const RecB *Bin = reinterpret_cast<const RecB *>(parts.B[cur]);
     for (int a = c0 + warp; a < c1; a += nwarps) {
         const int4 m = cells.meta[a];
-        const unsigned n = min(cells.count[cur][a], (unsigned)m.y);
+        const unsigned nb = min(cells.bot[cin][a], (unsigned)m.y);
+        const unsigned nt = min(cells.top[cin][a], (unsigned)m.y - nb);
+        const unsigned n = nb + nt;
         unsigned long long at = 0;
         if (lane == 0 && n) at = atomicAdd(cursor, (unsigned long long)n);
         at = __shfl_sync(0xffffffffu, at, 0);
@@ -126,8 +128,9 @@ __global__ void k_gather(const CellArrays cells, const ParticleArrays parts, int
             continue;
         }
         for (unsigned s = lane; s < n; s += 32) {
-            A[at + s] = Ain[m.x + s];
-            B[at + s] = Bin[m.x + s];
+            const unsigned addr = cell_slot(m.x, m.y, nb, nt, s);
+            A[at + s] = Ain[addr];
+            B[at + s] = Bin[addr];
             key[at + s] = a;
         }
         if (lane == 0 && n) atomicAdd(&hist[a], n);
@@ -154,15 +157,15 @@ __global__ void k_gather(const CellArrays cells, const ParticleArrays parts, int
 }
 
 // Flat records -> slots of buffer `cur` (counts must start at zero).
-__global__ void k_insert(const CellArrays cells, const ParticleArrays parts, int cur, long long n, const RecA *A,
-                         const RecB *B, const int *key, unsigned *err) {
+__global__ void k_insert(const CellArrays cells, const ParticleArrays parts, int cur, int cin, long long n,
+                         const RecA *A, const RecB *B, const int *key, unsigned *err) {
     RecA *Aout = reinterpret_cast<RecA *>(parts.A[cur]);
     RecB *Bout = reinterpret_cast<RecB *>(parts.B[cur]);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         const int a = key[i];
         if (a < 0) continue;
         const int4 m = cells.meta[a];
-        const unsigned slot = atomicAdd(&cells.count[cur][a], 1u);
+        const unsigned slot = atomicAdd(&cells.bot[cin][a], 1u);
         if (slot >= (unsigned)m.y) {
             atomicOr(err, DSMC_EBIT_SPILL_FULL);
             continue;
@@ -174,7 +177,7 @@ __global__ void k_insert(const CellArrays cells, const ParticleArrays parts, int
 
 // Slots of one system -> fp64 state ordered by id (dsmc/dsmc_io.cpp:98-113 layout).
 __global__ void k_to_fp64(const SysDev *sys, int s, const CellArrays cells, const ParticleArrays parts, int cur,
-                          uint32_t id_base, long long cap, double *r, double *v, int *cell, unsigned *err) {
+                          int cin, uint32_t id_base, long long cap, double *r, double *v, int *cell, unsigned *err) {
     const SysDev &g = sys[s];
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -183,10 +186,12 @@ __global__ void k_to_fp64(const SysDev *sys, int s, const CellArrays cells, cons
     const RecB *Bin = reinterpret_cast<const RecB *>(parts.B[cur]);
     for (int a = g.active_begin + warp; a < g.active_end; a += nwarps) {
         const int4 m = cells.meta[a];
-        const unsigned n = min(cells.count[cur][a], (unsigned)m.y);
-        for (unsigned q = lane; q < n; q += 32) {
+        const unsigned nb = min(cells.bot[cin][a], (unsigned)m.y);
+        const unsigned nt = min(cells.top[cin][a], (unsigned)m.y - nb);
+        for (unsigned q = lane; q < nb + nt; q += 32) {
             Particle p;
-            Prec::unpack(Ain[m.x + q], Bin[m.x + q], p);
+            const unsigned addr = cell_slot(m.x, m.y, nb, nt, q);
+            Prec::unpack(Ain[addr], Bin[addr], p);
             const long long i = (long long)p.id - (long long)id_base;
             if (i < 0 || i >= cap) {
                 atomicOr(err, DSMC_EBIT_CELL);
@@ -205,7 +210,7 @@ __global__ void k_to_fp64(const SysDev *sys, int s, const CellArrays cells, cons
 
 // Sum of |v|^2 over each cell's particles (MeasureEnergy's sum,
 // dsmc/statisticalproperty.cpp:21-41), one fp64 value per cell.
-__global__ void k_cell_energy(const CellArrays cells, const ParticleArrays parts, int cur, int c0, int c1,
+__global__ void k_cell_energy(const CellArrays cells, const ParticleArrays parts, int cur, int cin, int c0, int c1,
                               double *out) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -213,10 +218,11 @@ __global__ void k_cell_energy(const CellArrays cells, const ParticleArrays parts
     const RecB *Bin = reinterpret_cast<const RecB *>(parts.B[cur]);
     for (int a = c0 + warp; a < c1; a += nwarps) {
         const int4 m = cells.meta[a];
-        const unsigned n = min(cells.count[cur][a], (unsigned)m.y);
+        const unsigned nb = min(cells.bot[cin][a], (unsigned)m.y);
+        const unsigned nt = min(cells.top[cin][a], (unsigned)m.y - nb);
         double e = 0;
-        for (unsigned q = lane; q < n; q += 32) {
-            const RecB b = Bin[m.x + q];
+        for (unsigned q = lane; q < nb + nt; q += 32) {
+            const RecB b = Bin[cell_slot(m.x, m.y, nb, nt, q)];
             const double x = (double)b.x, y = (double)b.y, z = (double)b.z;
             e += x * x + y * y + z * z;
         }
@@ -290,30 +296,30 @@ cudaError_t launch_init(const SysDev *sys, int s, double sqrt_t_over_m, long lon
     return cudaGetLastError();
 }
 
-cudaError_t launch_gather(const CellArrays &cells, const ParticleArrays &parts, int cur, int c0, int c1,
+cudaError_t launch_gather(const CellArrays &cells, const ParticleArrays &parts, int cur, int cin, int c0, int c1,
                           unsigned nspill, void *A, void *B, int *key, unsigned *hist, unsigned long long *cursor,
                           unsigned long long limit, unsigned *err, cudaStream_t st) {
-    k_gather<<<148 * 8, 256, 0, st>>>(cells, parts, cur, c0, c1, nspill, (RecA *)A, (RecB *)B, key, hist, cursor,
+    k_gather<<<148 * 8, 256, 0, st>>>(cells, parts, cur, cin, c0, c1, nspill, (RecA *)A, (RecB *)B, key, hist, cursor,
                                       limit, err);
     return cudaGetLastError();
 }
 
-cudaError_t launch_insert(const CellArrays &cells, const ParticleArrays &parts, int cur, long long n, const void *A,
-                          const void *B, const int *key, unsigned *err, cudaStream_t st) {
-    k_insert<<<grid_for(n, 256), 256, 0, st>>>(cells, parts, cur, n, (const RecA *)A, (const RecB *)B, key, err);
+cudaError_t launch_insert(const CellArrays &cells, const ParticleArrays &parts, int cur, int cin, long long n,
+                          const void *A, const void *B, const int *key, unsigned *err, cudaStream_t st) {
+    k_insert<<<grid_for(n, 256), 256, 0, st>>>(cells, parts, cur, cin, n, (const RecA *)A, (const RecB *)B, key, err);
     return cudaGetLastError();
 }
 
 cudaError_t launch_to_fp64(const SysDev *sys, int s, const CellArrays &cells, const ParticleArrays &parts, int cur,
-                           uint32_t id_base, long long cap, double *r, double *v, int *cell, unsigned *err,
+                           int cin, uint32_t id_base, long long cap, double *r, double *v, int *cell, unsigned *err,
                            cudaStream_t st) {
-    k_to_fp64<<<148 * 8, 256, 0, st>>>(sys, s, cells, parts, cur, id_base, cap, r, v, cell, err);
+    k_to_fp64<<<148 * 8, 256, 0, st>>>(sys, s, cells, parts, cur, cin, id_base, cap, r, v, cell, err);
     return cudaGetLastError();
 }
 
-cudaError_t launch_cell_energy(const CellArrays &cells, const ParticleArrays &parts, int cur, int c0, int c1,
+cudaError_t launch_cell_energy(const CellArrays &cells, const ParticleArrays &parts, int cur, int cin, int c0, int c1,
                                double *out, cudaStream_t st) {
-    k_cell_energy<<<148 * 8, 256, 0, st>>>(cells, parts, cur, c0, c1, out);
+    k_cell_energy<<<148 * 8, 256, 0, st>>>(cells, parts, cur, cin, c0, c1, out);
     return cudaGetLastError();
 }
 

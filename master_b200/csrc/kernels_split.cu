@@ -9,58 +9,60 @@
 namespace dsmc {
 namespace split32 {
 
-// The production pass: smallest staging capacity that holds every cell.
-template <int CAP> static cudaError_t launch_fused_cap(const PassParams &P, int grid, cudaStream_t st) {
-    const size_t smem = fused::fused_smem_bytes<CAP>(8);
-    fused::fused_split_kernel<CAP><<<grid, 256, smem, st>>>(P);
+// The production pass: the smallest ring that holds the largest cell.
+template <int R> static cudaError_t launch_fused_ring(const PassParams &P, int grid, cudaStream_t st) {
+    fused::fused_split_kernel<R><<<grid, 32 * fused::FUSED_WARPS, fused::fused_smem_bytes<R>(), st>>>(P);
     return cudaGetLastError();
 }
-template <int CAP> static int fused_cap_blocks() {
-    const size_t smem = fused::fused_smem_bytes<CAP>(8);
+template <int R> static int fused_ring_blocks() {
+    const size_t smem = fused::fused_smem_bytes<R>();
     // the opt-in limit is a property of the function, shared by every
     // context: raise it to the device maximum, never lower it
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaFuncAttributes fa;
-    if (cudaFuncGetAttributes(&fa, fused::fused_split_kernel<CAP>) != cudaSuccess) return 0;
+    if (cudaFuncGetAttributes(&fa, fused::fused_split_kernel<R>) != cudaSuccess) return 0;
     if (smem + fa.sharedSizeBytes > (size_t)optin) return 0;
-    if (cudaFuncSetAttribute(fused::fused_split_kernel<CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(fused::fused_split_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              optin - (int)fa.sharedSizeBytes) != cudaSuccess)
         return 0;
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fused::fused_split_kernel<CAP>, 256, smem) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fused::fused_split_kernel<R>, 32 * fused::FUSED_WARPS,
+                                                      smem) != cudaSuccess)
         return 0;
     return nb;
 }
 
+// Ring slots per warp of the production pass for cells of at most
+// `smem_cap` slots (0: no ring is large enough).
 int fused_capacity(int smem_cap) {
-    if (smem_cap <= 64) return 64;
-    if (smem_cap <= 96) return 96;
-    if (smem_cap <= 128) return 128;
-    if (smem_cap <= 192) return 192;
-    if (smem_cap <= 256) return 256;
+    static const int rings[] = {64, 96, 128, 160, 192, 224, 256};
+    for (int r : rings)
+        if (smem_cap <= r) return r;
     return 0;
 }
 
+int fused_block() { return 32 * fused::FUSED_WARPS; }
+
+#define DSMC_FUSED_RINGS(X) X(64) X(96) X(128) X(160) X(192) X(224) X(256)
+
 int fused_blocks_per_sm(int smem_cap) {
     switch (fused_capacity(smem_cap)) {
-        case 64: return fused_cap_blocks<64>();
-        case 96: return fused_cap_blocks<96>();
-        case 128: return fused_cap_blocks<128>();
-        case 192: return fused_cap_blocks<192>();
-        case 256: return fused_cap_blocks<256>();
+#define X(r) \
+    case r: return fused_ring_blocks<r>();
+        DSMC_FUSED_RINGS(X)
+#undef X
     }
     return 0;
 }
 
 cudaError_t launch_fused(const PassParams &P, int grid, cudaStream_t st) {
     switch (fused_capacity(P.smem_cap)) {
-        case 64: return launch_fused_cap<64>(P, grid, st);
-        case 96: return launch_fused_cap<96>(P, grid, st);
-        case 128: return launch_fused_cap<128>(P, grid, st);
-        case 192: return launch_fused_cap<192>(P, grid, st);
-        case 256: return launch_fused_cap<256>(P, grid, st);
+#define X(r) \
+    case r: return launch_fused_ring<r>(P, grid, st);
+        DSMC_FUSED_RINGS(X)
+#undef X
     }
     return cudaErrorInvalidValue;
 }

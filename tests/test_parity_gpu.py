@@ -209,19 +209,28 @@ def test_geometry_gpu_matches_cpu():
         assert np.array_equal(getattr(a, k), getattr(b, k)), k
 
 
-def test_fused_equals_stages_dense_cells():
-    """~40 particles per cell: the pipelined pass with a 128-particle staging
-    capacity (above the default 48 KB shared-memory window) against the
-    stage kernels."""
+@pytest.mark.parametrize("capacity", [None, (1.3, 0)])
+def test_fused_equals_stages_dense_cells(capacity):
+    """~40 particles per cell: the pipelined pass against the stage kernels.
+    The default capacity gives a ring of at least 128 slots per warp; with
+    tight capacity the ring holds fewer than three of the largest cells, so
+    staging stops on a full ring, and cells overflow into the spill list."""
     from master_b200 import workloads
     w = workloads.Workload("dense32", n=32, radius_voxels=3, porosity=0.5, geometry_seed=3, cells=16,
                            atoms_per_molecule=workloads.simulators_per_cell_weight(2.5e24, 0.1, 2, 40))
     s = w.settings(rng_seed=99, statistics_interval=1)
     g = w.geometry()
     A = System(s, g)
+    if capacity:
+        A.ctx.check(A.ctx.lib.dsmc_ctx_set_capacity(A.ctx.handle, *capacity))
+        A.set_particles(*A.get_particles())  # re-lay the cells out at the tight capacity
     B = System(s, g)
     info = A.ctx.pass_info()
-    assert info["pipelined"] == 1 and info["stage_capacity"] >= 128
+    assert info["pipelined"] == 1
+    if capacity is None:
+        assert info["stage_capacity"] >= 128
+    else:
+        assert info["stage_capacity"] < 3 * A.cells()["count"].max()
     A.step(4)
     for _ in range(4):
         B.accelerate_and_move()
