@@ -64,9 +64,15 @@ struct DrawStream {
         k = 0;
     }
     DSMC_HD void words(uint32_t &a, uint32_t &b) {
-        if ((k & 1u) == 0) philox4x32_10(id, step, tag, k >> 1, key0, key1, w);
-        a = w[2 * (k & 1u)];
-        b = w[2 * (k & 1u) + 1];
+        // constant indexes only, so the block stays in registers
+        if ((k & 1u) == 0) {
+            philox4x32_10(id, step, tag, k >> 1, key0, key1, w);
+            a = w[0];
+            b = w[1];
+        } else {
+            a = w[2];
+            b = w[3];
+        }
         ++k;
     }
     DSMC_HD double uniform64() {

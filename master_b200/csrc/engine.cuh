@@ -299,7 +299,12 @@ struct Split32 {
             if (!(dt > 1e-5f && depth < 10)) break;
         }
         p.flag = here != DSMC_VOX_EMPTY;
-        // Periodic wrap, one box length at most, counting net crossings.
+        wrap(g, p, t);
+    }
+
+    // Periodic wrap, one box length at most, counting net crossings
+    // (System::move, dsmc/system.cpp:107-120).
+    static __device__ __forceinline__ void wrap(const SysDev &g, Particle &p, MoveTally &t) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             if (p.c[d] >= g.n[d]) {
@@ -315,6 +320,27 @@ struct Split32 {
                 p.o[d] = 0.5f;
             }
         }
+    }
+
+    // The general mover's outcome when its first flight is all there is: a
+    // particle in an empty voxel whose full-dt flight ends in an empty voxel
+    // stops there (dsmc/moleculemover.cpp:74-77), then wraps.  Same arithmetic
+    // as move_general's first sub-step; false (p untouched) when the flight
+    // ends in a wall or boundary voxel or starts outside an empty one.
+    static __device__ __forceinline__ bool move_open(const SysDev &g, Particle &p, MoveTally &t) {
+        if (p.flag) return false;
+        int c[3] = {p.c[0], p.c[1], p.c[2]};
+        float o[3] = {p.o[0], p.o[1], p.o[2]};
+        const float w[3] = {p.v[0] * g.inv_vox_f[0], p.v[1] * g.inv_vox_f[1], p.v[2] * g.inv_vox_f[2]};
+        advance(c, o, w, g.dt_f);
+        if (voxel_type(g, c[0], c[1], c[2]) != DSMC_VOX_EMPTY) return false;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            p.c[d] = c[d];
+            p.o[d] = o[d];
+        }
+        wrap(g, p, t);
+        return true;
     }
 
     // The whole move.  A particle whose full-dt flight stays inside its
@@ -715,11 +741,9 @@ __device__ __forceinline__ void ntc_scatter(double &ax, double &ay, double &az, 
 // Cell::collide (dsmc/cell.cpp:75-111) over the members in id order, on
 // velocities staged in shared memory.  Run by one lane.  Draws: stream
 // (cell, step, collide), three per candidate and two more per collision.
-template <class real, class Vel>
-__device__ void ntc_run(uint64_t seed, int cell_global_index, uint32_t step, int n, int pairs, double &vr_max,
-                        Vel vel, const uint16_t *perm, unsigned long long &collisions) {
-    DrawStream rs;
-    rs.init(seed, (uint32_t)cell_global_index, step, DSMC_TAG_COLLIDE);
+template <class real, class Vel, class Draws>
+__device__ void ntc_loop(Draws &rs, int n, int pairs, double &vr_max, Vel vel, const uint16_t *perm,
+                         unsigned long long &collisions) {
     double crm = vr_max;
     const real vmax = (real)vr_max;
     for (int isel = 0; isel < pairs; ++isel) {
@@ -744,6 +768,13 @@ __device__ void ntc_run(uint64_t seed, int cell_global_index, uint32_t step, int
         }
     }
     vr_max = crm;
+}
+template <class real, class Vel>
+__device__ void ntc_run(uint64_t seed, int cell_global_index, uint32_t step, int n, int pairs, double &vr_max,
+                        Vel vel, const uint16_t *perm, unsigned long long &collisions) {
+    DrawStream rs;
+    rs.init(seed, (uint32_t)cell_global_index, step, DSMC_TAG_COLLIDE);
+    ntc_loop<real>(rs, n, pairs, vr_max, vel, perm, collisions);
 }
 
 template <class Prec> struct StageVel {

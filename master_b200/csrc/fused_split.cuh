@@ -64,7 +64,9 @@ struct SlowRec {
     int pad[2];
 };
 
-constexpr int QCAP = 32;
+constexpr int QCAP = 32;   // mover queue
+constexpr int WCAP = 16;   // wall queue
+enum { T_WALL, T_RESEED, T_CROSS0, T_CROSS1, T_CROSS2, T_STRANDED, T_ERR, T_COLL, T_CAND, T_MOVED, TALLY_N };
 
 // Per-chunk cell table: entry i describes cell first + i of the chunk.
 struct CellTab {
@@ -87,68 +89,38 @@ template <int R> struct WarpSmem {
     uint4 A[R];
     float4 B[R];
     CellTab tab[2];
-    SlowRec q[QCAP];
+    SlowRec q[QCAP];     // left their voxel: the open-flight mover first
+    SlowRec wq[WCAP];    // flight meets a wall: the general mover
+    uint4 blk[32];       // Philox blocks 0..31 of the collide stream of the cell in work
     uint16_t perm[R];
-    int qn;
-    unsigned wtally[8];  // wall hits, reseeds, crossings x3, stranded, error bits (drained particles)
+    int qn, wqn;
+    // the warp's counts since its last flush: wall hits, reseeds, crossings
+    // x3, stranded, error bits, collisions, candidates, particles moved
+    unsigned wtally[TALLY_N];
 };
 
-struct LaneTally {
-    unsigned collisions, candidates, wall_hits, reseeds, moved, stranded;
-    int cross[3];
-    unsigned err;
-    int sys;
-};
-
-__device__ __forceinline__ void lane_tally_reset(LaneTally &t) {
-    t.collisions = t.candidates = t.wall_hits = t.reseeds = t.moved = t.stranded = 0;
-    t.cross[0] = t.cross[1] = t.cross[2] = 0;
-    t.err = 0;
-}
-
-__device__ __forceinline__ unsigned warp_sum_u32(unsigned x) { return __reduce_add_sync(0xffffffffu, x); }
-
-__device__ __forceinline__ void flush_lane_tally(const PassParams &P, LaneTally &t, int lane) {
-    const unsigned long long col = warp_sum_u32(t.collisions), cand = warp_sum_u32(t.candidates);
-    const unsigned long long wh = warp_sum_u32(t.wall_hits), rs = warp_sum_u32(t.reseeds);
-    const unsigned long long mv = warp_sum_u32(t.moved), sd = warp_sum_u32(t.stranded);
-    int cr[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) cr[d] = __reduce_add_sync(0xffffffffu, t.cross[d]);
-    const unsigned err = __reduce_or_sync(0xffffffffu, t.err);
-    if (lane == 0 && t.sys >= 0) {
-        SysTally &T = P.tally[t.sys];
-        if (col) atomicAdd(&T.collisions, col);
-        if (cand) atomicAdd(&T.candidates, cand);
-        if (wh) atomicAdd(&T.wall_hits, wh);
-        if (rs) atomicAdd(&T.reseeds, rs);
-        if (mv) atomicAdd(&T.particle_steps, mv);
-        if (sd) atomicAdd(&T.stranded, sd);
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-            if (cr[d]) atomicAdd((unsigned long long *)&T.count_periodic[d], (unsigned long long)(long long)cr[d]);
-        if (err) atomicOr(&P.status->error, err);
-    }
-    lane_tally_reset(t);
-}
-
-// Folds the drained particles' counts (warp shared tally) into lane 0's
-// tally and publishes the warp's counts for its current system.
-template <int R> __device__ __forceinline__ void flush_warp(const PassParams &P, WarpSmem<R> &W, LaneTally &t, int lane) {
+// Publishes the warp's counts for system `sys` and clears them (lane 0).
+template <int R> __device__ void flush_warp(const PassParams &P, WarpSmem<R> &W, int sys, int lane) {
     __syncwarp();
-    if (lane == 0) {
-        t.wall_hits += W.wtally[0];
-        t.reseeds += W.wtally[1];
-        t.cross[0] += (int)W.wtally[2];
-        t.cross[1] += (int)W.wtally[3];
-        t.cross[2] += (int)W.wtally[4];
-        t.stranded += W.wtally[5];
-        t.err |= W.wtally[6];
+    if (lane == 0 && sys >= 0) {
+        SysTally &T = P.tally[sys];
+        const unsigned *w = W.wtally;
+        if (w[T_COLL]) atomicAdd(&T.collisions, (unsigned long long)w[T_COLL]);
+        if (w[T_CAND]) atomicAdd(&T.candidates, (unsigned long long)w[T_CAND]);
+        if (w[T_WALL]) atomicAdd(&T.wall_hits, (unsigned long long)w[T_WALL]);
+        if (w[T_RESEED]) atomicAdd(&T.reseeds, (unsigned long long)w[T_RESEED]);
+        if (w[T_MOVED]) atomicAdd(&T.particle_steps, (unsigned long long)w[T_MOVED]);
+        if (w[T_STRANDED]) atomicAdd(&T.stranded, (unsigned long long)w[T_STRANDED]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const int c = (int)w[T_CROSS0 + d];
+            if (c) atomicAdd((unsigned long long *)&T.count_periodic[d], (unsigned long long)(long long)c);
+        }
+        if (w[T_ERR]) atomicOr(&P.status->error, w[T_ERR]);
     }
     __syncwarp();
-    if (lane < 8) W.wtally[lane] = 0;
+    if (lane < TALLY_N) W.wtally[lane] = 0;
     __syncwarp();
-    flush_lane_tally(P, t, lane);
 }
 
 // Places one particle per valid lane into a top slot of its new cell
@@ -192,9 +164,28 @@ __device__ __forceinline__ void insert_top(const PassParams &P, const Split32::P
     if (valid && lane == leader && over) atomicSub(&top_out[key], (unsigned)__popc(over));
 }
 
+__device__ __forceinline__ void tally_moves(unsigned *wtally, const MoveTally &mt, unsigned stranded) {
+    const unsigned wh = __reduce_add_sync(0xffffffffu, (unsigned)mt.wall_hits);
+    const unsigned rs = __reduce_add_sync(0xffffffffu, (unsigned)mt.reseeds);
+    const int c0 = __reduce_add_sync(0xffffffffu, mt.cross[0]);
+    const int c1 = __reduce_add_sync(0xffffffffu, mt.cross[1]);
+    const int c2 = __reduce_add_sync(0xffffffffu, mt.cross[2]);
+    const unsigned sd = __reduce_add_sync(0xffffffffu, stranded);
+    const unsigned er = __reduce_or_sync(0xffffffffu, mt.err);
+    if ((threadIdx.x & 31) == 0) {
+        wtally[T_WALL] += wh;
+        wtally[T_RESEED] += rs;
+        wtally[T_CROSS0] += (unsigned)c0;
+        wtally[T_CROSS1] += (unsigned)c1;
+        wtally[T_CROSS2] += (unsigned)c2;
+        wtally[T_STRANDED] += sd;
+        wtally[T_ERR] |= er;
+    }
+}
+
 // Runs the general mover on the queued particles, one per lane, and places
 // them; its counts go to the warp's shared tally.  All lanes call.
-__device__ __noinline__ void drain_queue(const PassParams &P, int sys, SlowRec *q, int *qn_p, unsigned *wtally,
+__device__ __noinline__ void drain_wall(const PassParams &P, int sys, SlowRec *q, int *qn_p, unsigned *wtally,
                                          int lane, uint32_t move_step) {
     const SysDev &g = P.sys[sys];
     const int qn = *qn_p;
@@ -224,50 +215,158 @@ __device__ __noinline__ void drain_queue(const PassParams &P, int sys, SlowRec *
     }
     __syncwarp();
     insert_top(P, p, valid, key, lane, mt.err);
-    const unsigned wh = __reduce_add_sync(0xffffffffu, (unsigned)mt.wall_hits);
-    const unsigned rs = __reduce_add_sync(0xffffffffu, (unsigned)mt.reseeds);
-    const int c0 = __reduce_add_sync(0xffffffffu, mt.cross[0]);
-    const int c1 = __reduce_add_sync(0xffffffffu, mt.cross[1]);
-    const int c2 = __reduce_add_sync(0xffffffffu, mt.cross[2]);
-    const unsigned sd = __reduce_add_sync(0xffffffffu, stranded);
-    const unsigned er = __reduce_or_sync(0xffffffffu, mt.err);
-    if (lane == 0) {
-        wtally[0] += wh;
-        wtally[1] += rs;
-        wtally[2] += (unsigned)c0;
-        wtally[3] += (unsigned)c1;
-        wtally[4] += (unsigned)c2;
-        wtally[5] += sd;
-        wtally[6] |= er;
-        *qn_p = 0;
-    }
+    tally_moves(wtally, mt, stranded);
+    if (lane == 0) *qn_p = 0;
     __syncwarp();
 }
 
-// The NTC collide of one staged cell by lane 0.  The warp first ranks the
-// cell's particles by id (the cell-list order of the reference's canonical
-// member order); perm[rank] is the ring slot of that particle.
-template <int R>
-__device__ __noinline__ unsigned collide_cell(uint64_t seed, int cell_global, uint32_t step, int n, int pairs,
-                                              double *vr_max, float4 *ring_b, int start, uint16_t *perm, int lane) {
-    for (int q = lane; q < n; q += 32) {
-        int sq = start + q;
-        if (sq >= R) sq -= R;
-        const uint32_t mine = __float_as_uint(ring_b[sq].w);
-        int rank = 0;
-        int sr = start;
-        for (int r = 0; r < n; ++r) {
-            rank += __float_as_uint(ring_b[sr].w) < mine;
-            if (++sr == R) sr = 0;
+// Particles that left their voxel, one per lane: a flight that ends in an
+// empty voxel completes here (Split32::move_open) and the particle takes a
+// top slot of its cell; the rest go to the wall queue unchanged, or, when
+// more of them than the wall queue holds arrive at once, take the general
+// mover right here.  All lanes call.
+__device__ __noinline__ void drain_movers(const PassParams &P, int sys, SlowRec *q, int *qn_p, SlowRec *wq,
+                                          int *wqn_p, unsigned *wtally, int lane, uint32_t move_step) {
+    const SysDev &g = P.sys[sys];
+    const int qn = *qn_p;
+    const bool valid = lane < qn;
+    Split32::Particle p;
+    MoveTally mt;
+    mt.wall_hits = mt.reseeds = 0;
+    mt.cross[0] = mt.cross[1] = mt.cross[2] = 0;
+    mt.err = 0;
+    unsigned stranded = 0, key = 0xffffffffu;
+    int from_cell = 0, from_global = 0;
+    bool done = false;
+    if (valid) {
+        const SlowRec &r = q[lane];
+        Split32::unpack(r.a, r.b, p);
+        from_cell = r.cell;
+        from_global = r.global;
+        done = Split32::move_open(g, p, mt);
+    }
+    const unsigned wall = __ballot_sync(0xffffffffu, valid && !done);
+    const int nwall = __popc(wall);
+    if (nwall) {
+        if (*wqn_p + nwall > WCAP && nwall <= WCAP) drain_wall(P, sys, wq, wqn_p, wtally, lane, move_step);
+        if (*wqn_p + nwall <= WCAP) {
+            if (valid && !done) wq[*wqn_p + __popc(wall & ((1u << lane) - 1u))] = q[lane];
+            __syncwarp();
+            if (lane == 0) *wqn_p += nwall;
+            __syncwarp();
+        } else if (valid && !done) {
+            Split32::move_general(g, p, move_step, mt);
+            done = true;
         }
-        perm[rank] = (uint16_t)sq;
+    }
+    if (done) {
+        key = (unsigned)from_cell;
+        const int cg = Split32::cell_global(g, p);
+        if (cg != from_global) {
+            const int ac = __ldg(g.cell_map + cg);
+            if (ac < 0) {
+                mt.err |= DSMC_EBIT_STRANDED;
+                stranded = 1;
+            } else {
+                key = (unsigned)ac;
+            }
+        }
+    }
+    insert_top(P, p, done, key, lane, mt.err);
+    tally_moves(wtally, mt, stranded);
+    if (lane == 0) *qn_p = 0;
+    __syncwarp();
+}
+
+// Draws of one collide stream: blocks 0..nblk-1 come from shared memory
+// (computed by the warp in parallel), later ones are computed here.  Same
+// layout as DrawStream.
+struct CachedDraws {
+    const uint4 *blk;
+    uint32_t nblk, key0, key1, id, step, k;
+    uint32_t w2, w3;
+    __device__ __forceinline__ void words(uint32_t &a, uint32_t &b) {
+        const uint32_t j = k >> 1;
+        if ((k & 1u) == 0) {
+            uint32_t w[4];
+            if (j < nblk) {
+                const uint4 c = blk[j];
+                w[0] = c.x;
+                w[1] = c.y;
+                w[2] = c.z;
+                w[3] = c.w;
+            } else {
+                philox4x32_10(id, step, DSMC_TAG_COLLIDE, j, key0, key1, w);
+            }
+            a = w[0];
+            b = w[1];
+            w2 = w[2];
+            w3 = w[3];
+        } else {
+            a = w2;
+            b = w3;
+        }
+        ++k;
+    }
+    template <class T> __device__ __forceinline__ T uniform() {
+        uint32_t a, b;
+        words(a, b);
+        return ((float)(a >> 9) + 0.5f) * (1.0f / 8388608.0f);
+    }
+};
+
+// The NTC collide of one staged cell.  The warp computes the cell's first
+// Philox blocks in parallel and ranks the cell's particles by id (the
+// reference's canonical member order); perm[rank] is the ring slot of that
+// particle.  Lane 0 then runs the candidate loop.
+template <int R>
+__device__ __forceinline__ unsigned collide_cell(uint64_t seed, int cell_global, uint32_t step, int n, int pairs,
+                                              double *vr_max, float4 *ring_b, int start, uint16_t *perm, uint4 *blk,
+                                              int lane) {
+    // three draws per candidate and two per collision: at most 5 * pairs
+    const uint32_t nblk = (uint32_t)min(32, (5 * pairs + 1) >> 1);
+    const uint32_t key0 = (uint32_t)seed, key1 = (uint32_t)(seed >> 32);
+    if ((uint32_t)lane < nblk) {
+        uint32_t w[4];
+        philox4x32_10((uint32_t)cell_global, step, DSMC_TAG_COLLIDE, (uint32_t)lane, key0, key1, w);
+        blk[lane] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+    if (n <= 32) {
+        int sq = start + lane;
+        if (sq >= R) sq -= R;
+        const uint32_t mine = lane < n ? __float_as_uint(ring_b[sq].w) : 0xffffffffu;
+        int rank = 0;
+#pragma unroll
+        for (int r = 0; r < 32; ++r) rank += __shfl_sync(0xffffffffu, mine, r) < mine;
+        if (lane < n) perm[rank] = (uint16_t)sq;
+    } else {
+        for (int q = lane; q < n; q += 32) {
+            int sq = start + q;
+            if (sq >= R) sq -= R;
+            const uint32_t mine = __float_as_uint(ring_b[sq].w);
+            int rank = 0;
+            int sr = start;
+            for (int r = 0; r < n; ++r) {
+                rank += __float_as_uint(ring_b[sr].w) < mine;
+                if (++sr == R) sr = 0;
+            }
+            perm[rank] = (uint16_t)sq;
+        }
     }
     __syncwarp();
     unsigned long long col = 0;
     if (lane == 0) {
+        CachedDraws rs;
+        rs.blk = blk;
+        rs.nblk = nblk;
+        rs.key0 = key0;
+        rs.key1 = key1;
+        rs.id = (uint32_t)cell_global;
+        rs.step = step;
+        rs.k = 0;
         SmemVel vel;
         vel.b = ring_b;
-        ntc_run<float>(seed, cell_global, step, n, pairs, *vr_max, vel, perm, col);
+        ntc_loop<float>(rs, n, pairs, *vr_max, vel, perm, col);
     }
     __syncwarp();
     return (unsigned)col;
@@ -276,7 +375,7 @@ __device__ __noinline__ unsigned collide_cell(uint64_t seed, int cell_global, ui
 constexpr int FUSED_WARPS = 4;  // warps per block of the pipelined pass
 
 template <int R>
-__global__ void __launch_bounds__(32 * FUSED_WARPS, 5) fused_split_kernel(const __grid_constant__ PassParams P) {
+__global__ void __launch_bounds__(32 * FUSED_WARPS, 4) fused_split_kernel(const __grid_constant__ PassParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     typedef Split32::Particle Particle;
     const int lane = threadIdx.x & 31;
@@ -287,17 +386,15 @@ __global__ void __launch_bounds__(32 * FUSED_WARPS, 5) fused_split_kernel(const 
     const uint32_t move_step = step + 1;
 
     WarpSmem<R> &W = reinterpret_cast<WarpSmem<R> *>(smem_raw)[wib];
-    if (lane == 0) W.qn = 0;
-    if (lane < 8) W.wtally[lane] = 0;
+    if (lane == 0) W.qn = W.wqn = 0;
+    if (lane < TALLY_N) W.wtally[lane] = 0;
 
     const uint4 *Ain = reinterpret_cast<const uint4 *>(P.parts.A[P.cur]);
     const float4 *Bin = reinterpret_cast<const float4 *>(P.parts.B[P.cur]);
     uint4 *Aout = reinterpret_cast<uint4 *>(P.parts.A[P.cur ^ 1]);
     float4 *Bout = reinterpret_cast<float4 *>(P.parts.B[P.cur ^ 1]);
 
-    LaneTally t;
-    lane_tally_reset(t);
-    t.sys = -1;
+    int tsys = -1;  // system of the counts in W.wtally
 
     const int C = P.cells.num_cells;
     const int nchunks = (C + 31) >> 5;
@@ -416,20 +513,21 @@ __global__ void __launch_bounds__(32 * FUSED_WARPS, 5) fused_split_kernel(const 
         const int base = T.base[ci];
         const int sys = T.sys[ci];
         const int pairs = T.pairs[ci];
-        if (sys != t.sys) {
-            if (W.qn) drain_queue(P, t.sys, W.q, &W.qn, W.wtally, lane, move_step);
-            if (t.sys >= 0) flush_warp(P, W, t, lane);
-            t.sys = sys;
+        if (sys != tsys) {
+            if (W.qn) drain_movers(P, tsys, W.q, &W.qn, W.wq, &W.wqn, W.wtally, lane, move_step);
+            if (W.wqn) drain_wall(P, tsys, W.wq, &W.wqn, W.wtally, lane, move_step);
+            if (tsys >= 0) flush_warp(P, W, tsys, lane);
+            tsys = sys;
         }
         const SysDev &g = P.sys[sys];
 
         // ---- collide: Cell::collide (dsmc/cell.cpp:52-111)
         if (pairs > 0) {
             const unsigned col = collide_cell<R>(g.seed, T.glob[ci], step, n, pairs, &W.tab[ct & 1].vr[ci], W.B,
-                                                 tail, W.perm, lane);
+                                                 tail, W.perm, W.blk, lane);
             if (lane == 0) {
-                t.collisions += col;
-                t.candidates += (unsigned)pairs;
+                W.wtally[T_COLL] += col;
+                W.wtally[T_CAND] += (unsigned)pairs;
             }
         }
 
@@ -509,7 +607,8 @@ __global__ void __launch_bounds__(32 * FUSED_WARPS, 5) fused_split_kernel(const 
             }
             n_fs += (unsigned)__popc(fast);
             if (slow) {
-                if (W.qn + __popc(slow) > QCAP) drain_queue(P, sys, W.q, &W.qn, W.wtally, lane, move_step);
+                if (W.qn + __popc(slow) > QCAP)
+                    drain_movers(P, sys, W.q, &W.qn, W.wq, &W.wqn, W.wtally, lane, move_step);
                 if (valid && !stay) {
                     SlowRec &rec = W.q[W.qn + __popc(slow & ((1u << lane) - 1u))];
                     Split32::pack(p, rec.a, rec.b);
@@ -522,7 +621,7 @@ __global__ void __launch_bounds__(32 * FUSED_WARPS, 5) fused_split_kernel(const 
             }
         }
         if (lane == ci) nfs_mine = n_fs;
-        if (lane == 0) t.moved += (unsigned)n;
+        if (lane == 0) W.wtally[T_MOVED] += (unsigned)n;
         // free the cell's ring slots once every lane is done with them
         __syncwarp();
         tail += n;
@@ -531,8 +630,9 @@ __global__ void __launch_bounds__(32 * FUSED_WARPS, 5) fused_split_kernel(const 
         --ahead;
         ++ci;
     }
-    if (W.qn) drain_queue(P, t.sys, W.q, &W.qn, W.wtally, lane, move_step);
-    if (t.sys >= 0) flush_warp(P, W, t, lane);
+    if (W.qn) drain_movers(P, tsys, W.q, &W.qn, W.wq, &W.wqn, W.wtally, lane, move_step);
+    if (W.wqn) drain_wall(P, tsys, W.wq, &W.wqn, W.wtally, lane, move_step);
+    if (tsys >= 0) flush_warp(P, W, tsys, lane);
 
     __syncthreads();
     if (threadIdx.x == 0) {
