@@ -287,7 +287,9 @@ def main():
                      "algorithmic_bytes_per_launch": BYTES_PER_PARTICLE_STEP * N},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48 * N / k_e2e,
                 "d2h_bytes_per_step": (48 * N + 64 * k_e2e) / k_e2e, "steps": k_e2e},
-        "gpu_launches": args.steps,
+        # collide_cells + move_cells + place_movers per step (pipelined pass),
+        # one pass kernel per step otherwise
+        "gpu_launches": args.steps * (3 if system.ctx.pass_info()["pipelined"] else 1),
         "clocks": clocks,
         "device_status": {"error_bits": err, "spill": spill},
         "pass": system.ctx.pass_info(),

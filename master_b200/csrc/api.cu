@@ -85,6 +85,7 @@ struct dsmc_ctx {
     DevBuf<int4> meta;
     DevBuf<double4> state;
     DevBuf<unsigned> bot[3], top[3], key;  // occupancy sets, rotating per re-binning pass
+    DevBuf<int2> room;                      // per cell: top-slot room of the pass in flight
     DevBuf<double> mom;
     std::vector<int4> h_meta;   // {base, cap, global, sys}
     size_t slots = 0;
@@ -93,6 +94,7 @@ struct dsmc_ctx {
     DevBuf<unsigned char> A0, A1, B0, B1;
     DevBuf<SpillRec> spill;
     unsigned spill_cap = 1u << 16;
+    DevBuf<int2> walls;       // wall-flight list of the production pass (one entry per slot at most)
     int cur = 0;
     int cphase = 0;           // occupancy set the next pass reads
     bool pending = false;     // the last step's collide/sample has not run yet
@@ -107,7 +109,7 @@ struct dsmc_ctx {
     // launch shape of the cell pass
     int block = 256;
     int grid = 0;
-    int fused_grid = 0;     // pipelined split-precision pass; 0 = not usable
+    int fused_grids[4] = {0, 0, 0, 0};  // production split-precision pass (collide, move, place, walls); 0 = not usable
     bool use_pipelined = true;
     double cap_factor = 2.0;
     int cap_pad = 24;
@@ -146,6 +148,7 @@ CellArrays cell_arrays(dsmc_ctx *ctx) {
     }
     c.mom = ctx->mom.p;
     c.key = ctx->key.p;
+    c.room = ctx->room.p;
     return c;
 }
 
@@ -157,6 +160,8 @@ ParticleArrays particle_arrays(dsmc_ctx *ctx) {
     p.B[1] = ctx->B1.p;
     p.spill = ctx->spill.p;
     p.spill_cap = ctx->spill_cap;
+    p.walls = ctx->walls.p;
+    p.walls_cap = (unsigned)std::min<size_t>(ctx->slots, 0xffffffffu);
     return p;
 }
 
@@ -215,6 +220,7 @@ int relayout(dsmc_ctx *ctx, long long total) {
     CK(ctx->B0.ensure(slots * half));
     CK(ctx->B1.ensure(slots * half));
     CK(ctx->key.ensure(slots));
+    CK(ctx->walls.ensure(std::max<size_t>(slots, 1)));
     CK(ctx->meta.ensure(std::max(C, 1)));
     if (C) {
         CK(cudaMemcpyAsync(ctx->meta.p, ctx->h_meta.data(), C * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
@@ -246,11 +252,9 @@ int relayout(dsmc_ctx *ctx, long long total) {
                                     : split32::pass_blocks_per_sm(PASS_SORT, ctx->block, ctx->smem_cap);
     if (bps_in <= 0 || bps_so <= 0) return fail(ctx, DSMC_ERR_CUDA, "stage passes cannot be resident (shared memory)");
     ctx->grid = bps * ctx->num_sms;
-    ctx->fused_grid = 0;
-    if (!is_fp64(ctx) && split32::fused_capacity(ctx->smem_cap) > 0) {
-        const int fb = split32::fused_blocks_per_sm(ctx->smem_cap);
-        ctx->fused_grid = fb * ctx->num_sms;
-    }
+    ctx->fused_grids[0] = ctx->fused_grids[1] = ctx->fused_grids[2] = ctx->fused_grids[3] = 0;
+    if (!is_fp64(ctx) && split32::fused_capacity(ctx->smem_cap) > 0)
+        split32::fused_grids(ctx->smem_cap, ctx->num_sms, ctx->fused_grids);
     Status st;
     cudaError_t e;
     st = read_status(ctx, &e);
@@ -322,9 +326,9 @@ int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, 
     P.smem_cap = ctx->smem_cap;
     P.advance_step = advance;
     cudaError_t e;
-    if (mode == PASS_FUSED && ctx->use_pipelined && ctx->fused_grid > 0) {
+    if (mode == PASS_FUSED && ctx->use_pipelined && ctx->fused_grids[1] > 0) {
         P.top_only = 0;
-        e = split32::launch_fused(P, ctx->fused_grid, ctx->stream);
+        e = split32::launch_fused(P, ctx->fused_grids, ctx->stream);
     } else {
         P.top_only = 1;
         e = is_fp64(ctx) ? fp64::launch_pass(mode, P, ctx->grid, ctx->block, ctx->stream)
@@ -418,6 +422,7 @@ int rebuild_cells(dsmc_ctx *ctx) {
         CK(ctx->top[q].alloc(Cn));
     }
     CK(ctx->mom.alloc(8 * Cn));
+    CK(ctx->room.alloc(Cn));
     CK(ctx->hist.alloc(Cn));
     if (C) {
         if (C_old > 0 && C_old <= C)
@@ -1024,9 +1029,9 @@ int dsmc_counters_get(dsmc_ctx *ctx, int sys_id, int64_t out[8]) {
 
 int dsmc_pass_info(dsmc_ctx *ctx, int *pipelined, int *grid, int *block, int *stage_capacity) {
     if (!ctx) return DSMC_ERR_ARG;
-    const bool pipe = ctx->use_pipelined && ctx->fused_grid > 0;
+    const bool pipe = ctx->use_pipelined && ctx->fused_grids[1] > 0;
     if (pipelined) *pipelined = pipe ? 1 : 0;
-    if (grid) *grid = pipe ? ctx->fused_grid : ctx->grid;
+    if (grid) *grid = pipe ? ctx->fused_grids[1] : ctx->grid;
     if (block) *block = pipe ? split32::fused_block() : ctx->block;
     if (stage_capacity) *stage_capacity = pipe ? split32::fused_capacity(ctx->smem_cap) : ctx->smem_cap;
     return DSMC_OK;

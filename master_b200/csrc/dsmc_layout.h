@@ -113,7 +113,8 @@ struct Status {
     unsigned int step;         // current step number (the reference's System::steps)
     unsigned int blocks_done;  // end-of-pass counter used to advance `step`
     unsigned int halted;       // non-zero: a pass saw spill/error; later passes do nothing
-    unsigned int pad[3];
+    unsigned int walls;        // entries in the wall-flight list this pass (production pass)
+    unsigned int pad[2];
 };
 
 struct SpillRec {
@@ -137,6 +138,7 @@ struct CellArrays {
     unsigned *top[3];          // top-segment occupancy
     double *mom;               // 8 fp64 per cell: n, sum v (3), sum v^2 (3), sum |v|^2
     unsigned *key;             // per slot: new active cell after a stand-alone move stage
+    int2 *room;                // per cell, this pass: {first slot past the cell, top slots free}
 };
 
 struct ParticleArrays {
@@ -144,6 +146,8 @@ struct ParticleArrays {
     void *B[2];
     SpillRec *spill;
     unsigned spill_cap;
+    int2 *walls;               // production pass: {output slot, system} of flights that meet a wall
+    unsigned walls_cap;
 };
 
 struct PassParams {

@@ -380,10 +380,13 @@ struct Split32 {
     }
 
     static __device__ __forceinline__ void accelerate(const SysDev &g, Particle &p) {
-        // unrolled select: a runtime index into p.v would put the particle in local memory
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-            if (d == g.flow_dir) p.v[d] += g.accel_dt_f;
+        // per-component selects: a store at a run-time index into p.v would
+        // put the particle in local memory
+        const int f = g.flow_dir;
+        const float a = g.accel_dt_f;
+        p.v[0] = f == 0 ? p.v[0] + a : p.v[0];
+        p.v[1] = f == 1 ? p.v[1] + a : p.v[1];
+        p.v[2] = f == 2 ? p.v[2] + a : p.v[2];
     }
 };
 
@@ -642,9 +645,11 @@ struct Fp64 {
     }
 
     static __device__ __forceinline__ void accelerate(const SysDev &g, Particle &p) {
-#pragma unroll
-        for (int d = 0; d < 3; ++d)
-            if (d == g.flow_dir) p.v[d] += g.accel_dt;
+        const int f = g.flow_dir;
+        const double a = g.accel_dt;
+        p.v[0] = f == 0 ? p.v[0] + a : p.v[0];
+        p.v[1] = f == 1 ? p.v[1] + a : p.v[1];
+        p.v[2] = f == 2 ? p.v[2] + a : p.v[2];
     }
 };
 
@@ -741,8 +746,8 @@ __device__ __forceinline__ void ntc_scatter(double &ax, double &ay, double &az, 
 // Cell::collide (dsmc/cell.cpp:75-111) over the members in id order, on
 // velocities staged in shared memory.  Run by one lane.  Draws: stream
 // (cell, step, collide), three per candidate and two more per collision.
-template <class real, class Vel, class Draws>
-__device__ void ntc_loop(Draws &rs, int n, int pairs, double &vr_max, Vel vel, const uint16_t *perm,
+template <class real, class Vel, class Draws, class Perm>
+__device__ __forceinline__ void ntc_loop(Draws &rs, int n, int pairs, double &vr_max, Vel vel, Perm perm,
                          unsigned long long &collisions) {
     double crm = vr_max;
     const real vmax = (real)vr_max;

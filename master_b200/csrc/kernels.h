@@ -37,11 +37,13 @@ DSMC_DECLARE_LAUNCHERS(split32)
 DSMC_DECLARE_LAUNCHERS(fp64)
 
 namespace split32 {
-// the bulk-copy pipelined production pass (fused_split.cuh)
-int fused_capacity(int smem_cap);   // ring slots per warp; 0: no instantiation holds smem_cap
-int fused_block();                  // threads per block of the pipelined pass
-int fused_blocks_per_sm(int smem_cap);
-cudaError_t launch_fused(const PassParams &P, int grid, cudaStream_t st);
+// the production pass (split_pass.cuh)
+int fused_capacity(int smem_cap);   // move_cells ring slots per warp; 0: the production pass cannot run
+int fused_block();                  // threads per block of the production kernels
+// Persistent grids of collide_cells, move_cells, place_movers and
+// place_walls; 0 when one of them cannot be resident.
+int fused_grids(int smem_cap, int num_sms, int grids[4]);
+cudaError_t launch_fused(const PassParams &P, const int grids[4], cudaStream_t st);
 }  // namespace split32
 
 // Pass modes (engine.cuh PassMode).

@@ -4,67 +4,94 @@
 #define DSMC_PREC_NS split32
 #include "kernels_impl.cuh"
 
-#include "fused_split.cuh"
+#include "split_pass.cuh"
 
 namespace dsmc {
 namespace split32 {
 
-// The production pass: the smallest ring that holds the largest cell.
-template <int R> static cudaError_t launch_fused_ring(const PassParams &P, int grid, cudaStream_t st) {
-    fused::fused_split_kernel<R><<<grid, 32 * fused::FUSED_WARPS, fused::fused_smem_bytes<R>(), st>>>(P);
+// The production pass (split_pass.cuh): collide_cells, move_cells with the
+// smallest ring that holds the largest cell, place_movers, place_walls.
+template <int R> static cudaError_t launch_move_ring(const PassParams &P, int grid, cudaStream_t st) {
+    pass3::move_cells_kernel<R><<<grid, 32 * pass3::M_WARPS, pass3::move_smem_bytes<R>(), st>>>(P);
     return cudaGetLastError();
 }
-template <int R> static int fused_ring_blocks() {
-    const size_t smem = fused::fused_smem_bytes<R>();
+template <int R> static int move_ring_blocks() {
+    const size_t smem = pass3::move_smem_bytes<R>();
     // the opt-in limit is a property of the function, shared by every
     // context: raise it to the device maximum, never lower it
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     cudaFuncAttributes fa;
-    if (cudaFuncGetAttributes(&fa, fused::fused_split_kernel<R>) != cudaSuccess) return 0;
+    if (cudaFuncGetAttributes(&fa, pass3::move_cells_kernel<R>) != cudaSuccess) return 0;
     if (smem + fa.sharedSizeBytes > (size_t)optin) return 0;
-    if (cudaFuncSetAttribute(fused::fused_split_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(pass3::move_cells_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              optin - (int)fa.sharedSizeBytes) != cudaSuccess)
         return 0;
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fused::fused_split_kernel<R>, 32 * fused::FUSED_WARPS,
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, pass3::move_cells_kernel<R>, 32 * pass3::M_WARPS,
                                                       smem) != cudaSuccess)
         return 0;
     return nb;
 }
+template <class K> static int static_blocks(K kernel, int threads) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, 0) != cudaSuccess) return 0;
+    return nb;
+}
 
-// Ring slots per warp of the production pass for cells of at most
-// `smem_cap` slots (0: no ring is large enough).
+// Ring slots per warp of move_cells for cells of at most `smem_cap` slots
+// (0: no ring is large enough, or a cell could exceed the collide batch).
 int fused_capacity(int smem_cap) {
     static const int rings[] = {64, 96, 128, 160, 192, 224, 256};
+    if (smem_cap > pass3::PCAP) return 0;
     for (int r : rings)
         if (smem_cap <= r) return r;
     return 0;
 }
 
-int fused_block() { return 32 * fused::FUSED_WARPS; }
+int fused_block() { return 32 * pass3::M_WARPS; }
 
-#define DSMC_FUSED_RINGS(X) X(64) X(96) X(128) X(160) X(192) X(224) X(256)
+#define DSMC_MOVE_RINGS(X) X(64) X(96) X(128) X(160) X(192) X(224) X(256)
 
-int fused_blocks_per_sm(int smem_cap) {
+int fused_grids(int smem_cap, int num_sms, int grids[4]) {
+    int bm = 0;
     switch (fused_capacity(smem_cap)) {
 #define X(r) \
-    case r: return fused_ring_blocks<r>();
-        DSMC_FUSED_RINGS(X)
+    case r: bm = move_ring_blocks<r>(); break;
+        DSMC_MOVE_RINGS(X)
 #undef X
     }
-    return 0;
+    const int bc = static_blocks(pass3::collide_cells_kernel, 32 * pass3::C_WARPS);
+    const int bp = static_blocks(pass3::place_movers_kernel, 32 * pass3::P_WARPS);
+    const int bw = static_blocks(pass3::place_walls_kernel, 32 * pass3::W_WARPS);
+    if (bm <= 0 || bc <= 0 || bp <= 0 || bw <= 0) return 0;
+    grids[0] = bc * num_sms;
+    grids[1] = bm * num_sms;
+    grids[2] = bp * num_sms;
+    grids[3] = bw * num_sms;
+    return 1;
 }
 
-cudaError_t launch_fused(const PassParams &P, int grid, cudaStream_t st) {
+cudaError_t launch_fused(const PassParams &P, const int grids[4], cudaStream_t st) {
+    if (P.do_collide || P.do_sample) {
+        pass3::collide_cells_kernel<<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e = cudaErrorInvalidValue;
     switch (fused_capacity(P.smem_cap)) {
 #define X(r) \
-    case r: return launch_fused_ring<r>(P, grid, st);
-        DSMC_FUSED_RINGS(X)
+    case r: e = launch_move_ring<r>(P, grids[1], st); break;
+        DSMC_MOVE_RINGS(X)
 #undef X
     }
-    return cudaErrorInvalidValue;
+    if (e != cudaSuccess) return e;
+    pass3::place_movers_kernel<<<grids[2], 32 * pass3::P_WARPS, 0, st>>>(P);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    pass3::place_walls_kernel<<<grids[3], 32 * pass3::W_WARPS, 0, st>>>(P);
+    return cudaGetLastError();
 }
 
 }  // namespace split32

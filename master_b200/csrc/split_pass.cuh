@@ -1,0 +1,746 @@
+// The production timestep pass for split-precision state: three kernels per
+// step over the active cells, which the previous pass left sorted by cell
+// (bottom segment + top segment of each cell's slots, counts in the `cin`
+// occupancy set).
+//
+//   collide_cells  Cell::prepare + Cell::collide (dsmc/cell.cpp:42-111) of
+//                  every cell, and the sampling on the reference's cadence.
+//                  Per chunk of 32 consecutive cells lane i selects for cell
+//                  i; the warp ranks each colliding cell's particles by id
+//                  (the reference's member order) into shared memory, then
+//                  every lane runs the candidate loop of its own cell.
+//                  Velocities are updated in place in the input buffer.
+//   move_cells     System::accelerate + the mover's first flight
+//                  (dsmc/system.cpp:133-144, dsmc/moleculemover.cpp:50-126)
+//                  for every particle.  A particle that stays inside its
+//                  empty voxel goes, moved, to the bottom segment of its cell
+//                  in the output buffer; the rest ("movers"), accelerated but
+//                  not moved, go to the gap just above: slots
+//                  [base + stayers, base + n_in) hold exactly the cell's
+//                  movers.  Particle records stream through a per-warp
+//                  shared-memory ring with 16-byte cp.async copies.
+//   place_movers   A mover whose flight ends in an empty voxel completes it
+//                  and takes a top slot of its new cell (warp-aggregated
+//                  atomics; the spill list when the cell is full).  Flights
+//                  that meet a wall go to a list of (slot, system) pairs.
+//   place_walls    The general mover (bisection, facet, diffuse wall) for
+//                  the listed flights, then the same placement.  The last
+//                  block ends the pass (step counter, halting).
+//
+// Top slots are taken from the top of the cell down and never below
+// base + n_in(cell), so they cannot meet the bottom segment or the gap.
+#pragma once
+#include "engine.cuh"
+
+namespace dsmc {
+namespace pass3 {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// 16-byte global -> shared copy, cached in L2 only (both addresses 16-byte
+// aligned: slots are uint4/float4 records).
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// Waits until at most `pending` of this thread's newest commit groups are
+// still in flight (more than 4 is treated as 4, which waits longer).
+__device__ __forceinline__ void cp_async_wait(int pending) {
+    switch (pending) {
+        case 0: asm volatile("cp.async.wait_group 0;" ::: "memory"); break;
+        case 1: asm volatile("cp.async.wait_group 1;" ::: "memory"); break;
+        case 2: asm volatile("cp.async.wait_group 2;" ::: "memory"); break;
+        case 3: asm volatile("cp.async.wait_group 3;" ::: "memory"); break;
+        default: asm volatile("cp.async.wait_group 4;" ::: "memory"); break;
+    }
+}
+
+// Input occupancy of active cell a (clamped to its capacity).
+__device__ __forceinline__ void input_counts(const PassParams &P, int a, const int4 &m, unsigned &nb, unsigned &nt) {
+    nb = min(P.cells.bot[P.cin][a], (unsigned)m.y);
+    nt = min(P.cells.top[P.cin][a], (unsigned)m.y - nb);
+}
+// Slot of member q of a cell: bottom segment, then top segment.
+__device__ __forceinline__ int member_slot(int base, int cap, int nb, int nt, int q) {
+    return q < nb ? base + q : base + cap - nt + (q - nb);
+}
+
+__device__ __forceinline__ unsigned warp_sum(unsigned x) { return __reduce_add_sync(0xffffffffu, x); }
+__device__ __forceinline__ int warp_sum(int x) { return __reduce_add_sync(0xffffffffu, x); }
+
+// The system shared by the valid lanes of a warp, or -2 when they differ
+// (-1 when no lane is valid).  All lanes call.
+__device__ __forceinline__ int common_system(bool valid, int sys) {
+    const unsigned vm = __ballot_sync(0xffffffffu, valid);
+    if (!vm) return -1;
+    const int s0 = __shfl_sync(0xffffffffu, sys, __ffs(vm) - 1);
+    return __all_sync(0xffffffffu, !valid || sys == s0) ? s0 : -2;
+}
+
+// ---- collide_cells ----------------------------------------------------------
+
+constexpr int C_WARPS = 4;
+constexpr int PCAP = 512;    // ranked members per warp and batch (>= the largest cell)
+constexpr int IDCAP = 256;   // ids of a cell of more than 32 members while it is ranked
+
+struct CollideSmem {
+    int perm[PCAP];
+    uint32_t ids[IDCAP];
+};
+
+// Velocities of one cell's members in the input buffer, by id rank.
+struct RankVel {
+    float4 *b;
+    const int *perm;
+    __device__ __forceinline__ void get(int r, float &x, float &y, float &z) const {
+        const float4 v = b[perm[r]];
+        x = v.x;
+        y = v.y;
+        z = v.z;
+    }
+    __device__ __forceinline__ void set(int r, float x, float y, float z) const {
+        float *q = reinterpret_cast<float *>(b + perm[r]);
+        q[0] = x;
+        q[1] = y;
+        q[2] = z;
+    }
+};
+struct IdentityPerm {
+    __device__ __forceinline__ int operator[](int i) const { return i; }
+};
+
+__device__ __forceinline__ void publish_collide(const PassParams &P, int sys, unsigned col, unsigned cand,
+                                                unsigned smp, bool per_lane) {
+    if (per_lane) {
+        if (sys >= 0) {
+            if (col) atomicAdd(&P.tally[sys].collisions, (unsigned long long)col);
+            if (cand) atomicAdd(&P.tally[sys].candidates, (unsigned long long)cand);
+            if (smp) atomicAdd(&P.tally[sys].samples, (unsigned long long)smp);
+        }
+        return;
+    }
+    const unsigned c = warp_sum(col), d = warp_sum(cand), s = warp_sum(smp);
+    if ((threadIdx.x & 31) == 0 && sys >= 0) {
+        if (c) atomicAdd(&P.tally[sys].collisions, (unsigned long long)c);
+        if (d) atomicAdd(&P.tally[sys].candidates, (unsigned long long)d);
+        if (s) atomicAdd(&P.tally[sys].samples, (unsigned long long)s);
+    }
+}
+
+__global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __grid_constant__ PassParams P) {
+    __shared__ CollideSmem smem[C_WARPS];
+    const int lane = threadIdx.x & 31;
+    const volatile Status *vs = P.status;
+    if (vs->halted) return;
+    const uint32_t step = vs->step;
+    CollideSmem &W = smem[threadIdx.x >> 5];
+    float4 *Bin = reinterpret_cast<float4 *>(P.parts.B[P.cur]);
+
+    const int C = P.cells.num_cells;
+    const int nchunks = (C + 31) >> 5;
+    unsigned col = 0, cand = 0, smp = 0;  // this lane's counts for system tsys
+    int tsys = -1;
+
+    for (int ch = blockIdx.x * C_WARPS + (threadIdx.x >> 5); ch < nchunks; ch += gridDim.x * C_WARPS) {
+        const int first = ch * 32;
+        const bool mine = lane < C - first;
+        const int a = first + lane;
+        int4 m = make_int4(0, 0, 0, -1);
+        unsigned nb = 0, nt = 0;
+        double vr = 0, rest = 0;
+        int pairs = 0;
+        if (mine) {
+            m = P.cells.meta[a];
+            input_counts(P, a, m, nb, nt);
+            const double4 st = P.cells.state[a];
+            vr = st.x;
+            rest = st.y;
+            if (P.do_collide) {
+                pairs = ntc_select(st.z, (int)(nb + nt), vr, rest);
+                if (nb + nt < 2) pairs = 0;
+                if (nb + nt > (unsigned)PCAP) {  // the host keeps every cap below PCAP
+                    atomicOr(&P.status->error, DSMC_EBIT_SMEM);
+                    pairs = 0;
+                }
+            }
+        }
+        const int n = (int)(nb + nt);
+        const int sys = m.w;
+        const int csys = common_system(mine, sys);
+        if (csys != tsys) {
+            publish_collide(P, tsys, col, cand, smp, false);
+            col = cand = smp = 0;
+            tsys = csys;
+        }
+
+        // Rank the colliding cells' members by id, a batch at a time, and
+        // run the batch's candidate loops one cell per lane.
+        unsigned todo = __ballot_sync(0xffffffffu, pairs > 0);
+        while (todo) {
+            int off = 0, my_off = 0;
+            unsigned ready = 0;
+            while (todo) {
+                const int c = __ffs(todo) - 1;
+                const int nc = __shfl_sync(0xffffffffu, n, c);
+                if (off + nc > PCAP) break;  // the batch is full (off > 0 here: nc <= PCAP)
+                const int base = __shfl_sync(0xffffffffu, m.x, c);
+                const int cap = __shfl_sync(0xffffffffu, m.y, c);
+                const int nbc = (int)__shfl_sync(0xffffffffu, nb, c);
+                const int ntc = nc - nbc;
+                if (nc <= 32) {
+                    const int sl = lane < nc ? member_slot(base, cap, nbc, ntc, lane) : 0;
+                    const uint32_t id = lane < nc ? __float_as_uint(Bin[sl].w) : 0xffffffffu;
+                    int rank = 0;
+#pragma unroll
+                    for (int r = 0; r < 32; ++r) rank += __shfl_sync(0xffffffffu, id, r) < id;
+                    if (lane < nc) W.perm[off + rank] = sl;
+                } else if (nc <= IDCAP) {
+                    for (int q = lane; q < nc; q += 32) W.ids[q] = __float_as_uint(Bin[member_slot(base, cap, nbc, ntc, q)].w);
+                    __syncwarp();
+                    for (int q = lane; q < nc; q += 32) {
+                        const uint32_t id = W.ids[q];
+                        int rank = 0;
+                        for (int r = 0; r < nc; ++r) rank += W.ids[r] < id;
+                        W.perm[off + rank] = member_slot(base, cap, nbc, ntc, q);
+                    }
+                    __syncwarp();
+                } else {
+                    for (int q = lane; q < nc; q += 32) {
+                        const uint32_t id = __float_as_uint(Bin[member_slot(base, cap, nbc, ntc, q)].w);
+                        int rank = 0;
+                        for (int r = 0; r < nc; ++r)
+                            rank += __float_as_uint(Bin[member_slot(base, cap, nbc, ntc, r)].w) < id;
+                        W.perm[off + rank] = member_slot(base, cap, nbc, ntc, q);
+                    }
+                }
+                if (lane == c) my_off = off;
+                off += nc;
+                ready |= 1u << c;
+                todo &= ~(1u << c);
+            }
+            __syncwarp();
+            if ((ready >> lane) & 1u) {
+                const SysDev &g = P.sys[sys];
+                DrawStream rs;
+                rs.init(g.seed, (uint32_t)m.z, step, DSMC_TAG_COLLIDE);
+                RankVel vel;
+                vel.b = Bin;
+                vel.perm = W.perm + my_off;
+                unsigned long long c_ = 0;
+                ntc_loop<float>(rs, n, pairs, vr, vel, IdentityPerm(), c_);
+                col += (unsigned)c_;
+                cand += (unsigned)pairs;
+            }
+            __syncwarp();
+        }
+        if (mine && P.do_collide)
+            *reinterpret_cast<double2 *>(&P.cells.state[a]) = make_double2(vr, rest);
+
+        // Sampling on the reference's cadence: cell moments in fp64.
+        if (mine && P.do_sample) {
+            const SysDev &g = P.sys[sys];
+            if (g.sample_interval > 0 && step > 0 && (step % (uint32_t)g.sample_interval) == 0 &&
+                step >= (uint32_t)g.sample_begin) {
+                double m1[3] = {0, 0, 0}, m2[3] = {0, 0, 0};
+                for (int q = 0; q < n; ++q) {
+                    const float4 b = Bin[member_slot(m.x, m.y, (int)nb, (int)nt, q)];
+                    const double x = b.x, y = b.y, z = b.z;
+                    m1[0] += x;
+                    m1[1] += y;
+                    m1[2] += z;
+                    m2[0] += x * x;
+                    m2[1] += y * y;
+                    m2[2] += z * z;
+                }
+                double *M = P.cells.mom + 8 * (size_t)a;
+                M[0] += (double)n;
+                M[1] += m1[0];
+                M[2] += m1[1];
+                M[3] += m1[2];
+                M[4] += m2[0];
+                M[5] += m2[1];
+                M[6] += m2[2];
+                M[7] += m2[0] + m2[1] + m2[2];
+                if (a == g.active_begin) ++smp;
+            }
+        }
+        if (tsys == -2) {  // a chunk that spans systems: per-lane counts
+            publish_collide(P, sys, col, cand, smp, true);
+            col = cand = smp = 0;
+        }
+    }
+    publish_collide(P, tsys, col, cand, smp, false);
+}
+
+// ---- move_cells -------------------------------------------------------------
+
+constexpr int M_WARPS = 4;
+constexpr int DEPTH = 4;  // cells staged ahead of the one in work
+
+struct MoveTab {
+    int base[32], cap[32];
+    unsigned nb[32], nt[32];
+    int sys[32];
+    int first, ncell;
+};
+template <int R> struct MoveSmem {
+    uint4 A[R];
+    float4 B[R];
+    MoveTab tab[2];
+};
+
+template <int R>
+__global__ void __launch_bounds__(32 * M_WARPS) move_cells_kernel(const __grid_constant__ PassParams P) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    typedef Split32::Particle Particle;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const volatile Status *vs = P.status;
+    if (vs->halted) return;
+
+    MoveSmem<R> &W = reinterpret_cast<MoveSmem<R> *>(smem_raw)[wib];
+    const uint4 *Ain = reinterpret_cast<const uint4 *>(P.parts.A[P.cur]);
+    const float4 *Bin = reinterpret_cast<const float4 *>(P.parts.B[P.cur]);
+    uint4 *Aout = reinterpret_cast<uint4 *>(P.parts.A[P.cur ^ 1]);
+    float4 *Bout = reinterpret_cast<float4 *>(P.parts.B[P.cur ^ 1]);
+
+    const int C = P.cells.num_cells;
+    const int nchunks = (C + 31) >> 5;
+    const int wstride = gridDim.x * M_WARPS;
+    const int chunk0 = blockIdx.x * M_WARPS + wib;
+
+    auto load_tab = [&](int b, int ch) {
+        MoveTab &T = W.tab[b];
+        const int first = ch * 32;
+        const int ncell = ch < nchunks ? min(32, C - first) : 0;
+        if (lane == 0) {
+            T.first = first;
+            T.ncell = ncell;
+        }
+        if (lane < ncell) {
+            const int a = first + lane;
+            const int4 m = P.cells.meta[a];
+            unsigned nb, nt;
+            input_counts(P, a, m, nb, nt);
+            if (nb + nt > (unsigned)R) atomicOr(&P.status->error, DSMC_EBIT_SMEM);  // the host sizes R above every cap
+            // top slots free for arrivals this pass: above the input occupancy
+            P.cells.room[a] = make_int2(m.x + m.y, m.y - (int)(nb + nt));
+            T.base[lane] = m.x;
+            T.cap[lane] = m.y;
+            T.nb[lane] = nb;
+            T.nt[lane] = nt;
+            T.sys[lane] = m.w;
+        }
+    };
+    // Lane i publishes cell i's bottom occupancy and clears the set the next
+    // pass writes.
+    auto write_tab = [&](int b, unsigned nfs) {
+        const MoveTab &T = W.tab[b];
+        if (lane < T.ncell) {
+            const int a = T.first + lane;
+            P.cells.bot[P.cout][a] = nfs;
+            P.cells.bot[P.cclear][a] = 0;
+            P.cells.top[P.cclear][a] = 0;
+        }
+    };
+
+    load_tab(0, chunk0);
+    load_tab(1, chunk0 + wstride);
+    __syncwarp();
+
+    int head = 0, tail = 0, used = 0;  // ring (warp-uniform)
+    int it = 0, ii = 0;                // next cell to stage: chunk ordinal, cell in chunk
+    int ct = 0, ci = 0;                // cell in work
+    int ahead = 0;                     // cells staged, the one in work included
+    unsigned nfs_mine = 0;             // lane i: bottom occupancy of cell i of the chunk in work
+    unsigned moved = 0;                // particles moved, system tsys (warp-uniform)
+    int tsys = -1;
+
+    auto stage_ahead = [&]() {
+        // (it, ii) moves past a full chunk as soon as its last cell is
+        // staged, so ii >= ncell only past the warp's last cell
+        while (ahead <= DEPTH && it <= ct + 1) {
+            const MoveTab &T = W.tab[it & 1];
+            if (ii >= T.ncell) return;
+            const int nb = (int)T.nb[ii], nt = (int)T.nt[ii];
+            const int n = min(nb + nt, R);
+            if (used + n > R) return;
+            const int base = T.base[ii], cap = T.cap[ii];
+            for (int q = lane; q < n; q += 32) {
+                const int slot = member_slot(base, cap, nb, nt, q);
+                int r = head + q;
+                if (r >= R) r -= R;
+                cp_async16(&W.A[r], Ain + slot);
+                cp_async16(&W.B[r], Bin + slot);
+            }
+            cp_async_commit();
+            head += n;
+            if (head >= R) head -= R;
+            used += n;
+            ++ahead;
+            if (++ii == 32) {
+                ++it;
+                ii = 0;
+            }
+        }
+    };
+
+    while (true) {
+        const MoveTab &T = W.tab[ct & 1];
+        if (ci >= T.ncell) {
+            if (T.ncell > 0) write_tab(ct & 1, nfs_mine);
+            if (T.ncell < 32) break;  // that was the warp's last chunk
+            __syncwarp();
+            load_tab(ct & 1, chunk0 + (ct + 2) * wstride);
+            __syncwarp();
+            ++ct;
+            ci = 0;
+            continue;
+        }
+        stage_ahead();  // the cell in work is staged once this returns
+        cp_async_wait(ahead - 1);
+        __syncwarp();
+
+        const int n = min((int)(T.nb[ci] + T.nt[ci]), R);
+        const int base = T.base[ci];
+        const int sys = T.sys[ci];
+        if (sys != tsys) {
+            if (lane == 0 && tsys >= 0 && moved) atomicAdd(&P.tally[tsys].particle_steps, (unsigned long long)moved);
+            moved = 0;
+            tsys = sys;
+        }
+        const SysDev &g = P.sys[sys];
+
+        unsigned n_fs = 0, n_mv = 0;
+        for (int c0 = 0; c0 < n; c0 += 32) {
+            const int q = c0 + lane;
+            const bool valid = q < n;
+            Particle p;
+            bool stay = false;
+            if (valid) {
+                int r = tail + q;
+                if (r >= R) r -= R;
+                Split32::unpack(W.A[r], W.B[r], p);
+                Split32::accelerate(g, p);
+                if (!p.flag) {
+                    float x[3];
+                    stay = true;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        x[d] = fmaf(p.v[d] * g.inv_vox_f[d], g.dt_f, p.o[d]);
+                        stay &= (x[d] >= 0.0f) & (x[d] < 1.0f);
+                    }
+                    if (stay) {
+                        p.o[0] = x[0];
+                        p.o[1] = x[1];
+                        p.o[2] = x[2];
+                    }
+                }
+            }
+            const unsigned fast = __ballot_sync(0xffffffffu, valid && stay);
+            const unsigned slow = __ballot_sync(0xffffffffu, valid && !stay);
+            const unsigned below = (1u << lane) - 1u;
+            if (valid) {
+                // stayers fill the bottom upwards, movers the gap downwards
+                const unsigned dst = stay ? (unsigned)base + n_fs + (unsigned)__popc(fast & below)
+                                          : (unsigned)(base + n) - 1u - n_mv - (unsigned)__popc(slow & below);
+                uint4 ra;
+                float4 rb;
+                Split32::pack(p, ra, rb);
+                Aout[dst] = ra;
+                Bout[dst] = rb;
+            }
+            n_fs += (unsigned)__popc(fast);
+            n_mv += (unsigned)__popc(slow);
+        }
+        if (lane == ci) nfs_mine = n_fs;
+        moved += (unsigned)n;
+        __syncwarp();  // every lane is done with the cell's ring slots
+        tail += n;
+        if (tail >= R) tail -= R;
+        used -= n;
+        --ahead;
+        ++ci;
+    }
+    if (lane == 0 && tsys >= 0 && moved) atomicAdd(&P.tally[tsys].particle_steps, (unsigned long long)moved);
+}
+
+template <int R> constexpr size_t move_smem_bytes() { return sizeof(MoveSmem<R>) * M_WARPS; }
+
+// ---- place_movers -----------------------------------------------------------
+
+constexpr int P_WARPS = 4;
+constexpr int W_WARPS = 4;
+constexpr int WQ = 32;  // wall-flight entries a warp collects before appending them to the list
+
+struct PlaceSmem {
+    int2 q[WQ];  // {output slot, system}
+    int qn;
+};
+
+struct MoveCounts {
+    unsigned wall, reseed, stranded, err;
+    int cross[3];
+};
+__device__ __forceinline__ void counts_reset(MoveCounts &c) {
+    c.wall = c.reseed = c.stranded = c.err = 0;
+    c.cross[0] = c.cross[1] = c.cross[2] = 0;
+}
+__device__ __forceinline__ void counts_add(MoveCounts &c, const MoveTally &t) {
+    c.wall += (unsigned)t.wall_hits;
+    c.reseed += (unsigned)t.reseeds;
+    c.err |= t.err;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) c.cross[d] += t.cross[d];
+}
+// Publishes the counts for system sys: the warp's sum (all lanes call) or,
+// per_lane, each lane's own.
+__device__ void counts_publish(const PassParams &P, int sys, MoveCounts &c, bool per_lane) {
+    unsigned w = c.wall, r = c.reseed, s = c.stranded, e = c.err;
+    int x[3] = {c.cross[0], c.cross[1], c.cross[2]};
+    if (!per_lane) {
+        w = warp_sum(w);
+        r = warp_sum(r);
+        s = warp_sum(s);
+        e = __reduce_or_sync(0xffffffffu, e);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) x[d] = warp_sum(x[d]);
+    }
+    if ((per_lane || (threadIdx.x & 31) == 0) && sys >= 0) {
+        SysTally &T = P.tally[sys];
+        if (w) atomicAdd(&T.wall_hits, (unsigned long long)w);
+        if (r) atomicAdd(&T.reseeds, (unsigned long long)r);
+        if (s) atomicAdd(&T.stranded, (unsigned long long)s);
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            if (x[d]) atomicAdd((unsigned long long *)&T.count_periodic[d], (unsigned long long)(long long)x[d]);
+    }
+    if ((per_lane || (threadIdx.x & 31) == 0) && e) atomicOr(&P.status->error, e);
+    counts_reset(c);
+}
+
+// Places one particle per valid lane into a top slot of cell `key`
+// (warp-aggregated atomics).  A slot at or below the cell's input occupancy
+// could meet its bottom segment or gap: that particle spills instead, and its
+// slot is given back so the counter ends at the number placed.
+__device__ __forceinline__ void insert_top(const PassParams &P, const Split32::Particle &p, bool valid,
+                                           unsigned key, unsigned &err) {
+    const int lane = threadIdx.x & 31;
+    unsigned *top_out = P.cells.top[P.cout];
+    const int2 rt = valid ? P.cells.room[key] : make_int2(0, 0);  // {first slot past the cell, room}
+    const unsigned peers = __match_any_sync(0xffffffffu, valid ? key : 0xffffffffu);
+    const int leader = __ffs(peers) - 1;
+    unsigned slot0 = 0;
+    if (valid && lane == leader) slot0 = atomicAdd(&top_out[key], (unsigned)__popc(peers));
+    slot0 = __shfl_sync(0xffffffffu, slot0, leader);
+    bool spilled = false;
+    if (valid) {
+        const unsigned j = slot0 + (unsigned)__popc(peers & ((1u << lane) - 1u));
+        uint4 ra;
+        float4 rb;
+        Split32::pack(p, ra, rb);
+        if (j < (unsigned)rt.y) {
+            const unsigned dst = (unsigned)rt.x - 1u - j;
+            reinterpret_cast<uint4 *>(P.parts.A[P.cur ^ 1])[dst] = ra;
+            reinterpret_cast<float4 *>(P.parts.B[P.cur ^ 1])[dst] = rb;
+        } else {
+            spilled = true;
+            const unsigned si = atomicAdd(&P.status->spill, 1u);
+            if (si < P.parts.spill_cap) {
+                SpillRec &sr = P.parts.spill[si];
+                sr.a = ra;
+                sr.b = *reinterpret_cast<const uint4 *>(&rb);
+                sr.cell = (int)key;
+            } else {
+                err |= DSMC_EBIT_SPILL_FULL;
+            }
+        }
+    }
+    const unsigned over = __ballot_sync(0xffffffffu, spilled) & peers;
+    if (valid && lane == leader && over) atomicSub(&top_out[key], (unsigned)__popc(over));
+}
+
+// New active cell of a particle that completed its flight; false when the
+// particle ended in a cell without free volume (stranded: it stays out).
+__device__ __forceinline__ bool new_cell(const SysDev &g, const Split32::Particle &p, unsigned &key) {
+    const int ac = __ldg(g.cell_map + Split32::cell_global(g, p));
+    key = (unsigned)ac;
+    return ac >= 0;
+}
+
+// Appends the warp's collected wall flights to the list (one atomic per
+// batch).  All lanes call.
+__device__ __forceinline__ void flush_walls(const PassParams &P, PlaceSmem &W) {
+    const int lane = threadIdx.x & 31;
+    const int qn = W.qn;
+    unsigned at = 0;
+    if (lane == 0 && qn) at = atomicAdd(&P.status->walls, (unsigned)qn);
+    at = __shfl_sync(0xffffffffu, at, 0);
+    if (lane < qn) {
+        if (at + lane < P.parts.walls_cap) P.parts.walls[at + lane] = W.q[lane];
+        else atomicOr(&P.status->error, DSMC_EBIT_SPILL_FULL);  // cannot happen: one entry per slot at most
+    }
+    __syncwarp();
+    if (lane == 0) W.qn = 0;
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(32 * P_WARPS, 8) place_movers_kernel(const __grid_constant__ PassParams P) {
+    __shared__ PlaceSmem smem[P_WARPS];
+    const int lane = threadIdx.x & 31;
+    const volatile Status *vs = P.status;
+    if (vs->halted) return;
+    PlaceSmem &W = smem[threadIdx.x >> 5];
+    if (lane == 0) W.qn = 0;
+    __syncwarp();
+    const uint4 *Aout = reinterpret_cast<const uint4 *>(P.parts.A[P.cur ^ 1]);
+    const float4 *Bout = reinterpret_cast<const float4 *>(P.parts.B[P.cur ^ 1]);
+
+    MoveCounts cnt;
+    counts_reset(cnt);
+    int tsys = -1;
+
+    const int C = P.cells.num_cells;
+    const int nchunks = (C + 31) >> 5;
+    for (int ch = blockIdx.x * P_WARPS + (threadIdx.x >> 5); ch < nchunks; ch += gridDim.x * P_WARPS) {
+        const int first = ch * 32;
+        const bool mine = lane < C - first;
+        // lane i: the movers of cell i sit in output slots [gap, gap + cnt)
+        int gap = 0, mv = 0, sys = -1;
+        if (mine) {
+            const int a = first + lane;
+            const int4 m = P.cells.meta[a];
+            unsigned nb, nt;
+            input_counts(P, a, m, nb, nt);
+            const unsigned nfs = min(P.cells.bot[P.cout][a], nb + nt);
+            gap = m.x + (int)nfs;
+            mv = (int)(nb + nt - nfs);
+            sys = m.w;
+        }
+        // exclusive prefix of the mover counts over the chunk's cells
+        int incl = mv;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        const int pre = mine ? incl - mv : 0x7fffffff;
+        for (int f0 = 0; f0 < total; f0 += 32) {
+            const int f = f0 + lane;
+            const bool valid = f < total;
+            // cell of mover f: the last cell whose prefix is <= f
+            int c = 0;
+#pragma unroll
+            for (int s = 16; s > 0; s >>= 1) {
+                const int pc = __shfl_sync(0xffffffffu, pre, (c + s) & 31);
+                if (c + s < 32 && pc <= f) c += s;
+            }
+            const int slot = __shfl_sync(0xffffffffu, gap, c) + (f - __shfl_sync(0xffffffffu, pre, c));
+            const int psys = __shfl_sync(0xffffffffu, sys, c);
+            const int csys = common_system(valid, psys);
+            if (csys != tsys) {
+                counts_publish(P, tsys, cnt, false);
+                tsys = csys;
+            }
+            Split32::Particle p;
+            MoveTally mt;
+            mt.wall_hits = mt.reseeds = 0;
+            mt.cross[0] = mt.cross[1] = mt.cross[2] = 0;
+            mt.err = 0;
+            bool done = false, place = false;
+            unsigned key = 0;
+            if (valid) {
+                Split32::unpack(Aout[slot], Bout[slot], p);
+                const SysDev &g = P.sys[psys];
+                done = Split32::move_open(g, p, mt);
+                if (done) {
+                    place = new_cell(g, p, key);
+                    if (!place) {
+                        mt.err |= DSMC_EBIT_STRANDED;
+                        ++cnt.stranded;
+                    }
+                }
+            }
+            // flights that meet a wall stay in their slot for place_walls
+            const unsigned wall = __ballot_sync(0xffffffffu, valid && !done);
+            if (wall) {
+                if (W.qn + __popc(wall) > WQ) flush_walls(P, W);
+                if (valid && !done) W.q[W.qn + __popc(wall & ((1u << lane) - 1u))] = make_int2(slot, psys);
+                __syncwarp();
+                if (lane == 0) W.qn += __popc(wall);
+                __syncwarp();
+            }
+            insert_top(P, p, place, key, mt.err);
+            counts_add(cnt, mt);
+            if (tsys == -2) counts_publish(P, psys, cnt, true);
+        }
+    }
+    if (W.qn) flush_walls(P, W);
+    counts_publish(P, tsys, cnt, false);
+}
+
+// The general mover for every listed wall flight, one per thread, then the
+// placement.  The last block ends the pass: it advances the step and halts
+// the pipeline if anything spilled or failed.
+__global__ void __launch_bounds__(32 * W_WARPS) place_walls_kernel(const __grid_constant__ PassParams P) {
+    const int lane = threadIdx.x & 31;
+    const volatile Status *vs = P.status;
+    if (vs->halted) return;
+    const uint32_t move_step = vs->step + 1;
+    const unsigned nwalls = min(vs->walls, P.parts.walls_cap);
+    const uint4 *Aout = reinterpret_cast<const uint4 *>(P.parts.A[P.cur ^ 1]);
+    const float4 *Bout = reinterpret_cast<const float4 *>(P.parts.B[P.cur ^ 1]);
+    MoveCounts cnt;
+    counts_reset(cnt);
+    int tsys = -1;
+    const unsigned wstride = gridDim.x * W_WARPS * 32u;
+    for (unsigned i0 = (blockIdx.x * W_WARPS + (threadIdx.x >> 5)) * 32u; i0 < nwalls; i0 += wstride) {
+        const unsigned i = i0 + lane;
+        const bool valid = i < nwalls;
+        const int2 e = valid ? P.parts.walls[i] : make_int2(0, -1);
+        const int csys = common_system(valid, e.y);
+        if (csys != tsys) {
+            counts_publish(P, tsys, cnt, false);
+            tsys = csys;
+        }
+        Split32::Particle p;
+        MoveTally mt;
+        mt.wall_hits = mt.reseeds = 0;
+        mt.cross[0] = mt.cross[1] = mt.cross[2] = 0;
+        mt.err = 0;
+        unsigned key = 0;
+        bool place = false;
+        if (valid) {
+            const SysDev &g = P.sys[e.y];
+            Split32::unpack(Aout[e.x], Bout[e.x], p);
+            Split32::move_general(g, p, move_step, mt);
+            place = new_cell(g, p, key);
+            if (!place) {
+                mt.err |= DSMC_EBIT_STRANDED;
+                ++cnt.stranded;
+            }
+        }
+        insert_top(P, p, place, key, mt.err);
+        counts_add(cnt, mt);
+        if (tsys == -2) counts_publish(P, e.y, cnt, true);
+    }
+    counts_publish(P, tsys, cnt, false);
+
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned done = atomicAdd(&P.status->blocks_done, 1u);
+        if (done == gridDim.x - 1) {
+            __threadfence();
+            if (P.advance_step) atomicAdd(&P.status->step, 1u);
+            if (atomicAdd(&P.status->spill, 0u) != 0u || (atomicAdd(&P.status->error, 0u) & DSMC_EBIT_FATAL) != 0u)
+                atomicExch(&P.status->halted, 1u);
+            atomicExch(&P.status->walls, 0u);
+            atomicExch(&P.status->blocks_done, 0u);
+        }
+    }
+}
+
+}  // namespace pass3
+}  // namespace dsmc
