@@ -148,7 +148,7 @@ struct Split32 {
 
     // System::find_position (dsmc/system.cpp:384-396): uniform in the box until
     // the voxel is empty.
-    static __device__ bool reseed(const SysDev &g, Particle &p, DrawStream &rs) {
+    static __device__ __forceinline__ bool reseed(const SysDev &g, Particle &p, DrawStream &rs) {
         for (int tries = 0; tries < 100000; ++tries) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) {
@@ -274,7 +274,8 @@ struct Split32 {
                 // fp32 offsets can round onto the face the fp64 reference stops
                 // 1e-7 time units short of; put the particle back outside.
                 if (outside && tau > 0.0f && p.c[0] == cb[0] && p.c[1] == cb[1] && p.c[2] == cb[2]) {
-                    const int out = side == 0 ? cb[axis] - 1 : cb[axis] + 1;
+                    const int cba = axis == 0 ? cb[0] : axis == 1 ? cb[1] : cb[2];  // no run-time index
+                    const int out = side == 0 ? cba - 1 : cba + 1;
                     const float oo = side == 0 ? one_minus_ulp() : 0.0f;
                     if (axis == 0) {
                         p.c[0] = out;
@@ -300,6 +301,151 @@ struct Split32 {
         }
         p.flag = here != DSMC_VOX_EMPTY;
         wrap(g, p, t);
+    }
+
+    // move_general as a state machine for a whole warp: every lane runs its
+    // own flight, and each turn of the loop issues at most one voxel lookup
+    // per lane at one program point, so the warp's lookups travel together
+    // instead of one divergent path after another.  The same arithmetic in
+    // the same order per particle as move_general.  All lanes call; inactive
+    // lanes only keep the loop company.
+    static __device__ __forceinline__ void move_general_warp(const SysDev &g, Particle &p, uint32_t step,
+                                                             MoveTally &t, bool active) {
+        enum { S_START, S_FIRST, S_BISECT, S_FACET, S_REFLECT, S_DONE };
+        DrawStream rs;
+        rs.init(g.seed, p.id, step, DSMC_TAG_MOVE);
+        float w[3] = {p.v[0] * g.inv_vox_f[0], p.v[1] * g.inv_vox_f[1], p.v[2] * g.inv_vox_f[2]};
+        float dt = g.dt_f, tau = 0.0f;
+        int here = p.flag ? DSMC_VOX_WALL : DSMC_VOX_EMPTY;
+        int depth = 0, count = 0, vt = DSMC_VOX_EMPTY;
+        int c0[3] = {0, 0, 0}, cb[3] = {0, 0, 0};
+        float o0[3] = {0.0f, 0.0f, 0.0f};
+        int state = active ? S_START : S_DONE;
+        while (__any_sync(0xffffffffu, state != S_DONE)) {
+            bool look = false;
+            while (state != S_DONE && !look) {
+                if (state == S_START) {
+                    if (here != DSMC_VOX_EMPTY) {
+                        ++t.reseeds;
+                        if (!reseed(g, p, rs)) t.err |= DSMC_EBIT_RESEED;
+                        here = DSMC_VOX_EMPTY;
+                        state = S_DONE;
+                    } else {
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            c0[a] = p.c[a];
+                            o0[a] = p.o[a];
+                        }
+                        tau = dt;
+                        advance(p.c, p.o, w, tau);
+                        look = true;
+                        state = S_FIRST;
+                    }
+                } else if (state == S_FIRST) {
+                    if (vt == DSMC_VOX_EMPTY) {
+                        state = S_DONE;
+                    } else {
+                        count = 0;
+                        state = S_BISECT;
+                    }
+                } else if (state == S_BISECT) {
+                    // bisect back out of solid (wall) voxels until a boundary voxel
+                    if (vt == DSMC_VOX_BOUNDARY) {
+                        cb[0] = p.c[0];
+                        cb[1] = p.c[1];
+                        cb[2] = p.c[2];
+                        count = 0;
+                        state = S_FACET;
+                    } else if (++count > 100) {
+                        ++t.reseeds;
+                        if (!reseed(g, p, rs)) t.err |= DSMC_EBIT_RESEED;
+                        state = S_DONE;
+                    } else if (vt == DSMC_VOX_WALL) {
+                        tau *= 0.5f;
+                        advance(p.c, p.o, w, -tau);
+                        look = true;
+                    } else {
+                        dt -= tau;
+                        if (dt > 1e-5f && depth < 10) {
+                            ++depth;
+                            state = S_START;
+                        } else {
+                            state = S_DONE;
+                        }
+                    }
+                } else if (state == S_FACET) {
+                    // back off and stop just short of the first boundary voxel's face
+                    if (vt != DSMC_VOX_BOUNDARY) {
+                        state = S_REFLECT;
+                    } else if (++count > 100) {
+                        ++t.reseeds;
+                        if (!reseed(g, p, rs)) t.err |= DSMC_EBIT_RESEED;
+                        state = S_DONE;
+                    } else {
+                        cb[0] = p.c[0];
+                        cb[1] = p.c[1];
+                        cb[2] = p.c[2];
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            p.c[a] = c0[a];
+                            p.o[a] = o0[a];
+                        }
+                        float d[3];
+                        bool outside = false;
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            d[a] = (float)(p.c[a] - cb[a]) + p.o[a];
+                            outside |= (d[a] < 0.0f) | (d[a] >= 1.0f);
+                        }
+                        int axis, side;
+                        const float tf = facet_time(d, w, axis, side);
+                        if (tf < 0.0f) {
+                            t.err |= DSMC_EBIT_FACET;
+                            ++t.reseeds;
+                            if (!reseed(g, p, rs)) t.err |= DSMC_EBIT_RESEED;
+                            state = S_DONE;
+                        } else {
+                            tau = tf;
+                            advance(p.c, p.o, w, tau);
+                            if (outside && tau > 0.0f && p.c[0] == cb[0] && p.c[1] == cb[1] && p.c[2] == cb[2]) {
+                                const int cba = axis == 0 ? cb[0] : axis == 1 ? cb[1] : cb[2];  // no run-time index
+                                const int out = side == 0 ? cba - 1 : cba + 1;
+                                const float oo = side == 0 ? one_minus_ulp() : 0.0f;
+                                if (axis == 0) {
+                                    p.c[0] = out;
+                                    p.o[0] = oo;
+                                } else if (axis == 1) {
+                                    p.c[1] = out;
+                                    p.o[1] = oo;
+                                } else {
+                                    p.c[2] = out;
+                                    p.o[2] = oo;
+                                }
+                            }
+                            look = true;
+                        }
+                    }
+                } else {  // S_REFLECT
+                    here = vt;
+                    dt -= tau;
+                    reflect(g, voxel_linear(g, cb[0], cb[1], cb[2]), p.v, rs);
+                    ++t.wall_hits;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) w[d] = p.v[d] * g.inv_vox_f[d];
+                    if (!(dt > 1e-5f && depth < 10)) {
+                        state = S_DONE;
+                    } else {
+                        ++depth;
+                        state = S_START;
+                    }
+                }
+            }
+            if (look) vt = voxel_type(g, p.c[0], p.c[1], p.c[2]);
+        }
+        if (active) {
+            p.flag = here != DSMC_VOX_EMPTY;
+            wrap(g, p, t);
+        }
     }
 
     // Periodic wrap, one box length at most, counting net crossings
@@ -516,7 +662,7 @@ struct Fp64 {
 
     // System::find_position (dsmc/system.cpp:384-396) with Grid::get_voxel(r, n)
     // (dsmc/grid.cpp:63-69): all-double index arithmetic.
-    static __device__ bool reseed(const SysDev &g, Particle &p, DrawStream &rs) {
+    static __device__ __forceinline__ bool reseed(const SysDev &g, Particle &p, DrawStream &rs) {
         for (int tries = 0; tries < 100000; ++tries) {
 #pragma unroll
             for (int d = 0; d < 3; ++d) p.r[d] = 0.0 + g.L[d] * rs.uniform64();

@@ -29,6 +29,14 @@
 //
 // Top slots are taken from the top of the cell down and never below
 // base + n_in(cell), so they cannot meet the bottom segment or the gap.
+//
+// Member order: move_cells writes each cell's stayers in id order, so a
+// bottom segment is normally sorted by id and only the few arrivals of the
+// top segment are out of order.  The id rank of a member (the reference's
+// cell-list order) is then its bottom position plus the arrivals below it,
+// which collide_cells and move_cells compute with one shuffle and ballot per
+// arrival.  A cell whose bottom segment is not sorted (after a repack or the
+// stand-alone stage kernels) is ranked in full and leaves move_cells sorted.
 #pragma once
 #include "engine.cuh"
 
@@ -80,12 +88,12 @@ __device__ __forceinline__ int common_system(bool valid, int sys) {
 // ---- collide_cells ----------------------------------------------------------
 
 constexpr int C_WARPS = 4;
-constexpr int PCAP = 512;    // ranked members per warp and batch (>= the largest cell)
-constexpr int IDCAP = 256;   // ids of a cell of more than 32 members while it is ranked
+constexpr int PCAP = 512;    // members per warp and batch (>= the largest cell)
 
 struct CollideSmem {
-    int perm[PCAP];
-    uint32_t ids[IDCAP];
+    uint32_t ids[PCAP];  // batch members: ids and slots, cell by cell
+    int slot[PCAP];
+    int perm[PCAP];      // batch members by id rank within each cell
 };
 
 // Velocities of one cell's members in the input buffer, by id rank.
@@ -177,55 +185,115 @@ __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __gri
         // run the batch's candidate loops one cell per lane.
         unsigned todo = __ballot_sync(0xffffffffu, pairs > 0);
         while (todo) {
-            int off = 0, my_off = 0;
+            // the batch: colliding cells, in order, whose members fit PCAP
             unsigned ready = 0;
-            while (todo) {
-                const int c = __ffs(todo) - 1;
+            {
+                int off = 0;
+                for (unsigned t2 = todo; t2;) {
+                    const int c = __ffs(t2) - 1;
+                    const int nc = __shfl_sync(0xffffffffu, n, c);
+                    if (off + nc > PCAP) break;  // off > 0 here: nc <= PCAP
+                    off += nc;
+                    ready |= 1u << c;
+                    t2 &= t2 - 1u;
+                }
+            }
+            todo &= ~ready;
+            // offsets of the batch cells' members: exclusive prefix over lanes
+            const bool rb = (ready >> lane) & 1u;
+            const int nr = rb ? n : 0;
+            int incl = nr;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int start = incl - nr;
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            // ids and slots of every batch member: independent loads
+            for (int f0 = 0; f0 < total; f0 += 32) {
+                const int f = f0 + lane;
+                int c = 0;  // the last lane whose start is <= f: a batch cell holding member f
+#pragma unroll
+                for (int st = 16; st > 0; st >>= 1) {
+                    const int sc = __shfl_sync(0xffffffffu, start, c + st);
+                    if (sc <= f) c += st;
+                }
+                const int k = f - __shfl_sync(0xffffffffu, start, c);
+                const int cb = __shfl_sync(0xffffffffu, m.x, c), cc = __shfl_sync(0xffffffffu, m.y, c);
+                const int cnb = (int)__shfl_sync(0xffffffffu, nb, c), cnt = __shfl_sync(0xffffffffu, n, c) - cnb;
+                if (f < total) {
+                    const int sl = member_slot(cb, cc, cnb, cnt, k);
+                    W.slot[f] = sl;
+                    W.ids[f] = __float_as_uint(Bin[sl].w);
+                }
+            }
+            __syncwarp();
+            // id ranks, cell by cell
+            for (unsigned t2 = ready; t2; t2 &= t2 - 1u) {
+                const int c = __ffs(t2) - 1;
+                const int off = __shfl_sync(0xffffffffu, start, c);
                 const int nc = __shfl_sync(0xffffffffu, n, c);
-                if (off + nc > PCAP) break;  // the batch is full (off > 0 here: nc <= PCAP)
-                const int base = __shfl_sync(0xffffffffu, m.x, c);
-                const int cap = __shfl_sync(0xffffffffu, m.y, c);
                 const int nbc = (int)__shfl_sync(0xffffffffu, nb, c);
                 const int ntc = nc - nbc;
                 if (nc <= 32) {
-                    const int sl = lane < nc ? member_slot(base, cap, nbc, ntc, lane) : 0;
-                    const uint32_t id = lane < nc ? __float_as_uint(Bin[sl].w) : 0xffffffffu;
+                    const uint32_t id = lane < nc ? W.ids[off + lane] : 0xffffffffu;
+                    const uint32_t nxt = __shfl_down_sync(0xffffffffu, id, 1);
+                    const bool sorted = !__any_sync(0xffffffffu, lane + 1 < nbc && !(id < nxt));
                     int rank = 0;
+                    if (sorted) {
+                        // bottom position (or the bottom members below an
+                        // arrival) plus the arrivals below
+                        const unsigned bmask = nbc >= 32 ? 0xffffffffu : (1u << nbc) - 1u;
+                        unsigned add = 0, pb = 0;
+                        for (int i = 0; i < ntc; ++i) {
+                            const uint32_t t = __shfl_sync(0xffffffffu, id, nbc + i);
+                            add += t < id;
+                            const unsigned bl = __popc(bmask & __ballot_sync(0xffffffffu, id < t));
+                            if (lane == nbc + i) pb = bl;
+                        }
+                        rank = (lane < nbc ? lane : (int)pb) + (int)add;
+                    } else {
 #pragma unroll
-                    for (int r = 0; r < 32; ++r) rank += __shfl_sync(0xffffffffu, id, r) < id;
-                    if (lane < nc) W.perm[off + rank] = sl;
-                } else if (nc <= IDCAP) {
-                    for (int q = lane; q < nc; q += 32) W.ids[q] = __float_as_uint(Bin[member_slot(base, cap, nbc, ntc, q)].w);
-                    __syncwarp();
-                    for (int q = lane; q < nc; q += 32) {
-                        const uint32_t id = W.ids[q];
-                        int rank = 0;
-                        for (int r = 0; r < nc; ++r) rank += W.ids[r] < id;
-                        W.perm[off + rank] = member_slot(base, cap, nbc, ntc, q);
+                        for (int r = 0; r < 32; ++r) rank += __shfl_sync(0xffffffffu, id, r) < id;
                     }
-                    __syncwarp();
+                    if (lane < nc) W.perm[off + rank] = W.slot[off + lane];
                 } else {
+                    const uint32_t *ids = W.ids + off;
+                    bool viol = false;
+                    for (int q = lane; q + 1 < nbc; q += 32) viol |= !(ids[q] < ids[q + 1]);
+                    const bool sorted = !__any_sync(0xffffffffu, viol);
                     for (int q = lane; q < nc; q += 32) {
-                        const uint32_t id = __float_as_uint(Bin[member_slot(base, cap, nbc, ntc, q)].w);
+                        const uint32_t id = ids[q];
                         int rank = 0;
-                        for (int r = 0; r < nc; ++r)
-                            rank += __float_as_uint(Bin[member_slot(base, cap, nbc, ntc, r)].w) < id;
-                        W.perm[off + rank] = member_slot(base, cap, nbc, ntc, q);
+                        if (sorted) {
+                            if (q < nbc) {
+                                rank = q;
+                            } else {  // bottom members below: binary search
+                                int lo = 0, hi = nbc;
+                                while (lo < hi) {
+                                    const int mid = (lo + hi) >> 1;
+                                    if (ids[mid] < id) lo = mid + 1;
+                                    else hi = mid;
+                                }
+                                rank = lo;
+                            }
+                            for (int i = nbc; i < nc; ++i) rank += ids[i] < id;
+                        } else {
+                            for (int r = 0; r < nc; ++r) rank += ids[r] < id;
+                        }
+                        W.perm[off + rank] = W.slot[off + q];
                     }
                 }
-                if (lane == c) my_off = off;
-                off += nc;
-                ready |= 1u << c;
-                todo &= ~(1u << c);
             }
             __syncwarp();
-            if ((ready >> lane) & 1u) {
+            if (rb) {
                 const SysDev &g = P.sys[sys];
                 DrawStream rs;
                 rs.init(g.seed, (uint32_t)m.z, step, DSMC_TAG_COLLIDE);
                 RankVel vel;
                 vel.b = Bin;
-                vel.perm = W.perm + my_off;
+                vel.perm = W.perm + start;
                 unsigned long long c_ = 0;
                 ntc_loop<float>(rs, n, pairs, vr, vel, IdentityPerm(), c_);
                 col += (unsigned)c_;
@@ -287,7 +355,100 @@ template <int R> struct MoveSmem {
     uint4 A[R];
     float4 B[R];
     MoveTab tab[2];
+    uint16_t pref[R + 2];  // two-pass placement: stayers before each member
 };
+
+// accelerate, then the first flight when it stays inside the particle's
+// empty voxel (the reference's outcome: r += v dt lands in an empty voxel,
+// dsmc/moleculemover.cpp:74-77); false leaves the particle accelerated.
+__device__ __forceinline__ bool first_flight(const SysDev &g, Split32::Particle &p) {
+    Split32::accelerate(g, p);
+    if (p.flag) return false;
+    float x[3];
+    bool stay = true;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        x[d] = fmaf(p.v[d] * g.inv_vox_f[d], g.dt_f, p.o[d]);
+        stay &= (x[d] >= 0.0f) & (x[d] < 1.0f);
+    }
+    if (stay) {
+        p.o[0] = x[0];
+        p.o[1] = x[1];
+        p.o[2] = x[2];
+    }
+    return stay;
+}
+
+// One cell of at most 32 * NR members whose bottom segment is sorted by id,
+// held in registers (member q = 32 k + lane in p[k]): flight of every member,
+// then stayers to the bottom segment in id order and movers to the gap.
+// Returns the number of stayers.  All lanes call.
+template <int R, int NR>
+__device__ __forceinline__ unsigned place_sorted(const SysDev &g, const MoveSmem<R> &W, int tail, int base, int n,
+                                                 int nb, uint4 *Aout, float4 *Bout, int lane) {
+    const unsigned below = (1u << lane) - 1u;
+    Split32::Particle p[NR];
+    bool stay[NR];
+    uint32_t id[NR];
+    unsigned fast[NR], slow[NR], bm[NR], add[NR], pb[NR];
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+        const int q = 32 * k + lane;
+        const bool valid = q < n;
+        stay[k] = false;
+        if (valid) {
+            int r = tail + q;
+            if (r >= R) r -= R;
+            Split32::unpack(W.A[r], W.B[r], p[k]);
+            stay[k] = first_flight(g, p[k]);
+        }
+        id[k] = valid ? p[k].id : 0xffffffffu;
+        fast[k] = __ballot_sync(0xffffffffu, valid && stay[k]);
+        slow[k] = __ballot_sync(0xffffffffu, valid && !stay[k]);
+        const int nbk = nb - 32 * k;  // bottom members of chunk k
+        bm[k] = nbk >= 32 ? 0xffffffffu : nbk <= 0 ? 0u : (1u << nbk) - 1u;
+        add[k] = pb[k] = 0;
+    }
+    // each arrival i: staying arrivals below every member, bottom stayers
+    // below the arrival
+    for (int i = nb; i < n; ++i) {
+        const int li = i & 31;
+        const bool hi = NR > 1 && i >= 32;
+        const uint32_t t = __shfl_sync(0xffffffffu, hi ? id[NR - 1] : id[0], li);
+        const unsigned ts = ((hi ? fast[NR - 1] : fast[0]) >> li) & 1u;
+        unsigned bl = 0;
+#pragma unroll
+        for (int k = 0; k < NR; ++k) {
+            add[k] += ts && t < id[k];
+            bl += (unsigned)__popc(fast[k] & bm[k] & __ballot_sync(0xffffffffu, id[k] < t));
+        }
+        if (lane == li) {
+            if (hi) pb[NR - 1] = bl;
+            else pb[0] = bl;
+        }
+    }
+    unsigned fs_before = 0, mv_before = 0;  // bottom stayers and movers of the earlier chunks
+#pragma unroll
+    for (int k = 0; k < NR; ++k) {
+        const int q = 32 * k + lane;
+        if (q < n) {
+            const unsigned dst =
+                stay[k] ? (unsigned)base + (q < nb ? fs_before + (unsigned)__popc(fast[k] & bm[k] & below) : pb[k]) + add[k]
+                        : (unsigned)(base + n) - 1u - mv_before - (unsigned)__popc(slow[k] & below);
+            uint4 ra;
+            float4 rb;
+            Split32::pack(p[k], ra, rb);
+            Aout[dst] = ra;
+            Bout[dst] = rb;
+        }
+        fs_before += (unsigned)__popc(fast[k] & bm[k]);
+        mv_before += (unsigned)__popc(slow[k]);
+    }
+    unsigned nfs = 0;
+#pragma unroll
+    for (int k = 0; k < NR; ++k) nfs += (unsigned)__popc(fast[k]);
+    return nfs;
+}
 
 template <int R>
 __global__ void __launch_bounds__(32 * M_WARPS) move_cells_kernel(const __grid_constant__ PassParams P) {
@@ -411,47 +572,79 @@ __global__ void __launch_bounds__(32 * M_WARPS) move_cells_kernel(const __grid_c
         }
         const SysDev &g = P.sys[sys];
 
-        unsigned n_fs = 0, n_mv = 0;
-        for (int c0 = 0; c0 < n; c0 += 32) {
-            const int q = c0 + lane;
-            const bool valid = q < n;
-            Particle p;
-            bool stay = false;
-            if (valid) {
-                int r = tail + q;
-                if (r >= R) r -= R;
-                Split32::unpack(W.A[r], W.B[r], p);
-                Split32::accelerate(g, p);
-                if (!p.flag) {
-                    float x[3];
-                    stay = true;
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        x[d] = fmaf(p.v[d] * g.inv_vox_f[d], g.dt_f, p.o[d]);
-                        stay &= (x[d] >= 0.0f) & (x[d] < 1.0f);
+        const int nb = min((int)T.nb[ci], n), nt = n - nb;
+        auto ring = [&](int q) {
+            const int r = tail + q;
+            return r >= R ? r - R : r;
+        };
+        auto rid = [&](int q) { return __float_as_uint(W.B[ring(q)].w); };
+        bool viol = false;
+        for (int q = lane; q + 1 < nb; q += 32) viol |= !(rid(q) < rid(q + 1));
+        const bool sorted = !__any_sync(0xffffffffu, viol);
+        const unsigned below = (1u << lane) - 1u;
+
+        // Stayers go to the bottom segment in id order, movers to the gap.
+        unsigned n_fs;
+        if (sorted && n <= 32) {
+            n_fs = place_sorted<R, 1>(g, W, tail, base, n, nb, Aout, Bout, lane);
+        } else if (sorted && n <= 64) {
+            n_fs = place_sorted<R, 2>(g, W, tail, base, n, nb, Aout, Bout, lane);
+        } else {
+            // pass 1: every member's flight; the record goes back into the
+            // ring and pref[q] counts the stayers before member q
+            unsigned S = 0;
+            for (int c0 = 0; c0 < n; c0 += 32) {
+                const int q = c0 + lane;
+                const bool valid = q < n;
+                bool stay = false;
+                if (valid) {
+                    const int r = ring(q);
+                    Particle p;
+                    Split32::unpack(W.A[r], W.B[r], p);
+                    stay = first_flight(g, p);
+                    Split32::pack(p, W.A[r], W.B[r]);
+                }
+                const unsigned fast = __ballot_sync(0xffffffffu, valid && stay);
+                if (valid) W.pref[q] = (uint16_t)(S + (unsigned)__popc(fast & below));
+                S += (unsigned)__popc(fast);
+            }
+            if (lane == 0) W.pref[n] = (uint16_t)S;
+            __syncwarp();
+            // pass 2: stayers in id order, movers below the top of the gap
+            for (int c0 = 0; c0 < n; c0 += 32) {
+                const int q = c0 + lane;
+                if (q < n) {
+                    const int r = ring(q);
+                    const uint32_t id = rid(q);
+                    unsigned dst;
+                    if (W.pref[q + 1] > W.pref[q]) {
+                        unsigned pos;
+                        if (sorted) {
+                            int lb = q;  // bottom members below this id
+                            if (q >= nb) {
+                                int lo = 0, hi = nb;
+                                while (lo < hi) {
+                                    const int mid = (lo + hi) >> 1;
+                                    if (rid(mid) < id) lo = mid + 1;
+                                    else hi = mid;
+                                }
+                                lb = lo;
+                            }
+                            pos = W.pref[lb];
+                            for (int i = nb; i < n; ++i) pos += (W.pref[i + 1] > W.pref[i]) && rid(i) < id;
+                        } else {
+                            pos = 0;
+                            for (int i = 0; i < n; ++i) pos += (W.pref[i + 1] > W.pref[i]) && rid(i) < id;
+                        }
+                        dst = (unsigned)base + pos;
+                    } else {
+                        dst = (unsigned)(base + n) - 1u - ((unsigned)q - W.pref[q]);
                     }
-                    if (stay) {
-                        p.o[0] = x[0];
-                        p.o[1] = x[1];
-                        p.o[2] = x[2];
-                    }
+                    Aout[dst] = W.A[r];
+                    Bout[dst] = W.B[r];
                 }
             }
-            const unsigned fast = __ballot_sync(0xffffffffu, valid && stay);
-            const unsigned slow = __ballot_sync(0xffffffffu, valid && !stay);
-            const unsigned below = (1u << lane) - 1u;
-            if (valid) {
-                // stayers fill the bottom upwards, movers the gap downwards
-                const unsigned dst = stay ? (unsigned)base + n_fs + (unsigned)__popc(fast & below)
-                                          : (unsigned)(base + n) - 1u - n_mv - (unsigned)__popc(slow & below);
-                uint4 ra;
-                float4 rb;
-                Split32::pack(p, ra, rb);
-                Aout[dst] = ra;
-                Bout[dst] = rb;
-            }
-            n_fs += (unsigned)__popc(fast);
-            n_mv += (unsigned)__popc(slow);
+            n_fs = S;
         }
         if (lane == ci) nfs_mine = n_fs;
         moved += (unsigned)n;
@@ -711,11 +904,18 @@ __global__ void __launch_bounds__(32 * W_WARPS) place_walls_kernel(const __grid_
         mt.err = 0;
         unsigned key = 0;
         bool place = false;
+        // the lanes of a warp share their system unless it is mixed; a mixed
+        // warp moves its lanes one system at a time
+        const int s0 = valid ? e.y : -1;
+        if (valid) Split32::unpack(Aout[e.x], Bout[e.x], p);
+        for (unsigned todo = __ballot_sync(0xffffffffu, valid); todo;) {
+            const int sys = __shfl_sync(0xffffffffu, s0, __ffs(todo) - 1);
+            const bool mine = valid && s0 == sys;
+            Split32::move_general_warp(P.sys[sys], p, move_step, mt, mine);
+            todo &= ~__ballot_sync(0xffffffffu, mine);
+        }
         if (valid) {
-            const SysDev &g = P.sys[e.y];
-            Split32::unpack(Aout[e.x], Bout[e.x], p);
-            Split32::move_general(g, p, move_step, mt);
-            place = new_cell(g, p, key);
+            place = new_cell(P.sys[e.y], p, key);
             if (!place) {
                 mt.err |= DSMC_EBIT_STRANDED;
                 ++cnt.stranded;
