@@ -119,8 +119,12 @@ struct Split32 {
     // Grid::get_time_until_collision (dsmc/grid.h:82-137) in voxel units: the
     // earliest positive crossing of a face of voxel cb whose hit point lies on
     // that face (bounds inclusive), faces in the reference's order
-    // x-, x+, y-, y+, z-, z+; 0 below 1e-5, else minus 1e-7.
-    static __device__ __forceinline__ float facet_time(const float d[3], const float w[3], int &axis, int &side) {
+    // x-, x+, y-, y+, z-, z+; 0 below 1e-5, else minus 1e-7.  The particle is
+    // at whole-voxel offset dc = c - cb plus in-voxel offset o; the distance
+    // to a face is formed as (face - dc) - o, exact for the near faces where
+    // dc + o itself would round (a particle 2e-8 above a face is not on it).
+    static __device__ __forceinline__ float facet_time(const int dc[3], const float o[3], const float w[3], int &axis,
+                                                       int &side) {
         float best = 1e9f;
         axis = -1;
         side = 0;
@@ -128,11 +132,11 @@ struct Split32 {
         for (int a = 0; a < 3; ++a) {
 #pragma unroll
             for (int s = 0; s < 2; ++s) {
-                const float t = ((float)s - d[a]) / w[a];
+                const float t = ((float)(s - dc[a]) - o[a]) / w[a];
                 if (!(t > 0.0f && t < best)) continue;
                 const int b1 = (a + 1) % 3, b2 = (a + 2) % 3;
-                const float h1 = fmaf(w[b1], t, d[b1]);
-                const float h2 = fmaf(w[b2], t, d[b2]);
+                const float h1 = fmaf(w[b1], t, (float)dc[b1] + o[b1]);
+                const float h2 = fmaf(w[b2], t, (float)dc[b2] + o[b2]);
                 // fp32 hit points on an edge can round just outside the face
                 const float eps = 1e-6f;
                 if (h1 >= -eps && h1 <= 1.0f + eps && h2 >= -eps && h2 <= 1.0f + eps) {
@@ -253,15 +257,12 @@ struct Split32 {
                     p.c[a] = c0[a];
                     p.o[a] = o0[a];
                 }
-                float d[3];
-                bool outside = false;
+                int dc[3];
 #pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    d[a] = (float)(p.c[a] - cb[a]) + p.o[a];
-                    outside |= (d[a] < 0.0f) | (d[a] >= 1.0f);
-                }
+                for (int a = 0; a < 3; ++a) dc[a] = p.c[a] - cb[a];
+                const bool outside = (dc[0] | dc[1] | dc[2]) != 0;  // offsets lie in [0, 1)
                 int axis, side;
-                const float tf = facet_time(d, w, axis, side);
+                const float tf = facet_time(dc, p.o, w, axis, side);
                 if (tf < 0.0f) {
                     t.err |= DSMC_EBIT_FACET;
                     ++t.reseeds;
@@ -390,15 +391,12 @@ struct Split32 {
                             p.c[a] = c0[a];
                             p.o[a] = o0[a];
                         }
-                        float d[3];
-                        bool outside = false;
+                        int dc[3];
 #pragma unroll
-                        for (int a = 0; a < 3; ++a) {
-                            d[a] = (float)(p.c[a] - cb[a]) + p.o[a];
-                            outside |= (d[a] < 0.0f) | (d[a] >= 1.0f);
-                        }
+                        for (int a = 0; a < 3; ++a) dc[a] = p.c[a] - cb[a];
+                        const bool outside = (dc[0] | dc[1] | dc[2]) != 0;  // offsets lie in [0, 1)
                         int axis, side;
-                        const float tf = facet_time(d, w, axis, side);
+                        const float tf = facet_time(dc, p.o, w, axis, side);
                         if (tf < 0.0f) {
                             t.err |= DSMC_EBIT_FACET;
                             ++t.reseeds;
