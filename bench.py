@@ -236,6 +236,19 @@ def main():
     n_total = allreduce_sum(pg, float(N))
     value = n_total * args.steps / (ms_max / 1e3)
     err, spill = system.ctx.device_status()
+
+    # ---- per-kernel durations (CUDA events around each kernel of each pass,
+    # recorded by the library on its stream), after the timed region -------
+    pipelined = system.ctx.pass_info()["pipelined"] == 1
+    kernels = None
+    if pipelined:
+        k_t = max(3, min(args.steps, 20))
+        system.ctx.set_timing(True)
+        system.step(k_t)
+        pt = system.ctx.pass_times()
+        system.ctx.set_timing(False)
+        kernels = {k: pt[k] / pt["passes"] for k in ("collide_cells", "move_cells", "place_movers", "place_walls")}
+        kernels["passes"] = pt["passes"]
     tal = system.tallies()
 
     # ---- end to end through the C ABI with host buffers --------------------
@@ -262,15 +275,21 @@ def main():
     e2e_s = allreduce_max(pg, e2e_s)
     e2e_value = n_total * k_e2e / e2e_s
 
-    # ---- roofline of the fused pass (the only kernel in the timed loop) -----
+    # ---- roofline of the dominant kernel: move_cells streams every particle
+    # record in and out once (32 B read + 32 B written per particle-step) ----
     peak, peak_kind = measured_peaks()
-    achieved = BYTES_PER_PARTICLE_STEP * N * args.steps / (ms_rank / 1e3) / 1e9
+    if kernels:
+        dominant = "move_cells"
+        achieved = BYTES_PER_PARTICLE_STEP * N / (kernels["move_cells"] / 1e3) / 1e9
+    else:
+        dominant = "cell pass"
+        achieved = BYTES_PER_PARTICLE_STEP * N * args.steps / (ms_rank / 1e3) / 1e9
     traffic = None
-    tfile = ROOT / "profiles" / "fused_pass_traffic.json"
-    if tfile.exists():
+    tfile = ROOT / "profiles" / "move_cells_traffic.json"
+    if tfile.exists() and kernels:
         try:
             t = json.loads(tfile.read_text())
-            traffic = float(t["dram_bytes_per_particle_step"]) * N
+            traffic = float(t["dram_bytes_per_particle"]) * N
         except Exception:
             traffic = None
 
@@ -282,14 +301,15 @@ def main():
                    "particles_total": int(n_total), "atoms_per_molecule": W.atoms_per_molecule,
                    "parallelism": f"replicas x{world}", "l2": "particle state 2 x %.1f GB > 126 MB L2" % (
                        system.info().slots * 32 / 1e9)},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": BYTES_PER_PARTICLE_STEP * N},
+        "kernels_ms": kernels,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48 * N / k_e2e,
                 "d2h_bytes_per_step": (48 * N + 64 * k_e2e) / k_e2e, "steps": k_e2e},
-        # collide_cells + move_cells + place_movers per step (pipelined pass),
-        # one pass kernel per step otherwise
-        "gpu_launches": args.steps * (3 if system.ctx.pass_info()["pipelined"] else 1),
+        # collide_cells + move_cells + place_movers + place_walls per step
+        # (production pass), one pass kernel per step otherwise
+        "gpu_launches": args.steps * (4 if pipelined else 1),
         "clocks": clocks,
         "device_status": {"error_bits": err, "spill": spill},
         "pass": system.ctx.pass_info(),

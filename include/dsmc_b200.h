@@ -242,10 +242,21 @@ int dsmc_cells_set_state(dsmc_ctx *ctx, int sys_id, const double *vr_max, const 
  * pipeline stops after that step and the host re-lays the buffers out. */
 int dsmc_ctx_set_capacity(dsmc_ctx *ctx, double factor, int pad);
 
-/* Launch shape of the timestep pass: pipelined = 1 when the bulk-copy
- * pipelined split-precision kernel runs dsmc_step (0: the generic cell pass,
- * e.g. fp64 contexts), its grid and block, and the per-warp staging capacity. */
+/* Launch shape of the timestep pass: pipelined = 1 when the split-precision
+ * production pass (collide_cells, move_cells, place_movers, place_walls) runs
+ * dsmc_step (0: the generic cell pass, e.g. fp64 contexts), the grid and
+ * block of move_cells, and its per-warp staging ring in particles. */
 int dsmc_pass_info(dsmc_ctx *ctx, int *pipelined, int *grid, int *block, int *stage_capacity);
+
+/* Per-kernel timers of the production pass, the device-side counterpart of
+ * the reference's stage timers (the Moving / Colliding / Accelerating /
+ * Sampling lines of its report, dsmc/system.cpp and dsmc/dsmc_io.cpp).  With
+ * timing on, dsmc_step records a CUDA event around each kernel of each pass
+ * and waits for the pass to finish; turning it on or off clears the sums.
+ * dsmc_pass_times_get returns the summed milliseconds of collide_cells,
+ * move_cells, place_movers and place_walls and the number of timed passes. */
+int dsmc_ctx_set_timing(dsmc_ctx *ctx, int on);
+int dsmc_pass_times_get(dsmc_ctx *ctx, double ms[4], int64_t *passes);
 
 /* Reads the status of the last pass: bit flags of device-side errors. */
 int dsmc_device_status(dsmc_ctx *ctx, uint32_t *error_bits, uint32_t *spill);

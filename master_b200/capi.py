@@ -36,7 +36,8 @@ EXPORTED = [
     "dsmc_particles_count", "dsmc_particles_get", "dsmc_step", "dsmc_stage_move", "dsmc_stage_sort",
     "dsmc_stage_collide", "dsmc_stage_sample", "dsmc_tallies_get", "dsmc_tallies_reset", "dsmc_cells_get",
     "dsmc_cells_set_state", "dsmc_device_status", "dsmc_stream", "dsmc_counters_get", "dsmc_cells_layout",
-    "dsmc_ctx_set_capacity", "dsmc_pass_info", "dsmc_geometry_finish_gpu_noalloc",
+    "dsmc_ctx_set_capacity", "dsmc_pass_info", "dsmc_geometry_finish_gpu_noalloc", "dsmc_ctx_set_timing",
+    "dsmc_pass_times_get",
 ]
 
 
@@ -143,6 +144,8 @@ def load() -> C.CDLL:
         "dsmc_counters_get": [_P, C.c_int, C.POINTER(C.c_int64)],
         "dsmc_ctx_set_capacity": [_P, C.c_double, C.c_int],
         "dsmc_pass_info": [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
+        "dsmc_ctx_set_timing": [_P, C.c_int],
+        "dsmc_pass_times_get": [_P, _D, C.POINTER(C.c_int64)],
         "dsmc_cells_layout": [C.POINTER(Settings), C.c_uint32, C.c_uint32, C.c_uint32, _U8, C.c_int, _I32, _I32,
                               _I32, _D, _D, C.POINTER(C.c_int)],
     }

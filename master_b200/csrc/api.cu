@@ -111,6 +111,11 @@ struct dsmc_ctx {
     int grid = 0;
     int fused_grids[4] = {0, 0, 0, 0};  // production split-precision pass (collide, move, place, walls); 0 = not usable
     bool use_pipelined = true;
+    // per-kernel timers of the production pass (dsmc_ctx_set_timing)
+    bool timing = false;
+    cudaEvent_t tev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double tms[4] = {0, 0, 0, 0};
+    long long tpasses = 0;
     double cap_factor = 2.0;
     int cap_pad = 24;
 
@@ -328,7 +333,16 @@ int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, 
     cudaError_t e;
     if (mode == PASS_FUSED && ctx->use_pipelined && ctx->fused_grids[1] > 0) {
         P.top_only = 0;
-        e = split32::launch_fused(P, ctx->fused_grids, ctx->stream);
+        e = split32::launch_fused(P, ctx->fused_grids, ctx->stream, ctx->timing ? ctx->tev : nullptr);
+        if (e == cudaSuccess && ctx->timing) {
+            CK(cudaEventSynchronize(ctx->tev[4]));
+            for (int k = 0; k < 4; ++k) {
+                float ms = 0;
+                CK(cudaEventElapsedTime(&ms, ctx->tev[k], ctx->tev[k + 1]));
+                ctx->tms[k] += ms;
+            }
+            ++ctx->tpasses;
+        }
     } else {
         P.top_only = 1;
         e = is_fp64(ctx) ? fp64::launch_pass(mode, P, ctx->grid, ctx->block, ctx->stream)
@@ -482,6 +496,8 @@ void dsmc_ctx_destroy(dsmc_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    for (cudaEvent_t &e : ctx->tev)
+        if (e) cudaEventDestroy(e);
     cudaStream_t s = ctx->stream;
     delete ctx;
     cudaStreamDestroy(s);
@@ -1034,6 +1050,26 @@ int dsmc_pass_info(dsmc_ctx *ctx, int *pipelined, int *grid, int *block, int *st
     if (grid) *grid = pipe ? ctx->fused_grids[1] : ctx->grid;
     if (block) *block = pipe ? split32::fused_block() : ctx->block;
     if (stage_capacity) *stage_capacity = pipe ? split32::fused_capacity(ctx->smem_cap) : ctx->smem_cap;
+    return DSMC_OK;
+}
+
+int dsmc_ctx_set_timing(dsmc_ctx *ctx, int on) {
+    if (!ctx) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    if (on) {
+        for (cudaEvent_t &e : ctx->tev)
+            if (!e) CK(cudaEventCreate(&e));
+    }
+    ctx->timing = on != 0;
+    for (double &t : ctx->tms) t = 0;
+    ctx->tpasses = 0;
+    return DSMC_OK;
+}
+
+int dsmc_pass_times_get(dsmc_ctx *ctx, double ms[4], int64_t *passes) {
+    if (!ctx || !ms) return DSMC_ERR_ARG;
+    for (int k = 0; k < 4; ++k) ms[k] = ctx->tms[k];
+    if (passes) *passes = ctx->tpasses;
     return DSMC_OK;
 }
 

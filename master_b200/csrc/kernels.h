@@ -43,7 +43,8 @@ int fused_block();                  // threads per block of the production kerne
 // Persistent grids of collide_cells, move_cells, place_movers and
 // place_walls; 0 when one of them cannot be resident.
 int fused_grids(int smem_cap, int num_sms, int grids[4]);
-cudaError_t launch_fused(const PassParams &P, const int grids[4], cudaStream_t st);
+// ev: null, or five events recorded before each kernel and after the last
+cudaError_t launch_fused(const PassParams &P, const int grids[4], cudaStream_t st, cudaEvent_t *ev = nullptr);
 }  // namespace split32
 
 // Pass modes (engine.cuh PassMode).

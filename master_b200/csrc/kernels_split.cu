@@ -73,12 +73,14 @@ int fused_grids(int smem_cap, int num_sms, int grids[4]) {
     return 1;
 }
 
-cudaError_t launch_fused(const PassParams &P, const int grids[4], cudaStream_t st) {
+cudaError_t launch_fused(const PassParams &P, const int grids[4], cudaStream_t st, cudaEvent_t *ev) {
+    if (ev) cudaEventRecord(ev[0], st);
     if (P.do_collide || P.do_sample) {
         pass3::collide_cells_kernel<<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
+    if (ev) cudaEventRecord(ev[1], st);
     cudaError_t e = cudaErrorInvalidValue;
     switch (fused_capacity(P.smem_cap)) {
 #define X(r) \
@@ -87,11 +89,15 @@ cudaError_t launch_fused(const PassParams &P, const int grids[4], cudaStream_t s
 #undef X
     }
     if (e != cudaSuccess) return e;
+    if (ev) cudaEventRecord(ev[2], st);
     pass3::place_movers_kernel<<<grids[2], 32 * pass3::P_WARPS, 0, st>>>(P);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (ev) cudaEventRecord(ev[3], st);
     pass3::place_walls_kernel<<<grids[3], 32 * pass3::W_WARPS, 0, st>>>(P);
-    return cudaGetLastError();
+    e = cudaGetLastError();
+    if (ev) cudaEventRecord(ev[4], st);
+    return e;
 }
 
 }  // namespace split32

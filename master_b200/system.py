@@ -197,6 +197,18 @@ class Context:
         self.check(self.lib.dsmc_pass_info(self.handle, *(C.byref(v) for v in vals)))
         return dict(zip(("pipelined", "grid", "block", "stage_capacity"), (v.value for v in vals)))
 
+    def set_timing(self, on: bool) -> None:
+        self.check(self.lib.dsmc_ctx_set_timing(self.handle, 1 if on else 0))
+
+    def pass_times(self) -> dict:
+        """Summed milliseconds per production kernel since timing was turned on."""
+        ms = np.zeros(4)
+        n = C.c_int64()
+        self.check(self.lib.dsmc_pass_times_get(self.handle, ms.ctypes.data_as(C.POINTER(C.c_double)), C.byref(n)))
+        out = dict(zip(("collide_cells", "move_cells", "place_movers", "place_walls"), ms.tolist()))
+        out["passes"] = n.value
+        return out
+
     def device_status(self):
         e, s = C.c_uint32(), C.c_uint32()
         self.check(self.lib.dsmc_device_status(self.handle, C.byref(e), C.byref(s)))

@@ -82,4 +82,9 @@ PACKED_256 = Workload("packed_256", n=256, radius_voxels=6, porosity=0.5, geomet
 PACKED_256_SAMPLE = Workload("packed_256_sample64", n=64, radius_voxels=6, porosity=0.5, geometry_seed=1, cells=32,
                              atoms_per_molecule=simulators_per_cell_weight(2.5e24, 0.1, 2, 30))
 
-WORKLOADS = {w.name: w for w in (PACKED_64, PACKED_256, PACKED_256_SAMPLE)}
+# packed_256 at 1/8 the volume (128^3 voxels, ~3.9e6 particles, ~0.5 GB of
+# particle slots): above the 126 MB L2, small enough for full ncu captures.
+PACKED_128 = Workload("packed_128", n=128, radius_voxels=6, porosity=0.5, geometry_seed=1, cells=64,
+                      atoms_per_molecule=simulators_per_cell_weight(2.5e24, 0.1, 2, 30))
+
+WORKLOADS = {w.name: w for w in (PACKED_64, PACKED_128, PACKED_256, PACKED_256_SAMPLE)}
