@@ -97,6 +97,7 @@ struct dsmc_ctx {
     DevBuf<int2> walls;       // wall-flight list of the production pass (one entry per slot at most)
     int cur = 0;
     int cphase = 0;           // occupancy set the next pass reads
+    bool sorted = false;      // every bottom segment is sorted by id (a production pass ran last)
     bool pending = false;     // the last step's collide/sample has not run yet
     bool keys_valid = false;  // a stand-alone move stage left new cell keys
     // staging
@@ -236,6 +237,7 @@ int relayout(dsmc_ctx *ctx, long long total) {
     }
     ctx->cur = 0;
     ctx->cphase = 0;
+    ctx->sorted = false;  // the repack inserts in arrival order
     CK(cudaMemsetAsync(ctx->status.p, 0, sizeof(unsigned) * 2, ctx->stream));  // error, spill
     unsigned zero = 0;
     CK(cudaMemcpyAsync(&ctx->status.p->halted, &zero, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
@@ -323,6 +325,7 @@ int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, 
     P.parts = particle_arrays(ctx);
     P.cur = ctx->cur;
     P.cin = ctx->cphase;
+    P.sorted_in = ctx->sorted ? 1 : 0;
     P.cout = (ctx->cphase + 1) % 3;
     P.cclear = (ctx->cphase + 2) % 3;
     P.do_collide = do_collide;
@@ -333,6 +336,7 @@ int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, 
     cudaError_t e;
     if (mode == PASS_FUSED && ctx->use_pipelined && ctx->fused_grids[1] > 0) {
         P.top_only = 0;
+        ctx->sorted = true;  // move_cells leaves every bottom segment sorted
         e = split32::launch_fused(P, ctx->fused_grids, ctx->stream, ctx->timing ? ctx->tev : nullptr);
         if (e == cudaSuccess && ctx->timing) {
             CK(cudaEventSynchronize(ctx->tev[4]));
@@ -345,6 +349,7 @@ int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, 
         }
     } else {
         P.top_only = 1;
+        if (mode != PASS_INPLACE) ctx->sorted = false;  // the generic passes fill top segments only
         e = is_fp64(ctx) ? fp64::launch_pass(mode, P, ctx->grid, ctx->block, ctx->stream)
                          : split32::launch_pass(mode, P, ctx->grid, ctx->block, ctx->stream);
     }

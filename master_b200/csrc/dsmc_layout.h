@@ -159,6 +159,7 @@ struct PassParams {
     int cur;                   // buffer read this pass
     int cin, cout, cclear;     // count sets: read, written, cleared this pass
     int top_only;              // every placement takes a top slot (generic passes)
+    int sorted_in;             // every bottom segment of the input is sorted by id
     int do_collide;            // collide the cells of the pass's input (step - 1's sort)
     int do_move;               // accelerate + move + re-bin (step)
     int do_sample;             // sample after the collide, on the reference's cadence

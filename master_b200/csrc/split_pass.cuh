@@ -89,11 +89,14 @@ __device__ __forceinline__ int common_system(bool valid, int sys) {
 
 constexpr int C_WARPS = 4;
 constexpr int PCAP = 512;    // members per warp and batch (>= the largest cell)
+constexpr int NTMAX = 8;     // arrivals a lane merges on its own (sorted bottom segments)
 
 struct CollideSmem {
     uint32_t ids[PCAP];  // batch members: ids and slots, cell by cell
     int slot[PCAP];
-    int perm[PCAP];      // batch members by id rank within each cell
+    int perm[PCAP];      // batch members by id rank within each cell (warp-ranked cells)
+    int apos[32 * (NTMAX + 1)];   // lane i: its cell's arrivals in id order: merged rank
+    int aslot[32 * (NTMAX + 1)];  //   and slot (rows of NTMAX + 1: no bank conflicts)
 };
 
 // Velocities of one cell's members in the input buffer, by id rank.
@@ -115,6 +118,38 @@ struct RankVel {
 };
 struct IdentityPerm {
     __device__ __forceinline__ int operator[](int i) const { return i; }
+};
+// Velocities of a cell's members by slot.
+struct SlotVel {
+    float4 *b;
+    __device__ __forceinline__ void get(int s, float &x, float &y, float &z) const {
+        const float4 v = b[s];
+        x = v.x;
+        y = v.y;
+        z = v.z;
+    }
+    __device__ __forceinline__ void set(int s, float x, float y, float z) const {
+        float *q = reinterpret_cast<float *>(b + s);
+        q[0] = x;
+        q[1] = y;
+        q[2] = z;
+    }
+};
+// Slot of the member of id rank r in a cell whose bottom segment is sorted:
+// an arrival if one has merged rank r, else the bottom member r minus the
+// arrivals below.
+struct PickPerm {
+    const int *apos, *aslot;
+    int nt, base;
+    __device__ __forceinline__ int operator[](int r) const {
+        int below = 0;
+        for (int j = 0; j < nt; ++j) {
+            const int p = apos[j];
+            if (p == r) return aslot[j];
+            below += p < r;
+        }
+        return base + (r - below);
+    }
 };
 
 __device__ __forceinline__ void publish_collide(const PassParams &P, int sys, unsigned col, unsigned cand,
@@ -229,8 +264,41 @@ __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __gri
                 }
             }
             __syncwarp();
-            // id ranks, cell by cell
-            for (unsigned t2 = ready; t2; t2 &= t2 - 1u) {
+            // Cells with a sorted bottom and few arrivals: each lane sorts its
+            // cell's arrivals and finds their merged ranks by binary search.
+            const bool lp = rb && P.sorted_in && (int)nt <= NTMAX;
+            if (lp) {
+                uint32_t *ids = W.ids + start;
+                int *sl = W.slot + start;
+                const int b = (int)nb;
+                for (int j = b + 1; j < n; ++j) {
+                    const uint32_t id = ids[j];
+                    const int s = sl[j];
+                    int i = j - 1;
+                    while (i >= b && ids[i] > id) {
+                        ids[i + 1] = ids[i];
+                        sl[i + 1] = sl[i];
+                        --i;
+                    }
+                    ids[i + 1] = id;
+                    sl[i + 1] = s;
+                }
+                int *ap = W.apos + lane * (NTMAX + 1), *as = W.aslot + lane * (NTMAX + 1);
+                for (int j = 0; j < (int)nt; ++j) {
+                    const uint32_t id = ids[b + j];
+                    int lo = 0, hi = b;
+                    while (lo < hi) {
+                        const int mid = (lo + hi) >> 1;
+                        if (ids[mid] < id) lo = mid + 1;
+                        else hi = mid;
+                    }
+                    ap[j] = lo + j;
+                    as[j] = sl[b + j];
+                }
+            }
+            // The other cells: id ranks by the warp, cell by cell.
+            const unsigned wr = ready & ~__ballot_sync(0xffffffffu, lp);
+            for (unsigned t2 = wr; t2; t2 &= t2 - 1u) {
                 const int c = __ffs(t2) - 1;
                 const int off = __shfl_sync(0xffffffffu, start, c);
                 const int nc = __shfl_sync(0xffffffffu, n, c);
@@ -291,11 +359,22 @@ __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __gri
                 const SysDev &g = P.sys[sys];
                 DrawStream rs;
                 rs.init(g.seed, (uint32_t)m.z, step, DSMC_TAG_COLLIDE);
-                RankVel vel;
-                vel.b = Bin;
-                vel.perm = W.perm + start;
                 unsigned long long c_ = 0;
-                ntc_loop<float>(rs, n, pairs, vr, vel, IdentityPerm(), c_);
+                if (lp) {
+                    SlotVel vel;
+                    vel.b = Bin;
+                    PickPerm pick;
+                    pick.apos = W.apos + lane * (NTMAX + 1);
+                    pick.aslot = W.aslot + lane * (NTMAX + 1);
+                    pick.nt = (int)nt;
+                    pick.base = m.x;
+                    ntc_loop<float>(rs, n, pairs, vr, vel, pick, c_);
+                } else {
+                    RankVel vel;
+                    vel.b = Bin;
+                    vel.perm = W.perm + start;
+                    ntc_loop<float>(rs, n, pairs, vr, vel, IdentityPerm(), c_);
+                }
                 col += (unsigned)c_;
                 cand += (unsigned)pairs;
             }
@@ -579,7 +658,8 @@ __global__ void __launch_bounds__(32 * M_WARPS) move_cells_kernel(const __grid_c
         };
         auto rid = [&](int q) { return __float_as_uint(W.B[ring(q)].w); };
         bool viol = false;
-        for (int q = lane; q + 1 < nb; q += 32) viol |= !(rid(q) < rid(q + 1));
+        if (!P.sorted_in)
+            for (int q = lane; q + 1 < nb; q += 32) viol |= !(rid(q) < rid(q + 1));
         const bool sorted = !__any_sync(0xffffffffu, viol);
         const unsigned below = (1u << lane) - 1u;
 
