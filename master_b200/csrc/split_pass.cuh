@@ -458,15 +458,50 @@ __device__ __forceinline__ bool first_flight(const SysDev &g, Split32::Particle 
     return stay;
 }
 
+// A system's constants of the first flight, held in registers.
+struct FlightConst {
+    float inv_vox[3], dt, accel;
+    int flow_dir;
+};
+__device__ __forceinline__ FlightConst flight_const(const SysDev &g) {
+    FlightConst k;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) k.inv_vox[d] = g.inv_vox_f[d];
+    k.dt = g.dt_f;
+    k.accel = g.accel_dt_f;
+    k.flow_dir = g.flow_dir;
+    return k;
+}
+// first_flight on the packed record itself: the voxel index is never
+// unpacked (a stayer changes only its offsets, a mover only its velocity).
+// Bit for bit what unpack + first_flight + pack give.
+__device__ __forceinline__ bool first_flight_raw(const FlightConst &k, uint4 &a, float4 &b) {
+    b.x = k.flow_dir == 0 ? b.x + k.accel : b.x;
+    b.y = k.flow_dir == 1 ? b.y + k.accel : b.y;
+    b.z = k.flow_dir == 2 ? b.z + k.accel : b.z;
+    if (a.y >> 31) return false;  // the voxel is not empty: general mover
+    const float x0 = fmaf(b.x * k.inv_vox[0], k.dt, __uint_as_float(a.y));
+    const float x1 = fmaf(b.y * k.inv_vox[1], k.dt, __uint_as_float(a.z));
+    const float x2 = fmaf(b.z * k.inv_vox[2], k.dt, __uint_as_float(a.w));
+    const bool stay = (x0 >= 0.0f) & (x0 < 1.0f) & (x1 >= 0.0f) & (x1 < 1.0f) & (x2 >= 0.0f) & (x2 < 1.0f);
+    if (stay) {
+        a.y = __float_as_uint(x0);
+        a.z = __float_as_uint(x1);
+        a.w = __float_as_uint(x2);
+    }
+    return stay;
+}
+
 // One cell of at most 32 * NR members whose bottom segment is sorted by id,
 // held in registers (member q = 32 k + lane in p[k]): flight of every member,
 // then stayers to the bottom segment in id order and movers to the gap.
 // Returns the number of stayers.  All lanes call.
 template <int R, int NR>
-__device__ __forceinline__ unsigned place_sorted(const SysDev &g, const MoveSmem<R> &W, int tail, int base, int n,
-                                                 int nb, uint4 *Aout, float4 *Bout, int lane) {
+__device__ __forceinline__ unsigned place_sorted(const FlightConst &fc, const MoveSmem<R> &W, int tail, int base,
+                                                 int n, int nb, uint4 *Aout, float4 *Bout, int lane) {
     const unsigned below = (1u << lane) - 1u;
-    Split32::Particle p[NR];
+    uint4 ra[NR];
+    float4 rb[NR];
     bool stay[NR];
     uint32_t id[NR];
     unsigned fast[NR], slow[NR], bm[NR], add[NR], pb[NR];
@@ -478,10 +513,11 @@ __device__ __forceinline__ unsigned place_sorted(const SysDev &g, const MoveSmem
         if (valid) {
             int r = tail + q;
             if (r >= R) r -= R;
-            Split32::unpack(W.A[r], W.B[r], p[k]);
-            stay[k] = first_flight(g, p[k]);
+            ra[k] = W.A[r];
+            rb[k] = W.B[r];
+            stay[k] = first_flight_raw(fc, ra[k], rb[k]);
         }
-        id[k] = valid ? p[k].id : 0xffffffffu;
+        id[k] = valid ? __float_as_uint(rb[k].w) : 0xffffffffu;
         fast[k] = __ballot_sync(0xffffffffu, valid && stay[k]);
         slow[k] = __ballot_sync(0xffffffffu, valid && !stay[k]);
         const int nbk = nb - 32 * k;  // bottom members of chunk k
@@ -514,11 +550,8 @@ __device__ __forceinline__ unsigned place_sorted(const SysDev &g, const MoveSmem
             const unsigned dst =
                 stay[k] ? (unsigned)base + (q < nb ? fs_before + (unsigned)__popc(fast[k] & bm[k] & below) : pb[k]) + add[k]
                         : (unsigned)(base + n) - 1u - mv_before - (unsigned)__popc(slow[k] & below);
-            uint4 ra;
-            float4 rb;
-            Split32::pack(p[k], ra, rb);
-            Aout[dst] = ra;
-            Bout[dst] = rb;
+            Aout[dst] = ra[k];
+            Bout[dst] = rb[k];
         }
         fs_before += (unsigned)__popc(fast[k] & bm[k]);
         mv_before += (unsigned)__popc(slow[k]);
@@ -595,6 +628,7 @@ __global__ void __launch_bounds__(32 * M_WARPS) move_cells_kernel(const __grid_c
     unsigned nfs_mine = 0;             // lane i: bottom occupancy of cell i of the chunk in work
     unsigned moved = 0;                // particles moved, system tsys (warp-uniform)
     int tsys = -1;
+    FlightConst fc = {};               // constants of system tsys
 
     auto stage_ahead = [&]() {
         // (it, ii) moves past a full chunk as soon as its last cell is
@@ -648,10 +682,11 @@ __global__ void __launch_bounds__(32 * M_WARPS) move_cells_kernel(const __grid_c
             if (lane == 0 && tsys >= 0 && moved) atomicAdd(&P.tally[tsys].particle_steps, (unsigned long long)moved);
             moved = 0;
             tsys = sys;
+            fc = flight_const(P.sys[sys]);
         }
         const SysDev &g = P.sys[sys];
 
-        const int nb = min((int)T.nb[ci], n), nt = n - nb;
+        const int nb = min((int)T.nb[ci], n);
         auto ring = [&](int q) {
             const int r = tail + q;
             return r >= R ? r - R : r;
@@ -666,9 +701,9 @@ __global__ void __launch_bounds__(32 * M_WARPS) move_cells_kernel(const __grid_c
         // Stayers go to the bottom segment in id order, movers to the gap.
         unsigned n_fs;
         if (sorted && n <= 32) {
-            n_fs = place_sorted<R, 1>(g, W, tail, base, n, nb, Aout, Bout, lane);
+            n_fs = place_sorted<R, 1>(fc, W, tail, base, n, nb, Aout, Bout, lane);
         } else if (sorted && n <= 64) {
-            n_fs = place_sorted<R, 2>(g, W, tail, base, n, nb, Aout, Bout, lane);
+            n_fs = place_sorted<R, 2>(fc, W, tail, base, n, nb, Aout, Bout, lane);
         } else {
             // pass 1: every member's flight; the record goes back into the
             // ring and pref[q] counts the stayers before member q
