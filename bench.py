@@ -114,26 +114,18 @@ def dist_setup(args):
 
 
 def allreduce_max(pg, x: float) -> float:
-    if pg is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
+    from master_b200 import ensemble
+    return ensemble.reduce_max(pg, x)
 
 
 def allreduce_sum(pg, x: float) -> float:
-    if pg is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.SUM)
-    return float(t.item())
+    from master_b200 import ensemble
+    return ensemble.reduce_sum(pg, x)
 
 
 def barrier(pg):
-    if pg is not None:
-        pg.barrier()
+    from master_b200 import ensemble
+    ensemble.barrier(pg)
 
 
 def cpu_reference(steps: int, replicas: int | None = None):
@@ -293,6 +285,12 @@ def main():
         except Exception:
             traffic = None
 
+    # every rank's tallies on rank 0: one all-reduce over a table by rank
+    from master_b200 import ensemble
+    tot = ensemble.totals(ensemble.gather_tallies(pg, world, {rank: tal}))
+    physics = {"temperature_K_rank0": tal.temperature, "collisions": int(tot["collisions"]),
+               "wall_collisions": int(tot["wall_collisions"]), "reseeds": int(tot["reseeds"]),
+               "stranded": int(tot["stranded"]), "ranks": world}
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -313,9 +311,7 @@ def main():
         "clocks": clocks,
         "device_status": {"error_bits": err, "spill": spill},
         "pass": system.ctx.pass_info(),
-        "physics": {"temperature_K": tal.temperature, "collisions": tal.collisions,
-                    "wall_collisions": tal.wall_collisions, "reseeds": tal.reseeds,
-                    "stranded": tal.stranded},
+        "physics": physics,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:

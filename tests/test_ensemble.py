@@ -1,0 +1,68 @@
+"""Runs over several ranks (master_b200/ensemble.py): systems sharded across
+ranks, fp64 tallies gathered with one all-reduce, the slowest rank's time.
+Two gloo ranks on the CPU, as a launch of one process per GPU would run."""
+from __future__ import annotations
+
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from master_b200 import ensemble
+
+
+def test_assign_covers_every_system_once():
+    for world in (1, 2, 3, 8):
+        seen = sorted(s for r in range(world) for s in ensemble.assign(13, r, world))
+        assert seen == list(range(13))
+    with pytest.raises(ValueError):
+        ensemble.assign(4, 2, 2)
+
+
+def fake_tallies(sid: int) -> dict:
+    return {"collisions": 1000 + sid, "wall_collisions": 7 * sid, "reseeds": 0, "particle_steps": 10 ** 9 + sid,
+            "count_periodic": [sid, -sid, 2 * sid], "samples": 3, "candidates": 4000 + sid,
+            "kinetic_energy": 0.5 * sid, "stranded": 0}
+
+
+def _rank(rank: int, world: int, port: int, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        mine = ensemble.assign(5, rank, world)
+        table = ensemble.gather_tallies(dist, 5, {s: fake_tallies(s) for s in mine})
+        slowest = ensemble.reduce_max(dist, 10.0 + rank)
+        total = ensemble.reduce_sum(dist, float(len(mine)))
+        ensemble.barrier(dist)
+        out.put((rank, table, slowest, total))
+    finally:
+        dist.destroy_process_group()
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_two_gloo_ranks_gather_every_systems_tallies():
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [out.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    expect = np.stack([ensemble.tally_row(fake_tallies(s)) for s in range(5)])
+    for rank, table, slowest, total in res:
+        assert np.array_equal(table, expect)
+        assert slowest == 11.0 and total == 5.0
+    tot = ensemble.totals(expect)
+    assert tot["collisions"] == sum(1000 + s for s in range(5))
+    assert tot["count_periodic_y"] == -sum(range(5))
