@@ -65,6 +65,7 @@ typedef struct dsmc_settings {
     int sample_begin;           /* first step sampled (0: from the start) */
     uint64_t rng_seed;          /* key of the counter-based draws */
     char world[512];            /* world folder (the ini's `world`) */
+    int load_previous_state;    /* continue from state_files/ + Tocontinue (dsmc/main.cpp:37-55) */
 } dsmc_settings;
 
 /* Fills the reference's Python-driver defaults (dsmcconfig.py:14-77). */
@@ -73,6 +74,21 @@ int dsmc_settings_defaults(dsmc_settings *s);
  * `key = value` lines, getint = (int)strtod, getbool = "true".  Replaces
  * Settings::Settings (dsmc/settings.cpp:3-44). */
 int dsmc_settings_load_ini(const char *path, dsmc_settings *s);
+
+/* ---- state files and continuation ----------------------------------- */
+/* The reference's particle state file (DSMC_IO::save_state_to_file_binary /
+ * load_state_from_file_binary, dsmc/dsmc_io.cpp:82-159, one per rank as
+ * state_files/state%04d.bin): int32 N, then per particle rx ry rz vx vy vz as
+ * doubles.  Host only.  Read: *n is set to N; DSMC_ERR_CAPACITY if cap < N
+ * (r and v may be NULL to ask for N). */
+int dsmc_state_file_read(const char *path, int64_t cap, double *r, double *v, int64_t *n);
+int dsmc_state_file_write(const char *path, int64_t n, const double *r, const double *v);
+/* The reference's Tocontinue counters (dsmc/main.cpp:37-55 reads, :110-112
+ * writes): "t steps collisions wall_collisions" as text.  Host only; written
+ * with 17 significant digits (the reference writes 6). */
+int dsmc_tocontinue_read(const char *path, double *t, uint64_t *steps, uint64_t *collisions,
+                         uint64_t *wall_collisions);
+int dsmc_tocontinue_write(const char *path, double t, uint64_t steps, uint64_t collisions, uint64_t wall_collisions);
 
 /* ---- world files ---------------------------------------------------- */
 typedef struct dsmc_world_header {
@@ -235,6 +251,22 @@ int dsmc_tallies_reset(dsmc_ctx *ctx, int sys_id);
 int dsmc_cells_get(dsmc_ctx *ctx, int sys_id, int cap, int32_t *global_index, int32_t *count,
                    double *vr_max, double *rest, double *moments, double *volume, int *num_cells);
 int dsmc_cells_set_state(dsmc_ctx *ctx, int sys_id, const double *vr_max, const double *rest);
+
+/* Continuation (dsmc/main.cpp:37-55): the step counter, collisions and wall
+ * collisions of an earlier run, typically read from its Tocontinue; the time
+ * becomes t and the flux window restarts there (the reference's t0 = t). */
+int dsmc_continue_from(dsmc_ctx *ctx, int sys_id, double t, uint64_t steps, uint64_t collisions,
+                       uint64_t wall_collisions);
+
+/* Exact checkpoint of a context: every particle record in its own precision
+ * with its cell, each cell's (sigma c_r)_max, selection remainder and moment
+ * sums, every system's tallies, flux window and draw key, and the step
+ * counter -- the fields the reference's state file and Tocontinue leave out
+ * (dsmc/dsmc_io.cpp:82-159).  A context set up with the same systems and
+ * precision continues from it with the same trajectories as the context that
+ * wrote it (the draws are keyed by particle id and step). */
+int dsmc_checkpoint_save(dsmc_ctx *ctx, const char *path);
+int dsmc_checkpoint_load(dsmc_ctx *ctx, const char *path);
 
 /* Slot capacity policy of the cell-sorted particle buffers: a cell gets
  * ceil(factor * max(expected, present) + pad) slots (default 2.0, 24).  An

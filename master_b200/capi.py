@@ -37,7 +37,8 @@ EXPORTED = [
     "dsmc_stage_collide", "dsmc_stage_sample", "dsmc_tallies_get", "dsmc_tallies_reset", "dsmc_cells_get",
     "dsmc_cells_set_state", "dsmc_device_status", "dsmc_stream", "dsmc_counters_get", "dsmc_cells_layout",
     "dsmc_ctx_set_capacity", "dsmc_pass_info", "dsmc_geometry_finish_gpu_noalloc", "dsmc_ctx_set_timing",
-    "dsmc_pass_times_get",
+    "dsmc_pass_times_get", "dsmc_state_file_read", "dsmc_state_file_write", "dsmc_tocontinue_read",
+    "dsmc_tocontinue_write", "dsmc_continue_from", "dsmc_checkpoint_save", "dsmc_checkpoint_load",
 ]
 
 
@@ -59,7 +60,7 @@ class Settings(C.Structure):
         ("Lx", C.c_double), ("Ly", C.c_double), ("Lz", C.c_double), ("dt", C.c_double),
         ("alpha_n", C.c_double), ("alpha_t", C.c_double), ("viscosity", C.c_double),
         ("surface_model", C.c_int), ("sample_begin", C.c_int), ("rng_seed", C.c_uint64),
-        ("world", C.c_char * 512),
+        ("world", C.c_char * 512), ("load_previous_state", C.c_int),
     ]
 
 
@@ -146,6 +147,14 @@ def load() -> C.CDLL:
         "dsmc_pass_info": [_P, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
         "dsmc_ctx_set_timing": [_P, C.c_int],
         "dsmc_pass_times_get": [_P, _D, C.POINTER(C.c_int64)],
+        "dsmc_state_file_read": [C.c_char_p, C.c_int64, _D, _D, C.POINTER(C.c_int64)],
+        "dsmc_state_file_write": [C.c_char_p, C.c_int64, _D, _D],
+        "dsmc_tocontinue_read": [C.c_char_p, _D, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                 C.POINTER(C.c_uint64)],
+        "dsmc_tocontinue_write": [C.c_char_p, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64],
+        "dsmc_continue_from": [_P, C.c_int, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64],
+        "dsmc_checkpoint_save": [_P, C.c_char_p],
+        "dsmc_checkpoint_load": [_P, C.c_char_p],
         "dsmc_cells_layout": [C.POINTER(Settings), C.c_uint32, C.c_uint32, C.c_uint32, _U8, C.c_int, _I32, _I32,
                               _I32, _D, _D, C.POINTER(C.c_int)],
     }

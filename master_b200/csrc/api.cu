@@ -59,6 +59,7 @@ struct SysHost {
     DevBuf<int> cell_map_dev;         // global -> absolute active index
     SysDev dev;
     double t0_reduced = 0;            // time of the last tally reset
+    double t_offset = 0;              // t - step * dt after a continuation
     double sqrt_t_over_m = 0;
     double vr_max0 = 0;
 };
@@ -779,6 +780,188 @@ int dsmc_particles_init(dsmc_ctx *ctx, int sys_id, int64_t n) {
     return place_particles(ctx, sys_id, n, nullptr, nullptr);
 }
 
+// main.cpp:37-55: t, steps, collisions and wall collisions carried over from
+// an earlier run; the flux window restarts at t (system.t0 = t).
+int dsmc_continue_from(dsmc_ctx *ctx, int sys_id, double t, uint64_t steps, uint64_t collisions,
+                       uint64_t wall_collisions) {
+    if (!ctx || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+    if (steps > 0xffffffffULL) return fail(ctx, DSMC_ERR_CAPACITY, "the step counter holds 32 bits");
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    SysHost &h = *ctx->systems[sys_id];
+    SysTally T;
+    CK(cudaMemcpyAsync(&T, ctx->tally.p + sys_id, sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    T.collisions = collisions;
+    T.wall_hits = wall_collisions;
+    CK(cudaMemcpyAsync(ctx->tally.p + sys_id, &T, sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    const unsigned st = (unsigned)steps;
+    CK(cudaMemcpyAsync(&ctx->status.p->step, &st, sizeof(st), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    h.t0_reduced = t;
+    h.t_offset = t - (double)steps * h.settings.dt;
+    return DSMC_OK;
+}
+
+namespace {
+const char kCkptMagic[8] = {'D', 'S', 'M', 'C', 'B', '2', '0', '0'};
+struct CkptHeader {
+    char magic[8];
+    uint32_t version, step;
+    int32_t precision, num_systems, num_cells, pad;
+    uint64_t records;
+};
+struct CkptSystem {
+    int64_t num_particles;
+    uint32_t id_count;
+    int32_t active_begin, active_end, pad;
+    double t0_reduced, t_offset;
+    uint64_t rng_seed;
+    SysTally tally;
+};
+}  // namespace
+
+int dsmc_checkpoint_save(dsmc_ctx *ctx, const char *path) {
+    if (!ctx || !path) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    long long staged = 0;
+    rc = stage_present(ctx, 0, -1, &staged);  // every particle record with its cell key
+    if (rc) return rc;
+    const int C = ctx->num_cells, S = (int)ctx->systems.size();
+    const size_t half = ctx->rec_half();
+    std::vector<unsigned char> A(staged * half), B(staged * half);
+    std::vector<int> key(staged);
+    std::vector<double4> state(C);
+    std::vector<double> mom(8 * (size_t)C);
+    std::vector<SysTally> tally(S);
+    if (staged) {
+        CK(cudaMemcpyAsync(A.data(), ctx->fA.p, A.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(B.data(), ctx->fB.p, B.size(), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(key.data(), ctx->fkey.p, staged * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (C) {
+        CK(cudaMemcpyAsync(state.data(), ctx->state.p, C * sizeof(double4), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaMemcpyAsync(mom.data(), ctx->mom.p, mom.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    if (S) CK(cudaMemcpyAsync(tally.data(), ctx->tally.p, S * sizeof(SysTally), cudaMemcpyDeviceToHost, ctx->stream));
+    cudaError_t e;
+    Status st = read_status(ctx, &e);
+    CK(e);
+    CkptHeader hd;
+    std::memset(&hd, 0, sizeof(hd));
+    std::memcpy(hd.magic, kCkptMagic, 8);
+    hd.version = 1;
+    hd.step = st.step;
+    hd.precision = ctx->precision;
+    hd.num_systems = S;
+    hd.num_cells = C;
+    hd.records = (uint64_t)staged;
+    FILE *f = std::fopen(path, "wb");
+    if (!f) return fail(ctx, DSMC_ERR_IO, std::string("could not open ") + path);
+    bool ok = std::fwrite(&hd, sizeof(hd), 1, f) == 1;
+    for (int s = 0; s < S && ok; ++s) {
+        const SysHost &h = *ctx->systems[s];
+        CkptSystem cs;
+        std::memset(&cs, 0, sizeof(cs));
+        cs.num_particles = h.num_particles;
+        cs.id_count = h.id_count;
+        cs.active_begin = h.active_begin;
+        cs.active_end = h.active_end;
+        cs.t0_reduced = h.t0_reduced;
+        cs.t_offset = h.t_offset;
+        cs.rng_seed = h.settings.rng_seed;
+        cs.tally = tally[s];
+        ok = std::fwrite(&cs, sizeof(cs), 1, f) == 1;
+    }
+    ok = ok && std::fwrite(state.data(), sizeof(double4), C, f) == (size_t)C;
+    ok = ok && std::fwrite(mom.data(), sizeof(double), mom.size(), f) == mom.size();
+    ok = ok && std::fwrite(A.data(), 1, A.size(), f) == A.size();
+    ok = ok && std::fwrite(B.data(), 1, B.size(), f) == B.size();
+    ok = ok && std::fwrite(key.data(), sizeof(int), key.size(), f) == key.size();
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return fail(ctx, DSMC_ERR_IO, std::string("could not write ") + path);
+    return DSMC_OK;
+}
+
+int dsmc_checkpoint_load(dsmc_ctx *ctx, const char *path) {
+    if (!ctx || !path) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    FILE *f = std::fopen(path, "rb");
+    if (!f) return fail(ctx, DSMC_ERR_IO, std::string("could not open ") + path);
+    auto bad = [&](const char *why) {
+        std::fclose(f);
+        return fail(ctx, DSMC_ERR_CONFIG, std::string(path) + ": " + why);
+    };
+    CkptHeader hd;
+    if (std::fread(&hd, sizeof(hd), 1, f) != 1 || std::memcmp(hd.magic, kCkptMagic, 8) || hd.version != 1)
+        return bad("not a checkpoint of this library");
+    const int C = ctx->num_cells, S = (int)ctx->systems.size();
+    if (hd.precision != ctx->precision) return bad("written by a context of the other precision");
+    if (hd.num_systems != S || hd.num_cells != C) return bad("the context's systems differ from the checkpoint's");
+    std::vector<CkptSystem> cs(S);
+    if (S && std::fread(cs.data(), sizeof(CkptSystem), S, f) != (size_t)S) return bad("truncated");
+    for (int s = 0; s < S; ++s)
+        if (cs[s].active_begin != ctx->systems[s]->active_begin || cs[s].active_end != ctx->systems[s]->active_end)
+            return bad("the context's cells differ from the checkpoint's");
+    const long long R = (long long)hd.records;
+    const size_t half = ctx->rec_half();
+    std::vector<double4> state(C);
+    std::vector<double> mom(8 * (size_t)C);
+    std::vector<unsigned char> A(R * half), B(R * half);
+    std::vector<int> key(R);
+    bool ok = std::fread(state.data(), sizeof(double4), C, f) == (size_t)C;
+    ok = ok && std::fread(mom.data(), sizeof(double), mom.size(), f) == mom.size();
+    ok = ok && std::fread(A.data(), 1, A.size(), f) == A.size();
+    ok = ok && std::fread(B.data(), 1, B.size(), f) == B.size();
+    ok = ok && std::fread(key.data(), sizeof(int), key.size(), f) == key.size();
+    if (!ok) return bad("truncated");
+    std::fclose(f);
+    std::vector<unsigned> hist(std::max(C, 1), 0);
+    for (long long i = 0; i < R; ++i) {
+        if (key[i] < 0 || key[i] >= C) return fail(ctx, DSMC_ERR_CONFIG, "checkpoint record outside the cells");
+        ++hist[key[i]];
+    }
+    ctx->pending = false;  // the saved state had its collide and sample done
+    CK(ctx->fA.ensure(std::max<long long>(R, 1) * half));
+    CK(ctx->fB.ensure(std::max<long long>(R, 1) * half));
+    CK(ctx->fkey.ensure(std::max<long long>(R, 1)));
+    CK(ctx->hist.ensure(std::max(C, 1)));
+    if (R) {
+        CK(cudaMemcpyAsync(ctx->fA.p, A.data(), A.size(), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->fB.p, B.data(), B.size(), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->fkey.p, key.data(), R * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CK(cudaMemcpyAsync(ctx->hist.p, hist.data(), hist.size() * sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+    for (int s = 0; s < S; ++s) {
+        SysHost &h = *ctx->systems[s];
+        h.num_particles = cs[s].num_particles;
+        h.id_count = cs[s].id_count;
+        h.t0_reduced = cs[s].t0_reduced;
+        h.t_offset = cs[s].t_offset;
+        if (h.settings.rng_seed != cs[s].rng_seed) {
+            h.settings.rng_seed = cs[s].rng_seed;  // the draws continue the saved streams
+            h.dev.seed = cs[s].rng_seed;
+        }
+    }
+    int rc = upload_sys_table(ctx);
+    if (rc) return rc;
+    rc = relayout(ctx, R);
+    if (rc) return rc;
+    std::vector<SysTally> tally(S);
+    for (int s = 0; s < S; ++s) tally[s] = cs[s].tally;
+    if (C) {
+        CK(cudaMemcpyAsync(ctx->state.p, state.data(), C * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->mom.p, mom.data(), mom.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    if (S) CK(cudaMemcpyAsync(ctx->tally.p, tally.data(), S * sizeof(SysTally), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(&ctx->status.p->step, &hd.step, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DSMC_OK;
+}
+
 int dsmc_particles_count(dsmc_ctx *ctx, int sys_id, int64_t *n) {
     if (!ctx || !n || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
     *n = ctx->systems[sys_id]->num_particles;
@@ -916,7 +1099,7 @@ int dsmc_tallies_get(dsmc_ctx *ctx, int sys_id, dsmc_tallies *t) {
     t->samples = T.samples;
     t->candidates = T.candidates;
     t->stranded = T.stranded;
-    t->time = st.step * h.settings.dt;
+    t->time = st.step * h.settings.dt + h.t_offset;
     // MeasureEnergy / MeasureTemperature (dsmc/statisticalproperty.cpp:21-71)
     // from the current velocities, summed per cell and then in cell order.
     const int C = h.active_end - h.active_begin;
@@ -957,7 +1140,7 @@ int dsmc_tallies_reset(dsmc_ctx *ctx, int sys_id) {
     cudaError_t e;
     Status st = read_status(ctx, &e);
     CK(e);
-    h.t0_reduced = st.step * h.settings.dt;
+    h.t0_reduced = st.step * h.settings.dt + h.t_offset;
     return DSMC_OK;
 }
 

@@ -179,6 +179,8 @@ int dsmc_settings_load_ini(const char *path, dsmc_settings *s) {
         out = (int)d;
     };
     // Settings::Settings (dsmc/settings.cpp:3-44): every key is required.
+    if (const IniFile::Item *it = ini.find("load_previous_state")) s->load_previous_state = it->str == "true";
+    else missing = "load_previous_state";
     integer("statistics_interval", s->statistics_interval);
     integer("atoms_per_molecule", s->atoms_per_molecule);
     integer("timesteps", s->timesteps);
@@ -568,6 +570,107 @@ int dsmc_geometry_packed_spheres(const dsmc_sphere_params *p, uint8_t *vox, floa
         *porosity_out = (float)((double)e / V);
     }
     return DSMC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// State files and continuation counters (dsmc/dsmc_io.cpp:82-159,
+// dsmc/main.cpp:37-55 and 110-112).
+
+int dsmc_state_file_read(const char *path, int64_t cap, double *r, double *v, int64_t *n) {
+    if (!path || !n) return DSMC_ERR_ARG;
+    FILE *f = std::fopen(path, "rb");
+    if (!f) {
+        set_thread_error(std::string("Error, could not open file ") + path);
+        return DSMC_ERR_IO;
+    }
+    int32_t N = 0;
+    if (std::fread(&N, sizeof(N), 1, f) != 1 || N < 0) {
+        std::fclose(f);
+        set_thread_error(std::string("state file has no particle count: ") + path);
+        return DSMC_ERR_IO;
+    }
+    *n = N;
+    if (!r || !v) {
+        std::fclose(f);
+        return DSMC_OK;
+    }
+    if (cap < N) {
+        std::fclose(f);
+        set_thread_error("output buffers smaller than the state file's particle count");
+        return DSMC_ERR_CAPACITY;
+    }
+    std::vector<double> buf(6 * (size_t)N);
+    const bool ok = std::fread(buf.data(), sizeof(double), buf.size(), f) == buf.size();
+    std::fclose(f);
+    if (!ok) {
+        set_thread_error(std::string("state file shorter than its particle count: ") + path);
+        return DSMC_ERR_IO;
+    }
+    for (int64_t k = 0; k < N; ++k)
+        for (int d = 0; d < 3; ++d) {
+            r[3 * k + d] = buf[6 * k + d];
+            v[3 * k + d] = buf[6 * k + 3 + d];
+        }
+    return DSMC_OK;
+}
+
+int dsmc_state_file_write(const char *path, int64_t n, const double *r, const double *v) {
+    if (!path || n < 0 || n > 0x7fffffff || (n > 0 && (!r || !v))) return DSMC_ERR_ARG;
+    std::vector<double> buf(6 * (size_t)n);
+    for (int64_t k = 0; k < n; ++k)
+        for (int d = 0; d < 3; ++d) {
+            buf[6 * k + d] = r[3 * k + d];
+            buf[6 * k + 3 + d] = v[3 * k + d];
+        }
+    FILE *f = std::fopen(path, "wb");
+    if (!f) {
+        set_thread_error(std::string("Error, could not open file ") + path);
+        return DSMC_ERR_IO;
+    }
+    const int32_t N = (int32_t)n;
+    bool ok = std::fwrite(&N, sizeof(N), 1, f) == 1;
+    ok = ok && std::fwrite(buf.data(), sizeof(double), buf.size(), f) == buf.size();
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) {
+        set_thread_error(std::string("could not write ") + path);
+        return DSMC_ERR_IO;
+    }
+    return DSMC_OK;
+}
+
+int dsmc_tocontinue_read(const char *path, double *t, uint64_t *steps, uint64_t *collisions,
+                         uint64_t *wall_collisions) {
+    if (!path || !t || !steps || !collisions || !wall_collisions) return DSMC_ERR_ARG;
+    std::ifstream in(path);
+    if (!in.is_open()) {
+        set_thread_error(std::string("could not open ") + path);
+        return DSMC_ERR_IO;
+    }
+    // the reference extracts t, then the three counters as unsigned long
+    double tt = 0;
+    unsigned long long a = 0, b = 0, c = 0;
+    in >> tt >> a >> b >> c;
+    if (in.fail()) {
+        set_thread_error(std::string("Tocontinue needs 't steps collisions wall_collisions': ") + path);
+        return DSMC_ERR_IO;
+    }
+    *t = tt;
+    *steps = a;
+    *collisions = b;
+    *wall_collisions = c;
+    return DSMC_OK;
+}
+
+int dsmc_tocontinue_write(const char *path, double t, uint64_t steps, uint64_t collisions, uint64_t wall_collisions) {
+    if (!path) return DSMC_ERR_ARG;
+    FILE *f = std::fopen(path, "w");
+    if (!f) {
+        set_thread_error(std::string("could not open ") + path);
+        return DSMC_ERR_IO;
+    }
+    std::fprintf(f, "%.17g %llu %llu %llu", t, (unsigned long long)steps, (unsigned long long)collisions,
+                 (unsigned long long)wall_collisions);
+    return std::fclose(f) == 0 ? DSMC_OK : DSMC_ERR_IO;
 }
 
 }  // extern "C"

@@ -2,14 +2,19 @@
 // libdsmc_b200.  Reads dsmc.ini from the working directory, sets the system
 // up from the ini's world folder, runs `timesteps` steps (System::step +
 // StatisticsSampler::sample), prints the run's time analysis in the
-// reference's layout and writes the Tocontinue counters
-// (t steps collisions wall_collisions) as the reference does at the end.
+// reference's layout, and at the end writes the particle state
+// (state_files/state0000.bin) and the Tocontinue counters
+// (t steps collisions wall_collisions) as the reference does.  With
+// load_previous_state = true in the ini it continues from those two files
+// (dsmc/main.cpp:37-55, dsmc/system.cpp:412-415).
 //
 //   dsmc_b200_main [--fp64] [--device N]
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <sys/stat.h>
+#include <vector>
 
 #include "dsmc_b200.h"
 
@@ -41,7 +46,21 @@ int main(int argc, char **argv) {
     if ((rc = dsmc_ctx_create(device, precision, &ctx))) return die(ctx, "creating the context", rc);
     int sys = -1;
     if ((rc = dsmc_system_add_world(ctx, &s, &sys))) return die(ctx, "System::initialize", rc);
-    if ((rc = dsmc_particles_init(ctx, sys, -1))) return die(ctx, "setup_molecules", rc);
+    if (s.load_previous_state) {
+        double t = 0;
+        uint64_t steps = 0, collisions = 0, walls = 0;
+        if ((rc = dsmc_tocontinue_read("Tocontinue", &t, &steps, &collisions, &walls))) return die(ctx, "Tocontinue", rc);
+        int64_t n = 0;
+        if ((rc = dsmc_state_file_read("state_files/state0000.bin", 0, nullptr, nullptr, &n)))
+            return die(ctx, "load_state_from_file_binary", rc);
+        std::vector<double> r(3 * n), v(3 * n);
+        if ((rc = dsmc_state_file_read("state_files/state0000.bin", n, r.data(), v.data(), &n)))
+            return die(ctx, "load_state_from_file_binary", rc);
+        if ((rc = dsmc_particles_set(ctx, sys, n, r.data(), v.data()))) return die(ctx, "setting the state", rc);
+        if ((rc = dsmc_continue_from(ctx, sys, t, steps, collisions, walls))) return die(ctx, "continuing", rc);
+    } else if ((rc = dsmc_particles_init(ctx, sys, -1))) {
+        return die(ctx, "setup_molecules", rc);
+    }
     if ((rc = dsmc_sync(ctx))) return die(ctx, "initialisation", rc);
     const auto t_init = std::chrono::steady_clock::now();
 
@@ -74,12 +93,16 @@ int main(int argc, char **argv) {
     std::printf("collisions %llu, wall collisions %llu, T = %.3f K\n", (unsigned long long)t.collisions,
                 (unsigned long long)t.wall_collisions, t.temperature);
 
-    FILE *f = std::fopen("Tocontinue", "w");
-    if (f) {
-        std::fprintf(f, "%.17g %llu %llu %llu", t.time, (unsigned long long)t.step, (unsigned long long)t.collisions,
-                     (unsigned long long)t.wall_collisions);
-        std::fclose(f);
-    }
+    // save_state_to_file_binary (dsmc/dsmc_io.cpp:82-118) and Tocontinue
+    std::vector<double> r(3 * info.num_particles), v(3 * info.num_particles);
+    int64_t n = 0;
+    if ((rc = dsmc_particles_get(ctx, sys, info.num_particles, r.data(), v.data(), nullptr, &n)))
+        return die(ctx, "reading the state", rc);
+    mkdir("state_files", 0755);
+    if ((rc = dsmc_state_file_write("state_files/state0000.bin", n, r.data(), v.data())))
+        return die(ctx, "save_state_to_file_binary", rc);
+    if ((rc = dsmc_tocontinue_write("Tocontinue", t.time, t.step, t.collisions, t.wall_collisions)))
+        return die(ctx, "Tocontinue", rc);
     dsmc_ctx_destroy(ctx);
     return 0;
 }

@@ -153,6 +153,36 @@ def cells_layout(settings: Settings, geometry: Geometry) -> dict:
     return out
 
 
+def read_state_file(path) -> tuple[np.ndarray, np.ndarray]:
+    """The reference's state file (state_files/state%04d.bin,
+    dsmc/dsmc_io.cpp:82-159) as (r, v), each (N, 3) float64."""
+    lib = capi.load()
+    n = C.c_int64()
+    check(lib.dsmc_state_file_read(str(path).encode(), 0, None, None, C.byref(n)))
+    r = np.empty((n.value, 3))
+    v = np.empty((n.value, 3))
+    check(lib.dsmc_state_file_read(str(path).encode(), n.value, ptr(r, C.c_double), ptr(v, C.c_double), C.byref(n)))
+    return r, v
+
+
+def write_state_file(path, r, v) -> None:
+    r = np.ascontiguousarray(r, np.float64)
+    v = np.ascontiguousarray(v, np.float64)
+    check(capi.load().dsmc_state_file_write(str(path).encode(), len(r), ptr(r, C.c_double), ptr(v, C.c_double)))
+
+
+def read_tocontinue(path) -> dict:
+    """The reference's Tocontinue counters (dsmc/main.cpp:37-55)."""
+    t = C.c_double()
+    a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    check(capi.load().dsmc_tocontinue_read(str(path).encode(), C.byref(t), C.byref(a), C.byref(b), C.byref(c)))
+    return {"t": t.value, "steps": a.value, "collisions": b.value, "wall_collisions": c.value}
+
+
+def write_tocontinue(path, t: float, steps: int, collisions: int, wall_collisions: int) -> None:
+    check(capi.load().dsmc_tocontinue_write(str(path).encode(), t, steps, collisions, wall_collisions))
+
+
 class Context:
     """One GPU context holding any number of systems (geometry + gas)."""
 
@@ -196,6 +226,13 @@ class Context:
         vals = [C.c_int() for _ in range(4)]
         self.check(self.lib.dsmc_pass_info(self.handle, *(C.byref(v) for v in vals)))
         return dict(zip(("pipelined", "grid", "block", "stage_capacity"), (v.value for v in vals)))
+
+    def checkpoint_save(self, path) -> None:
+        """Exact checkpoint of every system of the context."""
+        self.check(self.lib.dsmc_checkpoint_save(self.handle, str(path).encode()))
+
+    def checkpoint_load(self, path) -> None:
+        self.check(self.lib.dsmc_checkpoint_load(self.handle, str(path).encode()))
 
     def set_timing(self, on: bool) -> None:
         self.check(self.lib.dsmc_ctx_set_timing(self.handle, 1 if on else 0))
@@ -274,6 +311,11 @@ class System:
         rest = np.ascontiguousarray(rest, np.float64)
         self.ctx.check(self.ctx.lib.dsmc_cells_set_state(self.ctx.handle, self.id, ptr(vr_max, C.c_double),
                                                          ptr(rest, C.c_double)))
+
+    def continue_from(self, t: float, steps: int, collisions: int, wall_collisions: int) -> None:
+        """Carry over an earlier run's time and counters (dsmc/main.cpp:37-55)."""
+        self.ctx.check(self.ctx.lib.dsmc_continue_from(self.ctx.handle, self.id, t, steps, collisions,
+                                                       wall_collisions))
 
     def tallies(self) -> capi.Tallies:
         t = capi.Tallies()

@@ -61,3 +61,24 @@ def test_executable_runs_like_reference_main(tmp_path):
     assert "Time analysis" in r.stdout and "atom-timesteps / second" in r.stdout
     t, steps, collisions, walls = (tmp_path / "Tocontinue").read_text().split()
     assert int(steps) == 6 and int(walls) > 0 and float(t) > 0
+
+
+@pytest.mark.gpu
+def test_executable_continues_from_its_state_files(tmp_path):
+    """load_previous_state: the second run reads state_files/state0000.bin and
+    Tocontinue written by the first and carries the counters on."""
+    g = Geometry.packed_spheres(32, 3, wanted_porosity=0.6, seed=2)
+    (tmp_path / "worlds" / "test").mkdir(parents=True)
+    g.write_world(tmp_path / "worlds" / "test")
+    (tmp_path / "dsmc.ini").write_text(INI)
+    r = subprocess.run([str(EXE)], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    first = (tmp_path / "Tocontinue").read_text().split()
+    assert (tmp_path / "state_files" / "state0000.bin").exists()
+    (tmp_path / "dsmc.ini").write_text(INI.replace("load_previous_state = false", "load_previous_state = true"))
+    r = subprocess.run([str(EXE)], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    t, steps, collisions, walls = (tmp_path / "Tocontinue").read_text().split()
+    assert int(steps) == 12 and int(collisions) >= int(first[2]) and int(walls) > int(first[3])
+    assert float(t) > float(first[0])
+
