@@ -61,7 +61,8 @@ typedef struct dsmc_settings {
     double dt;                  /* reduced time */
     double alpha_n, alpha_t;
     double viscosity;
-    int surface_model;          /* 0 = thermal (diffuse) walls */
+    int surface_model;          /* wall model (dsmc/system.cpp:345-352): 0 thermal (diffuse),
+                                   1 specular, 2 cercignani_lampis (alpha_n, alpha_t) */
     int sample_begin;           /* first step sampled (0: from the start) */
     uint64_t rng_seed;          /* key of the counter-based draws */
     char world[512];            /* world folder (the ini's `world`) */

@@ -525,7 +525,10 @@ int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t
     if (s->cells_x <= 0 || s->cells_y <= 0 || s->cells_z <= 0) return fail(ctx, DSMC_ERR_CONFIG, "cells must be > 0");
     if (s->nx != 1 || s->ny != 1 || s->nz != 1)
         return fail(ctx, DSMC_ERR_CONFIG, "one system is one domain: processor grid must be 1 1 1");
-    if (s->surface_model != 0) return fail(ctx, DSMC_ERR_CONFIG, "only thermal walls are built");
+    if (s->surface_model < DSMC_WALL_THERMAL || s->surface_model > DSMC_WALL_CL)
+        return fail(ctx, DSMC_ERR_CONFIG, "unknown wall model");
+    if (s->surface_model == DSMC_WALL_CL && !(s->alpha_n > 0 && s->alpha_n <= 1 && s->alpha_t >= 0 && s->alpha_t <= 1))
+        return fail(ctx, DSMC_ERR_CONFIG, "Cercignani-Lampis accommodation needs 0 < alpha_n <= 1, 0 <= alpha_t <= 1");
     // System::validate_number_of_cells (dsmc/system.cpp:221-239).
     if (nx % s->cells_x || ny % s->cells_y || nz % s->cells_z)
         return fail(ctx, DSMC_ERR_CONFIG, "Error: voxel-cell-cpu configuration not good.");
@@ -613,6 +616,17 @@ int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t
     d.accel_dt_f = (float)d.accel_dt;
     d.wall_s = std::sqrt(wall_temperature / s->mass);
     d.wall_s_f = (float)d.wall_s;
+    d.wall_model = s->surface_model;
+    d.alpha_t = s->alpha_t;
+    d.sqrt_1m_an = std::sqrt(1 - s->alpha_n);
+    d.sqrt_1m_an_over_an = std::sqrt(1 - s->alpha_n) / s->alpha_n;
+    d.sqrt_an_over_2 = std::sqrt(s->alpha_n / 2);
+    d.cl_vmax = 1500.0 / ctx->units.v0;  // UnitConverter::velocity_from_SI(1500)
+    d.alpha_t_f = (float)d.alpha_t;
+    d.sqrt_1m_an_f = (float)d.sqrt_1m_an;
+    d.sqrt_1m_an_over_an_f = (float)d.sqrt_1m_an_over_an;
+    d.sqrt_an_over_2_f = (float)d.sqrt_an_over_2;
+    d.cl_vmax_f = (float)d.cl_vmax;
     d.seed = s->rng_seed;
     d.sample_interval = s->statistics_interval;
     d.sample_begin = s->sample_begin;

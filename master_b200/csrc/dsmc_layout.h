@@ -43,13 +43,14 @@
 #define DSMC_EBIT_NAN 32u        // non-finite position or velocity
 #define DSMC_EBIT_TIMEOUT 128u   // a bounded wait on a bulk copy ran out
 #define DSMC_EBIT_ALIGN 256u     // a bulk copy operand was not 16-byte aligned (copy skipped)
+#define DSMC_EBIT_WALL 512u      // the Cercignani-Lampis sampler accepted nothing within its limit
 #define DSMC_EBIT_STRANDED 64u   // a move ended inside solid whose cell has no free volume; the
                                  // particle stays in its previous cell and is re-seeded next step
 // bits that stop the pipeline (a failed facet search or a stranded particle is
 // re-seeded, counted, and the pipeline goes on)
 #define DSMC_EBIT_FATAL \
     (DSMC_EBIT_CELL | DSMC_EBIT_RESEED | DSMC_EBIT_SPILL_FULL | DSMC_EBIT_SMEM | DSMC_EBIT_NAN | DSMC_EBIT_TIMEOUT | \
-     DSMC_EBIT_ALIGN)
+     DSMC_EBIT_ALIGN | DSMC_EBIT_WALL)
 
 #define DSMC_VOX_PACK(i, j, k) ((uint32_t)(i) | ((uint32_t)(j) << 11) | ((uint32_t)(k) << 22))
 #define DSMC_VOX_I(p) ((int)((p)&0x7FFu))
@@ -91,10 +92,19 @@ struct SysDev {
     int flow_dir;              // -1: no acceleration
     double wall_s;             // sqrt(T_wall/m) (dsmc/system.cpp:343)
     float wall_s_f;
+    // wall model (dsmc/system.cpp:345-352): DSMC_WALL_* and the constants of
+    // Random(seed, alpha_n, alpha_t) (dsmc/random.cpp:8-15)
+    int wall_model;
+    double alpha_t, sqrt_1m_an, sqrt_1m_an_over_an, sqrt_an_over_2, cl_vmax;
+    float alpha_t_f, sqrt_1m_an_f, sqrt_1m_an_over_an_f, sqrt_an_over_2_f, cl_vmax_f;
     uint64_t seed;
     int sample_interval;       // sample when step % interval == 0 and step >= sample_begin
     int sample_begin;
 };
+
+#define DSMC_WALL_THERMAL 0    // diffuse reflection at the wall temperature
+#define DSMC_WALL_SPECULAR 1
+#define DSMC_WALL_CL 2         // Cercignani-Lampis
 
 struct SysTally {
     unsigned long long collisions;

@@ -53,6 +53,66 @@ struct MoveTally {
 // ============================================================================
 // Split precision: int voxel + fp32 offset in [0,1) voxel units, fp32 velocity.
 // ============================================================================
+// ---- wall models besides the diffuse wall ----------------------------------
+// ColliderSpecular (dsmc/colliderspecular.cpp:8-32) and
+// ColliderCercignaniLampis (dsmc/collidercercignanilampis.cpp:13-45) with
+// Random::next_cercignani_lampis_normal_component (dsmc/random.cpp:70-91).
+
+// Modified Bessel function I0 by the polynomial approximations of Abramowitz
+// & Stegun (1964), eqs. 9.8.1 (|x| < 3.75) and 9.8.2 (|x| >= 3.75), nested as
+// the reference's Random::bessel_i0 evaluates them (dsmc/random.cpp:27-40).
+template <class real> __device__ __forceinline__ real bessel_i0_as(real x) {
+    const real ax = fabs(x);
+    if (ax < (real)3.75) {
+        real y = x / (real)3.75;
+        y *= y;
+        return (real)1.0 +
+               y * ((real)3.5156229 +
+                    y * ((real)3.0899424 +
+                         y * ((real)1.2067492 + y * ((real)0.2659732 + y * ((real)0.360768e-1 + y * (real)0.45813e-2)))));
+    }
+    const real y = (real)3.75 / ax;
+    return (exp(ax) / sqrt(ax)) *
+           ((real)0.39894228 +
+            y * ((real)0.1328592e-1 +
+                 y * ((real)0.225319e-2 +
+                      y * ((real)-0.157565e-2 +
+                           y * ((real)0.916281e-2 +
+                                y * ((real)-0.2057706e-1 +
+                                     y * ((real)0.2635537e-1 + y * ((real)-0.1647633e-1 + y * (real)0.392377e-2))))))));
+}
+
+// Random::next_gauss (dsmc/random.cpp:21-25) on a draw stream: the ln(1-U)
+// draw first.
+template <class real> __device__ __forceinline__ real gauss_draw(DrawStream &rs) {
+    const real u1 = rs.template uniform<real>();
+    const real u2 = rs.template uniform<real>();
+    return sqrt((real)-2.0 * log((real)1.0 - u1)) * cos((real)6.283185307 * u2);
+}
+
+// The reference's rejection sampler loops until it accepts; here it gives up
+// after DSMC_CL_TRIALS and the caller records DSMC_EBIT_WALL.
+#define DSMC_CL_TRIALS 100000
+template <class real>
+__device__ __forceinline__ bool cl_normal(real v_norm_in, real factor, real max_v_out, real sqrt_an_over_2,
+                                          real sqrt_1m_an, real sqrt_1m_an_over_an, DrawStream &rs, real &out) {
+    max_v_out /= factor;
+    v_norm_in /= factor;
+    const real std_dev = sqrt_an_over_2;
+    const real mu = sqrt_1m_an * v_norm_in;
+    for (int trial = 0; trial < DSMC_CL_TRIALS; ++trial) {
+        const real v_out = std_dev * gauss_draw<real>(rs) + mu;
+        const real u = rs.template uniform<real>();
+        const real arg = (real)2 * sqrt_1m_an_over_an * v_norm_in * v_out;
+        const real b = v_out * exp(-arg) * bessel_i0_as<real>(arg) / max_v_out;
+        if (b >= u) {
+            out = v_out * factor;
+            return true;
+        }
+    }
+    return false;
+}
+
 struct Split32 {
     typedef float real;
     typedef uint4 RecA;
@@ -169,8 +229,37 @@ struct Split32 {
         return false;
     }
 
-    // ColliderThermal::collide (dsmc/colliderthermal.cpp:13-46).
-    static __device__ __forceinline__ void reflect(const SysDev &g, uint32_t vlin, float v[3], DrawStream &rs) {
+    // The wall model's collide: ColliderThermal::collide
+    // (dsmc/colliderthermal.cpp:13-46), ColliderSpecular::collide or
+    // ColliderCercignaniLampis::collide.  Returns error bits.
+    static __device__ __forceinline__ unsigned reflect(const SysDev &g, uint32_t vlin, float v[3], DrawStream &rs) {
+        if (g.wall_model != DSMC_WALL_THERMAL) {
+            const float *np = g.nrm + 3 * (size_t)vlin, *ap = g.t1 + 3 * (size_t)vlin, *bp = g.t2 + 3 * (size_t)vlin;
+            const float n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
+            const float a0 = __ldg(ap), a1 = __ldg(ap + 1), a2 = __ldg(ap + 2);
+            const float b0 = __ldg(bp), b1 = __ldg(bp + 1), b2 = __ldg(bp + 2);
+            const float vni = v[0] * n0 + v[1] * n1 + v[2] * n2;
+            const float vt1i = v[0] * a0 + v[1] * a1 + v[2] * a2;
+            const float vt2i = v[0] * b0 + v[1] * b1 + v[2] * b2;
+            float vn, vt1, vt2;
+            if (g.wall_model == DSMC_WALL_SPECULAR) {
+                vn = -vni;
+                vt1 = vt1i;
+                vt2 = vt2i;
+            } else {
+                const float factor = sqrtf(2.0f) * g.wall_s_f;
+                if (!cl_normal<float>(vni, factor, g.cl_vmax_f, g.sqrt_an_over_2_f, g.sqrt_1m_an_f,
+                                      g.sqrt_1m_an_over_an_f, rs, vn))
+                    return DSMC_EBIT_WALL;
+                const float sigma = 1.0f - sqrtf(1.0f - g.alpha_t_f);
+                vt1 = gauss_draw<float>(rs) * sqrtf(g.alpha_t_f) * g.wall_s_f + vt1i * (1.0f - sigma);
+                vt2 = gauss_draw<float>(rs) * sqrtf(g.alpha_t_f) * g.wall_s_f + vt2i * (1.0f - sigma);
+            }
+            v[0] = vn * n0 + vt1 * a0 + vt2 * b0;
+            v[1] = vn * n1 + vt1 * a1 + vt2 * b1;
+            v[2] = vn * n2 + vt1 * a2 + vt2 * b2;
+            return 0;
+        }
         const float s = g.wall_s_f;
         const float vn = s * sqrtf(-2.0f * logf(rs.uniform32()));
         float u = rs.uniform32();
@@ -185,6 +274,7 @@ struct Split32 {
         const float *b = g.t2 + 3 * (size_t)vlin;
 #pragma unroll
         for (int d = 0; d < 3; ++d) v[d] = vn * __ldg(n + d) + vt1 * __ldg(a + d) + vt2 * __ldg(b + d);
+        return 0;
     }
 
     // MoleculeMover::move_molecule (dsmc/moleculemover.cpp:50-126) with its
@@ -294,7 +384,7 @@ struct Split32 {
             if (stop) break;
             here = vt;
             dt -= tau;
-            reflect(g, voxel_linear(g, cb[0], cb[1], cb[2]), p.v, rs);
+            t.err |= reflect(g, voxel_linear(g, cb[0], cb[1], cb[2]), p.v, rs);
             ++t.wall_hits;
 #pragma unroll
             for (int d = 0; d < 3; ++d) w[d] = p.v[d] * g.inv_vox_f[d];
@@ -426,7 +516,7 @@ struct Split32 {
                 } else {  // S_REFLECT
                     here = vt;
                     dt -= tau;
-                    reflect(g, voxel_linear(g, cb[0], cb[1], cb[2]), p.v, rs);
+                    t.err |= reflect(g, voxel_linear(g, cb[0], cb[1], cb[2]), p.v, rs);
                     ++t.wall_hits;
 #pragma unroll
                     for (int d = 0; d < 3; ++d) w[d] = p.v[d] * g.inv_vox_f[d];
@@ -674,7 +764,38 @@ struct Fp64 {
     }
 
     // ColliderThermal::collide (dsmc/colliderthermal.cpp:13-46).
-    static __device__ __forceinline__ void reflect(const SysDev &g, uint32_t vlin, double v[3], DrawStream &rs) {
+    static __device__ __forceinline__ unsigned reflect(const SysDev &g, uint32_t vlin, double v[3], DrawStream &rs) {
+        if (g.wall_model != DSMC_WALL_THERMAL) {
+            // the reference's mix: float wall frames, double velocities
+            const float *np = g.nrm + 3 * (size_t)vlin, *ap = g.t1 + 3 * (size_t)vlin, *bp = g.t2 + 3 * (size_t)vlin;
+            const float n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2);
+            const float a0 = __ldg(ap), a1 = __ldg(ap + 1), a2 = __ldg(ap + 2);
+            const float b0 = __ldg(bp), b1 = __ldg(bp + 1), b2 = __ldg(bp + 2);
+            if (g.wall_model == DSMC_WALL_SPECULAR) {
+                const double vn = n0 * v[0] + n1 * v[1] + n2 * v[2];
+                const double vt1 = a0 * v[0] + a1 * v[1] + a2 * v[2];
+                const double vt2 = b0 * v[0] + b1 * v[1] + b2 * v[2];
+                v[0] = -vn * n0 + vt1 * a0 + vt2 * b0;
+                v[1] = -vn * n1 + vt1 * a1 + vt2 * b1;
+                v[2] = -vn * n2 + vt1 * a2 + vt2 * b2;
+                return 0;
+            }
+            const double factor = sqrt(2.0) * g.wall_s;
+            const double vni = v[0] * n0 + v[1] * n1 + v[2] * n2;
+            const double vt1i = v[0] * a0 + v[1] * a1 + v[2] * a2;
+            const double vt2i = v[0] * b0 + v[1] * b1 + v[2] * b2;
+            double vn;
+            if (!cl_normal<double>(vni, factor, g.cl_vmax, g.sqrt_an_over_2, g.sqrt_1m_an, g.sqrt_1m_an_over_an, rs,
+                                   vn))
+                return DSMC_EBIT_WALL;
+            const double sigma = 1 - sqrt(1 - g.alpha_t);
+            const double vt1 = gauss_draw<double>(rs) * sqrt(g.alpha_t) * g.wall_s + vt1i * (1 - sigma);
+            const double vt2 = gauss_draw<double>(rs) * sqrt(g.alpha_t) * g.wall_s + vt2i * (1 - sigma);
+            v[0] = vn * n0 + vt1 * a0 + vt2 * b0;
+            v[1] = vn * n1 + vt1 * a1 + vt2 * b1;
+            v[2] = vn * n2 + vt1 * a2 + vt2 * b2;
+            return 0;
+        }
         const double s = g.wall_s;
         const double vn = s * sqrt(-2 * log(rs.uniform64()));
         double u = rs.uniform64();
@@ -692,6 +813,7 @@ struct Fp64 {
             const float nf = __ldg(n + d), af = __ldg(a + d), bf = __ldg(b + d);
             v[d] = vn * nf + vt1 * af + vt2 * bf;
         }
+        return 0;
     }
 
     static __device__ bool move(const SysDev &g, Particle &p, uint32_t step, MoveTally &t) {
@@ -758,7 +880,7 @@ struct Fp64 {
             }
             if (stop) break;
             dt -= tau;
-            reflect(g, voxel_linear(g, b[0], b[1], b[2]), p.v, rs);
+            t.err |= reflect(g, voxel_linear(g, b[0], b[1], b[2]), p.v, rs);
             ++t.wall_hits;
             if (!(dt > 1e-5 && depth < 10)) break;
         }

@@ -210,8 +210,16 @@ int dsmc_settings_load_ini(const char *path, dsmc_settings *s) {
     const IniFile::Item *model = ini.find("surface_interaction_model");
     if (!model) {
         if (missing.empty()) missing = "surface_interaction_model";
-    } else if (model->str != "thermal") {
-        set_thread_error("surface_interaction_model '" + model->str + "' is not built; only 'thermal'");
+    } else if (model->str == "thermal") {
+        s->surface_model = DSMC_WALL_THERMAL;
+    } else if (model->str == "specular") {
+        s->surface_model = DSMC_WALL_SPECULAR;
+    } else if (model->str == "cercignani_lampis") {
+        s->surface_model = DSMC_WALL_CL;
+    } else {
+        // "maxwell" is a stub in the reference (dsmc/collidermaxwell.cpp:13-16)
+        set_thread_error("surface_interaction_model '" + model->str +
+                         "' has no model; thermal, specular and cercignani_lampis are built");
         return DSMC_ERR_CONFIG;
     }
     const IniFile::Item *world = ini.find("world");

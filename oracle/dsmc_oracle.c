@@ -121,7 +121,77 @@ static void find_position(const oracle_system *s, double r[3], draws *d) {
 }
 
 /* ColliderThermal::collide (dsmc/colliderthermal.cpp:13-46). */
+/* Random::bessel_i0 (dsmc/random.cpp:27-40): the modified Bessel function I0
+ * by Abramowitz & Stegun (1964) 9.8.1 and 9.8.2, in the reference's nesting. */
+static double bessel_i0(double x) {
+    const double ax = fabs(x);
+    if (ax < 3.75) {
+        double y = x / 3.75;
+        y *= y;
+        return 1.0 + y * (3.5156229 + y * (3.0899424 + y * (1.2067492 + y * (0.2659732 + y * (0.360768e-1 +
+                                                                                               y * 0.45813e-2)))));
+    }
+    const double y = 3.75 / ax;
+    return (exp(ax) / sqrt(ax)) *
+           (0.39894228 +
+            y * (0.1328592e-1 +
+                 y * (0.225319e-2 +
+                      y * (-0.157565e-2 +
+                           y * (0.916281e-2 +
+                                y * (-0.2057706e-1 + y * (0.2635537e-1 + y * (-0.1647633e-1 + y * 0.392377e-2))))))));
+}
+
+/* Random::next_cercignani_lampis_normal_component (dsmc/random.cpp:70-91):
+ * rejection sampling; 0 with *ok = 0 when 100000 trials accept nothing. */
+static double cl_normal(const oracle_system *s, double v_norm_in, double factor, double max_v_out, draws *d,
+                        int *ok) {
+    max_v_out /= factor;
+    v_norm_in /= factor;
+    const double std_dev = sqrt(s->alpha_n / 2);
+    const double mu = sqrt(1 - s->alpha_n) * v_norm_in;
+    const double k = sqrt(1 - s->alpha_n) / s->alpha_n;
+    for (long trial = 0; trial < 100000; ++trial) {
+        const double v_out = std_dev * gauss(d) + mu;
+        const double u = uni(d);
+        const double arg = 2 * k * v_norm_in * v_out;
+        const double bb = v_out * exp(-arg) * bessel_i0(arg) / max_v_out;
+        if (bb >= u) {
+            *ok = 1;
+            return v_out * factor;
+        }
+    }
+    *ok = 0;
+    return 0;
+}
+
+/* ColliderThermal (dsmc/colliderthermal.cpp:13-46), ColliderSpecular
+ * (dsmc/colliderspecular.cpp:8-32) or ColliderCercignaniLampis
+ * (dsmc/collidercercignanilampis.cpp:13-45): float wall frames, double
+ * velocities, as the reference mixes them. */
 static void reflect(const oracle_system *s, const int b[3], double v[3], draws *d) {
+    if (s->wall_model == 1 || s->wall_model == 2) {
+        const size_t q = 3 * lin_at(s, b);
+        const float *n = s->nrm + q, *a = s->t1 + q, *t = s->t2 + q;
+        if (s->wall_model == 1) {
+            const double vn = n[0] * v[0] + n[1] * v[1] + n[2] * v[2];
+            const double vt1 = a[0] * v[0] + a[1] * v[1] + a[2] * v[2];
+            const double vt2 = t[0] * v[0] + t[1] * v[1] + t[2] * v[2];
+            for (int k = 0; k < 3; ++k) v[k] = -vn * n[k] + vt1 * a[k] + vt2 * t[k];
+            return;
+        }
+        const double factor = sqrt(2.0) * s->wall_s;
+        const double vni = v[0] * n[0] + v[1] * n[1] + v[2] * n[2];
+        const double vt1i = v[0] * a[0] + v[1] * a[1] + v[2] * a[2];
+        const double vt2i = v[0] * t[0] + v[1] * t[1] + v[2] * t[2];
+        int ok = 0;
+        const double vn = cl_normal(s, vni, factor, s->cl_vmax, d, &ok);
+        if (!ok) return;  /* the GPU flags DSMC_EBIT_WALL and keeps the velocity */
+        const double sigma = 1 - sqrt(1 - s->alpha_t);
+        const double vt1 = gauss(d) * sqrt(s->alpha_t) * s->wall_s + vt1i * (1 - sigma);
+        const double vt2 = gauss(d) * sqrt(s->alpha_t) * s->wall_s + vt2i * (1 - sigma);
+        for (int k = 0; k < 3; ++k) v[k] = vn * n[k] + vt1 * a[k] + vt2 * t[k];
+        return;
+    }
     const double vn = s->wall_s * sqrt(-2 * log(uni(d)));
     const double vt1 = s->wall_s * gauss(d);
     const double vt2 = s->wall_s * gauss(d);

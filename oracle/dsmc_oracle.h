@@ -25,6 +25,9 @@ typedef struct oracle_system {
     const unsigned char *vox;  /* voxel types, (i*ny + j)*nz + k, no halo */
     const float *nrm, *t1, *t2;
     uint64_t seed;
+    int wall_model;         /* 0 thermal, 1 specular, 2 Cercignani-Lampis (dsmc/system.cpp:345-352) */
+    double alpha_n, alpha_t;  /* Cercignani-Lampis accommodation */
+    double cl_vmax;         /* UnitConverter::velocity_from_SI(1500) */
 } oracle_system;
 
 typedef struct oracle_counters {

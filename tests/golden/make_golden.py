@@ -40,6 +40,11 @@ CASES = {
     # five times the timestep: multi-voxel flights and many wall hits
     "small_dt5": dict(n=24, radius_voxels=2, porosity=0.6, geom_seed=11, cells=12, dt_si=5e-11, apm=10000,
                       rng_seed=0x0BADC0FFEE, steps=10),
+    # the other wall models of the reference (dsmc/system.cpp:345-352)
+    "small_specular": dict(n=24, radius_voxels=2, porosity=0.6, geom_seed=11, cells=12, dt_si=5e-11, apm=10000,
+                           rng_seed=0x5BEC, steps=10, surface="specular"),
+    "small_cl": dict(n=24, radius_voxels=2, porosity=0.6, geom_seed=11, cells=12, dt_si=5e-11, apm=10000,
+                     rng_seed=0xC1C1, steps=10, surface="cercignani_lampis", alpha_n=0.5, alpha_t=0.8),
 }
 
 
@@ -49,7 +54,8 @@ def settings_dict(c):
                 statistics_interval=1, sampling_bins=c["cells"], dt=time_from_si(c["dt_si"]),
                 gravity=acceleration_from_si(1e9), flow_direction=0, seed=c["geom_seed"], density=2.5e24,
                 diam=3.66e-4, mass=6.63e-26 / 1.66053886e-27, Lx=L, Ly=L, Lz=L, cells_x=c["cells"],
-                cells_y=c["cells"], cells_z=c["cells"])
+                cells_y=c["cells"], cells_z=c["cells"], surface=c.get("surface", "thermal"),
+                alpha_n=c.get("alpha_n", 0.5), alpha_t=c.get("alpha_t", 0.8))
 
 
 def make_case(name, c):
@@ -124,6 +130,9 @@ def geometry_digests():
 if __name__ == "__main__":
     if not rh.available():
         raise SystemExit("build oracle/_ref first: make -C oracle ref")
+    only = sys.argv[1:]  # case names to (re)generate; all when none
     for name, c in CASES.items():
-        make_case(name, c)
-    geometry_digests()
+        if not only or name in only:
+            make_case(name, c)
+    if not only:
+        geometry_digests()

@@ -15,7 +15,8 @@ class System(C.Structure):
     _fields_ = [("n", C.c_int * 3), ("cells", C.c_int * 3), ("L", C.c_double * 3), ("dt", C.c_double),
                 ("gravity", C.c_double), ("flow_dir", C.c_int), ("wall_s", C.c_double),
                 ("sqrt_t_over_m", C.c_double), ("vox", C.c_void_p), ("nrm", C.c_void_p), ("t1", C.c_void_p),
-                ("t2", C.c_void_p), ("seed", C.c_uint64)]
+                ("t2", C.c_void_p), ("seed", C.c_uint64), ("wall_model", C.c_int), ("alpha_n", C.c_double),
+                ("alpha_t", C.c_double), ("cl_vmax", C.c_double)]
 
 
 class Counters(C.Structure):
@@ -67,6 +68,11 @@ class Oracle:
         s.t1 = self.t1.ctypes.data
         s.t2 = self.t2.ctypes.data
         s.seed = seed
+        s.wall_model = {"thermal": 0, "specular": 1, "cercignani_lampis": 2}[st.get("surface", "thermal")]
+        s.alpha_n = st.get("alpha_n", 0.5)
+        s.alpha_t = st.get("alpha_t", 0.8)
+        L0, m0, E0 = 1e-6, 1.66053886e-27, 1.65088e-21   # dsmc/unitconverter.cpp:3-21
+        s.cl_vmax = 1500.0 / (L0 / (L0 * np.sqrt(m0 / E0)))
         self.s = s
         ncell = int(np.prod(s.cells[:]))
         self.cell_map = np.empty(ncell, np.int32)

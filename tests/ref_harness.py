@@ -45,9 +45,9 @@ pressure_A = 100000
 pressure_B = 100000
 reservoir_fraction = 0
 world = {world}
-surface_interaction_model = thermal
-alpha_n = 0.5
-alpha_t = 0.8
+surface_interaction_model = {surface}
+alpha_n = {alpha_n!r}
+alpha_t = {alpha_t!r}
 seed = {seed}
 density = {density!r}
 diam = {diam!r}
@@ -66,6 +66,9 @@ nz = 1
 
 
 def write_ini(path: Path, **kw) -> None:
+    kw.setdefault("surface", "thermal")
+    kw.setdefault("alpha_n", 0.5)
+    kw.setdefault("alpha_t", 0.8)
     path.write_text(INI_TEMPLATE.format(**kw))
 
 

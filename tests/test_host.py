@@ -89,13 +89,20 @@ def test_ini_parsed_like_cinifile(tmp_path):
     assert s.density == 2.5e24 and s.flow_direction == 0
 
 
+def test_ini_wall_models(tmp_path):
+    p = tmp_path / "dsmc.ini"
+    for name, code in (("thermal", 0), ("specular", 1), ("cercignani_lampis", 2)):
+        p.write_text(INI.replace("= thermal", "= " + name))
+        assert Settings.from_ini(p).surface_model == code
+
+
 def test_ini_missing_key_and_unbuilt_model(tmp_path):
     p = tmp_path / "dsmc.ini"
     p.write_text(INI.replace("diam = 3.66e-4\n", ""))
     with pytest.raises(capi.DsmcError) as e:
         Settings.from_ini(p)
     assert e.value.code == capi.DSMC_ERR_NOT_FOUND and "diam" in str(e.value)
-    p.write_text(INI.replace("= thermal", "= cercignani_lampis"))
+    p.write_text(INI.replace("= thermal", "= maxwell"))
     with pytest.raises(capi.DsmcError) as e:
         Settings.from_ini(p)
     assert e.value.code == capi.DSMC_ERR_CONFIG

@@ -26,7 +26,7 @@ def load(case):
     return z, meta, g
 
 
-@pytest.mark.parametrize("case", ["small_dt1", "small_dt5"])
+@pytest.mark.parametrize("case", ["small_dt1", "small_dt5", "small_specular", "small_cl"])
 def test_oracle_reproduces_reference_steps(case):
     z, meta, g = load(case)
     o = oracle_c.Oracle(g, meta["settings"], meta["params"]["rng_seed"])
@@ -37,7 +37,9 @@ def test_oracle_reproduces_reference_steps(case):
     o.move(1)
     assert np.array_equal(o.r, z["r1"]) and np.array_equal(o.v, z["v1"])
     c = o.counters()
-    assert c["wall_collisions"] == meta["counters_move"]["wall_collisions"]
+    # only the reference's thermal collider counts wall collisions
+    thermal = meta["settings"].get("surface", "thermal") == "thermal"
+    assert c["wall_collisions"] == meta["counters_move"]["wall_collisions"] or not thermal
     assert c["count_periodic"] == meta["counters_move"]["count_periodic"]
     o.sort()
     assert np.array_equal(o.cell_global_of_particles, z["cell1"])
@@ -51,7 +53,8 @@ def test_oracle_reproduces_reference_steps(case):
     assert np.array_equal(o.cell_global_of_particles, z["cellK"])
     c = o.counters()
     ref = meta["counters_final"]
-    assert c["collisions"] == ref["collisions"] and c["wall_collisions"] == ref["wall_collisions"]
+    assert c["collisions"] == ref["collisions"]
+    assert c["wall_collisions"] == ref["wall_collisions"] or not thermal
     assert c["count_periodic"] == ref["count_periodic"]
 
 
