@@ -195,6 +195,7 @@ typedef struct dsmc_system_info {
     double dt;
     int64_t expected_particles; /* density*volume/atoms_per_molecule (dsmc/system.cpp:323) */
     int slots;                  /* particle slots reserved per buffer */
+    double volume_global;       /* L_x L_y L_z * porosity_global (dsmc/system.cpp:314) */
 } dsmc_system_info;
 int dsmc_system_info_get(dsmc_ctx *ctx, int sys_id, dsmc_system_info *info);
 
@@ -245,6 +246,46 @@ typedef struct dsmc_tallies {
 } dsmc_tallies;
 int dsmc_tallies_get(dsmc_ctx *ctx, int sys_id, dsmc_tallies *t);
 int dsmc_tallies_reset(dsmc_ctx *ctx, int sys_id);
+
+/* The sampler's scalar measurements at the current step, as each
+ * Measure*::update computes them (dsmc/statisticalproperty.cpp:21-210) and
+ * StatisticsSampler::sample prints them (dsmc/statisticssampler.cpp:45-66).
+ * Flow rates count from the last tally reset or continuation; permeability
+ * is 0 without a flow direction or gravity. */
+typedef struct dsmc_measures {
+    uint64_t step;
+    double t_ns;                 /* System::t_in_nano_seconds */
+    double energy_eV;            /* MeasureEnergy: 1/2 m sum |v|^2 * atoms_per_molecule */
+    double temperature_K;        /* MeasureTemperature */
+    double number_flow_rate;     /* MeasureNumberFlowRate, reduced units */
+    double volumetric_flow_rate; /* MeasureVolumetricFlowRate, reduced units */
+    double pressure_Pa;          /* MeasurePressure */
+    double permeability_darcy;   /* MeasurePermeability, finalize's unit */
+    uint64_t collisions, wall_collisions, molecules;
+} dsmc_measures;
+int dsmc_measures_get(dsmc_ctx *ctx, int sys_id, dsmc_measures *m);
+
+/* Sampler profiles over the samples since the last tally reset
+ * (StatisticsSampler, dsmc/statisticssampler.cpp:22-26): sampling_bins bins
+ * in y of {count, sum v_z, sum 1/2 m v_z^2} (MeasureCount,
+ * MeasureVelocityDistributionPoiseuille, MeasureTemperatureDistribution,
+ * dsmc/statisticalproperty.cpp:229-362) and a v_x histogram over
+ * [-4, 4] sqrt(T/m) (MeasureVelocityDistribution, :432-458).
+ *
+ * dsmc_profile_sums_get: the raw sums, 4*bins doubles: {count, sum v_z,
+ * sum 1/2 m v_z^2} per y bin, then the v_x histogram; sums NULL gives only
+ * *bins.  Sums of several ranks add up before finishing.
+ * dsmc_profiles_finish: finishes sums as the reference's finalize() does
+ * (:303-309, 364-371, 393-426, 462-478): count, v_z (m/s), temperature (K)
+ * and pressure (Pa) per y bin, v_x bin centres (m/s) and counts.  Host only;
+ * any output may be NULL; volume_global from dsmc_system_info.
+ * dsmc_profiles_get: both for one system; outputs hold cap >= bins values. */
+int dsmc_profile_sums_get(dsmc_ctx *ctx, int sys_id, int cap, double *sums, int *bins);
+int dsmc_profiles_finish(const dsmc_settings *s, double volume_global, int bins, const double *sums, double *count,
+                         double *velocity_z, double *temperature, double *pressure, double *vx_center,
+                         double *vx_count);
+int dsmc_profiles_get(dsmc_ctx *ctx, int sys_id, int cap, double *count, double *velocity_z, double *temperature,
+                      double *pressure, double *vx_center, double *vx_count, int *bins);
 
 /* Per active cell: global cell index (dsmc/system.h:130-132), particle count,
  * vr_max, selection remainder, and 8 fp64 moment sums over the sampled steps

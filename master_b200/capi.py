@@ -39,6 +39,7 @@ EXPORTED = [
     "dsmc_ctx_set_capacity", "dsmc_pass_info", "dsmc_geometry_finish_gpu_noalloc", "dsmc_ctx_set_timing",
     "dsmc_pass_times_get", "dsmc_state_file_read", "dsmc_state_file_write", "dsmc_tocontinue_read",
     "dsmc_tocontinue_write", "dsmc_continue_from", "dsmc_checkpoint_save", "dsmc_checkpoint_load",
+    "dsmc_profile_sums_get", "dsmc_profiles_finish", "dsmc_profiles_get", "dsmc_measures_get",
 ]
 
 
@@ -80,7 +81,8 @@ class SphereParams(C.Structure):
 class SystemInfo(C.Structure):
     _fields_ = [("num_particles", C.c_int64), ("num_cells_total", C.c_int), ("num_active_cells", C.c_int),
                 ("volume", C.c_double), ("porosity", C.c_double), ("atoms_per_molecule", C.c_double),
-                ("dt", C.c_double), ("expected_particles", C.c_int64), ("slots", C.c_int)]
+                ("dt", C.c_double), ("expected_particles", C.c_int64), ("slots", C.c_int),
+                ("volume_global", C.c_double)]
 
 
 class Tallies(C.Structure):
@@ -88,6 +90,14 @@ class Tallies(C.Structure):
                 ("reseeds", C.c_uint64), ("particle_steps", C.c_uint64), ("count_periodic", C.c_int64 * 3),
                 ("samples", C.c_uint64), ("candidates", C.c_uint64), ("kinetic_energy", C.c_double),
                 ("temperature", C.c_double), ("flux", C.c_double), ("time", C.c_double), ("stranded", C.c_uint64)]
+
+
+class Measures(C.Structure):
+    _fields_ = [("step", C.c_uint64), ("t_ns", C.c_double), ("energy_eV", C.c_double),
+                ("temperature_K", C.c_double), ("number_flow_rate", C.c_double),
+                ("volumetric_flow_rate", C.c_double), ("pressure_Pa", C.c_double),
+                ("permeability_darcy", C.c_double), ("collisions", C.c_uint64), ("wall_collisions", C.c_uint64),
+                ("molecules", C.c_uint64)]
 
 
 _lib = None
@@ -155,6 +165,10 @@ def load() -> C.CDLL:
         "dsmc_continue_from": [_P, C.c_int, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64],
         "dsmc_checkpoint_save": [_P, C.c_char_p],
         "dsmc_checkpoint_load": [_P, C.c_char_p],
+        "dsmc_profile_sums_get": [_P, C.c_int, C.c_int, _D, C.POINTER(C.c_int)],
+        "dsmc_measures_get": [_P, C.c_int, C.POINTER(Measures)],
+        "dsmc_profiles_finish": [C.POINTER(Settings), C.c_double, C.c_int, _D, _D, _D, _D, _D, _D, _D],
+        "dsmc_profiles_get": [_P, C.c_int, C.c_int, _D, _D, _D, _D, _D, _D, C.POINTER(C.c_int)],
         "dsmc_cells_layout": [C.POINTER(Settings), C.c_uint32, C.c_uint32, C.c_uint32, _U8, C.c_int, _I32, _I32,
                               _I32, _D, _D, C.POINTER(C.c_int)],
     }

@@ -62,6 +62,9 @@ struct SysHost {
     double t_offset = 0;              // t - step * dt after a continuation
     double sqrt_t_over_m = 0;
     double vr_max0 = 0;
+    double volume_global = 0;         // L_x L_y L_z * porosity_global (dsmc/system.cpp:314)
+    int prof_bins = 0;
+    DevBuf<double> prof;              // sampler profiles: 3*bins y-binned sums, then the v_x histogram
 };
 
 }  // namespace dsmc
@@ -360,6 +363,19 @@ int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, 
     return DSMC_OK;
 }
 
+// Whether the collide of a pass that sees step counter `step` samples any
+// system (the cadence of StatisticsSampler::sample; the kernels check it again
+// per system).
+bool samples_at(const dsmc_ctx *ctx, unsigned step) {
+    for (const auto &s : ctx->systems) {
+        const SysDev &d = s->dev;
+        if (d.sample_interval > 0 && step > 0 && step % (unsigned)d.sample_interval == 0 &&
+            step >= (unsigned)d.sample_begin)
+            return true;
+    }
+    return false;
+}
+
 // After a batch of passes: find how many ran, fix the buffer parity, and
 // repack if one of them spilled.
 int settle(dsmc_ctx *ctx, unsigned step_before, int cur_before, int cphase_before, int *ran) {
@@ -527,6 +543,8 @@ int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t
         return fail(ctx, DSMC_ERR_CONFIG, "one system is one domain: processor grid must be 1 1 1");
     if (s->surface_model < DSMC_WALL_THERMAL || s->surface_model > DSMC_WALL_CL)
         return fail(ctx, DSMC_ERR_CONFIG, "unknown wall model");
+    if (s->sampling_bins < 1 || s->sampling_bins > (1 << 20))
+        return fail(ctx, DSMC_ERR_CONFIG, "sampling_bins must be in 1 .. 2^20");
     if (s->surface_model == DSMC_WALL_CL && !(s->alpha_n > 0 && s->alpha_n <= 1 && s->alpha_t >= 0 && s->alpha_t <= 1))
         return fail(ctx, DSMC_ERR_CONFIG, "Cercignani-Lampis accommodation needs 0 < alpha_n <= 1, 0 <= alpha_t <= 1");
     // System::validate_number_of_cells (dsmc/system.cpp:221-239).
@@ -564,6 +582,7 @@ int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t
     double volume = L[0] * L[1] * L[2];
     volume = volume / 1 * h->porosity;
     h->volume = volume;
+    h->volume_global = L[0] * L[1] * L[2] * h->porosity_global;
     h->expected = (int64_t)(density * volume / h->atoms_per_molecule);
     {
         int nc = 0;
@@ -630,6 +649,19 @@ int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t
     d.seed = s->rng_seed;
     d.sample_interval = s->statistics_interval;
     d.sample_begin = s->sample_begin;
+    // Sampler profiles (dsmc/statisticssampler.cpp:22-26): sampling_bins bins
+    // in y, and a v_x histogram over [-4 sigma, 4 sigma], sigma = sqrt(T/m).
+    h->prof_bins = s->sampling_bins;
+    CK(h->prof.alloc(4 * (size_t)h->prof_bins));
+    CK(cudaMemsetAsync(h->prof.p, 0, 4 * (size_t)h->prof_bins * sizeof(double), ctx->stream));
+    d.prof = h->prof.p;
+    d.prof_bins = h->prof_bins;
+    d.mass = s->mass;
+    {
+        const double sd = std::sqrt(temperature / s->mass);
+        d.vx_min = -4 * sd;
+        d.vx_bin = (4 * sd - d.vx_min) / h->prof_bins;
+    }
 
     ctx->systems.push_back(std::move(h));
     *sys_id = (int)ctx->systems.size() - 1;
@@ -724,6 +756,7 @@ int dsmc_system_info_get(dsmc_ctx *ctx, int sys_id, dsmc_system_info *info) {
     info->num_cells_total = h.cells[0] * h.cells[1] * h.cells[2];
     info->num_active_cells = (int)h.cell_global.size();
     info->volume = h.volume;
+    info->volume_global = h.volume_global;
     info->porosity = h.porosity;
     info->atoms_per_molecule = h.atoms_per_molecule;
     info->dt = h.settings.dt;
@@ -861,13 +894,20 @@ int dsmc_checkpoint_save(dsmc_ctx *ctx, const char *path) {
         CK(cudaMemcpyAsync(mom.data(), ctx->mom.p, mom.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     }
     if (S) CK(cudaMemcpyAsync(tally.data(), ctx->tally.p, S * sizeof(SysTally), cudaMemcpyDeviceToHost, ctx->stream));
+    std::vector<std::vector<double>> prof(S);
+    for (int s = 0; s < S; ++s) {
+        const SysHost &h = *ctx->systems[s];
+        prof[s].resize(4 * (size_t)h.prof_bins);
+        CK(cudaMemcpyAsync(prof[s].data(), h.prof.p, prof[s].size() * sizeof(double), cudaMemcpyDeviceToHost,
+                           ctx->stream));
+    }
     cudaError_t e;
     Status st = read_status(ctx, &e);
     CK(e);
     CkptHeader hd;
     std::memset(&hd, 0, sizeof(hd));
     std::memcpy(hd.magic, kCkptMagic, 8);
-    hd.version = 1;
+    hd.version = 2;
     hd.step = st.step;
     hd.precision = ctx->precision;
     hd.num_systems = S;
@@ -895,6 +935,11 @@ int dsmc_checkpoint_save(dsmc_ctx *ctx, const char *path) {
     ok = ok && std::fwrite(A.data(), 1, A.size(), f) == A.size();
     ok = ok && std::fwrite(B.data(), 1, B.size(), f) == B.size();
     ok = ok && std::fwrite(key.data(), sizeof(int), key.size(), f) == key.size();
+    for (int s = 0; s < S && ok; ++s) {  // version 2: the sampler profiles, per system {bins, pad, 4*bins doubles}
+        const int32_t bp[2] = {ctx->systems[s]->prof_bins, 0};
+        ok = std::fwrite(bp, sizeof(bp), 1, f) == 1;
+        ok = ok && std::fwrite(prof[s].data(), sizeof(double), prof[s].size(), f) == prof[s].size();
+    }
     ok = (std::fclose(f) == 0) && ok;
     if (!ok) return fail(ctx, DSMC_ERR_IO, std::string("could not write ") + path);
     return DSMC_OK;
@@ -910,7 +955,8 @@ int dsmc_checkpoint_load(dsmc_ctx *ctx, const char *path) {
         return fail(ctx, DSMC_ERR_CONFIG, std::string(path) + ": " + why);
     };
     CkptHeader hd;
-    if (std::fread(&hd, sizeof(hd), 1, f) != 1 || std::memcmp(hd.magic, kCkptMagic, 8) || hd.version != 1)
+    if (std::fread(&hd, sizeof(hd), 1, f) != 1 || std::memcmp(hd.magic, kCkptMagic, 8) ||
+        (hd.version != 1 && hd.version != 2))
         return bad("not a checkpoint of this library");
     const int C = ctx->num_cells, S = (int)ctx->systems.size();
     if (hd.precision != ctx->precision) return bad("written by a context of the other precision");
@@ -931,6 +977,14 @@ int dsmc_checkpoint_load(dsmc_ctx *ctx, const char *path) {
     ok = ok && std::fread(A.data(), 1, A.size(), f) == A.size();
     ok = ok && std::fread(B.data(), 1, B.size(), f) == B.size();
     ok = ok && std::fread(key.data(), sizeof(int), key.size(), f) == key.size();
+    std::vector<std::vector<double>> prof(S);  // version 1 carries no profiles: they restart from zero
+    for (int s = 0; s < S; ++s) prof[s].assign(4 * (size_t)ctx->systems[s]->prof_bins, 0.0);
+    for (int s = 0; s < S && ok && hd.version >= 2; ++s) {
+        int32_t bp[2];
+        ok = std::fread(bp, sizeof(bp), 1, f) == 1;
+        if (ok && bp[0] != ctx->systems[s]->prof_bins) return bad("the context's sampling bins differ from the checkpoint's");
+        ok = ok && std::fread(prof[s].data(), sizeof(double), prof[s].size(), f) == prof[s].size();
+    }
     if (!ok) return bad("truncated");
     std::fclose(f);
     std::vector<unsigned> hist(std::max(C, 1), 0);
@@ -971,6 +1025,9 @@ int dsmc_checkpoint_load(dsmc_ctx *ctx, const char *path) {
         CK(cudaMemcpyAsync(ctx->mom.p, mom.data(), mom.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     }
     if (S) CK(cudaMemcpyAsync(ctx->tally.p, tally.data(), S * sizeof(SysTally), cudaMemcpyHostToDevice, ctx->stream));
+    for (int s = 0; s < S; ++s)
+        CK(cudaMemcpyAsync(ctx->systems[s]->prof.p, prof[s].data(), prof[s].size() * sizeof(double),
+                           cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(&ctx->status.p->step, &hd.step, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return DSMC_OK;
@@ -1028,7 +1085,9 @@ int dsmc_step(dsmc_ctx *ctx, int nsteps) {
         // cells, then accelerate + move + re-bin of this step.
         for (int i = 0; i < left; ++i) {
             const int prologue = (i == 0 && !pending0);
-            int rc = launch(ctx, PASS_FUSED, !prologue, 1, !prologue, 1);
+            // pass i collides at step step0 + i (a halted batch runs no later pass)
+            const int sample = !prologue && samples_at(ctx, step0 + (unsigned)i);
+            int rc = launch(ctx, PASS_FUSED, !prologue, 1, sample, 1);
             if (rc) return rc;
             ctx->cur ^= 1;
         }
@@ -1142,6 +1201,73 @@ int dsmc_tallies_get(dsmc_ctx *ctx, int sys_id, dsmc_tallies *t) {
     return DSMC_OK;
 }
 
+int dsmc_measures_get(dsmc_ctx *ctx, int sys_id, dsmc_measures *m) {
+    if (!ctx || !m || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+    dsmc_tallies t;
+    int rc = dsmc_tallies_get(ctx, sys_id, &t);
+    if (rc) return rc;
+    const SysHost &h = *ctx->systems[sys_id];
+    const dsmc_settings &s = h.settings;
+    const Units &u = ctx->units;
+    // System::get_number_of_atoms_global and the reduced temperature of
+    // MeasureTemperature (dsmc/statisticalproperty.cpp:57-68)
+    const double atoms = (double)h.num_particles * h.atoms_per_molecule;
+    const double T = atoms > 0 ? 2.0 / 3.0 * t.kinetic_energy / atoms : 0.0;
+    const double density = u.number_density_from_SI(s.density);
+    std::memset(m, 0, sizeof(*m));
+    m->step = t.step;
+    m->t_ns = u.time_to_SI(t.time) * 1e9;
+    m->energy_eV = u.energy_to_eV(t.kinetic_energy);
+    m->temperature_K = u.temperature_to_SI(T);
+    m->number_flow_rate = t.flux;
+    m->volumetric_flow_rate = t.flux * (1.0 / density);  // MeasureVolumetricFlowRate (:118-133)
+    if (h.volume_global > 0) m->pressure_Pa = u.pressure_to_SI(atoms / h.volume_global * T);  // MeasurePressure
+    const int fd = s.flow_direction;
+    if (fd >= 0 && fd < 3 && s.gravity != 0 && density > 0) {
+        // MeasurePermeability::update (:180-210): kinetic-theory viscosity of
+        // hard spheres, permeability = Q mu / (A m n g)
+        const double L[3] = {s.Lx, s.Ly, s.Lz};
+        double area = 1;
+        for (int a = 0; a < 3; ++a)
+            if (a != fd) area *= L[a];
+        const double viscosity = 5.0 / (16 * s.diam * s.diam) * std::sqrt(s.mass * T / M_PI);
+        const double k = m->volumetric_flow_rate * viscosity / (area * s.mass * density * s.gravity);
+        m->permeability_darcy = u.permeability_to_darcy(k);
+    }
+    m->collisions = t.collisions;
+    m->wall_collisions = t.wall_collisions;
+    m->molecules = (uint64_t)h.num_particles;
+    return DSMC_OK;
+}
+
+int dsmc_profile_sums_get(dsmc_ctx *ctx, int sys_id, int cap, double *sums, int *bins) {
+    if (!ctx || !bins || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    const SysHost &h = *ctx->systems[sys_id];
+    *bins = h.prof_bins;
+    if (!sums) return DSMC_OK;
+    if (cap < 4 * h.prof_bins) return fail(ctx, DSMC_ERR_CAPACITY, "profile buffer smaller than 4 * sampling_bins");
+    CK(cudaMemcpyAsync(sums, h.prof.p, 4 * (size_t)h.prof_bins * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return DSMC_OK;
+}
+
+int dsmc_profiles_get(dsmc_ctx *ctx, int sys_id, int cap, double *count, double *velocity_z, double *temperature,
+                      double *pressure, double *vx_center, double *vx_count, int *bins) {
+    if (!ctx || !bins || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+    int rc = dsmc_profile_sums_get(ctx, sys_id, 0, nullptr, bins);
+    if (rc) return rc;
+    if (cap < *bins) return fail(ctx, DSMC_ERR_CAPACITY, "profile buffers smaller than sampling_bins");
+    const SysHost &h = *ctx->systems[sys_id];
+    std::vector<double> sums(4 * (size_t)*bins);
+    rc = dsmc_profile_sums_get(ctx, sys_id, (int)sums.size(), sums.data(), bins);
+    if (rc) return rc;
+    return dsmc_profiles_finish(&h.settings, h.volume_global, *bins, sums.data(), count, velocity_z, temperature,
+                                pressure, vx_center, vx_count);
+}
+
 int dsmc_tallies_reset(dsmc_ctx *ctx, int sys_id) {
     if (!ctx || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
     cudaSetDevice(ctx->device);
@@ -1151,6 +1277,7 @@ int dsmc_tallies_reset(dsmc_ctx *ctx, int sys_id) {
     CK(cudaMemsetAsync(ctx->tally.p + sys_id, 0, sizeof(SysTally), ctx->stream));
     const int C = h.active_end - h.active_begin;
     if (C > 0) CK(cudaMemsetAsync(ctx->mom.p + 8 * (size_t)h.active_begin, 0, 8 * (size_t)C * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(h.prof.p, 0, 4 * (size_t)h.prof_bins * sizeof(double), ctx->stream));
     cudaError_t e;
     Status st = read_status(ctx, &e);
     CK(e);

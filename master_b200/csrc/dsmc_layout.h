@@ -100,6 +100,13 @@ struct SysDev {
     uint64_t seed;
     int sample_interval;       // sample when step % interval == 0 and step >= sample_begin
     int sample_begin;
+    // y-binned profiles of the sampler (dsmc/statisticalproperty.cpp:229-362):
+    // per bin {particle count, sum v_z, sum 1/2 m v_z^2} over the samples
+    // and the v_x histogram of MeasureVelocityDistribution (bins of width
+    // vx_bin from vx_min = -4 sqrt(T/m)), stored after the 3*bins sums
+    double *prof;
+    int prof_bins;
+    double mass, vx_min, vx_bin;
 };
 
 #define DSMC_WALL_THERMAL 0    // diffuse reflection at the wall temperature

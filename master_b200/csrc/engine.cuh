@@ -113,6 +113,43 @@ __device__ __forceinline__ bool cl_normal(real v_norm_in, real factor, real max_
     return false;
 }
 
+// ---- sampler profiles -------------------------------------------------------
+// Bin of a y position as MeasureCount and friends take it
+// (dsmc/statisticalproperty.cpp:236): int(r_y * (1/L_y) * bins), kept in range.
+__device__ __forceinline__ int profile_bin(const SysDev &g, double y) {
+    const int b = (int)(y * g.invL[1] * g.prof_bins);
+    return min(max(b, 0), g.prof_bins - 1);
+}
+// Adds per-lane {count, sum v_z, sum 1/2 m v_z^2} to the system's profile,
+// one atomic per distinct bin of the warp.  All lanes call.
+__device__ __forceinline__ void profile_add_warp(const SysDev &g, bool valid, int bin, double c, double s, double e) {
+    unsigned todo = __ballot_sync(0xffffffffu, valid);
+    while (todo) {
+        const int b = __shfl_sync(0xffffffffu, bin, __ffs(todo) - 1);
+        const bool in = valid && bin == b;
+        double cc = in ? c : 0.0, ss = in ? s : 0.0, ee = in ? e : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            cc += __shfl_xor_sync(0xffffffffu, cc, o);
+            ss += __shfl_xor_sync(0xffffffffu, ss, o);
+            ee += __shfl_xor_sync(0xffffffffu, ee, o);
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(g.prof + 3 * b, cc);
+            atomicAdd(g.prof + 3 * b + 1, ss);
+            atomicAdd(g.prof + 3 * b + 2, ee);
+        }
+        todo &= ~__ballot_sync(0xffffffffu, in);
+    }
+}
+
+// MeasureVelocityDistribution::update (dsmc/statisticalproperty.cpp:441-458):
+// bin int((v_x - v_min) / width), truncated toward zero, counted when in range.
+__device__ __forceinline__ void profile_vx(const SysDev &g, double vx) {
+    const int b = (int)((vx - g.vx_min) / g.vx_bin);
+    if (b >= 0 && b < g.prof_bins) atomicAdd(g.prof + 3 * g.prof_bins + b, 1.0);
+}
+
 struct Split32 {
     typedef float real;
     typedef uint4 RecA;
@@ -151,6 +188,10 @@ struct Split32 {
         b.y = p.v[1];
         b.z = p.v[2];
         b.w = __uint_as_float(p.id);
+    }
+    // y position of a record in box units (for the sampler's bins)
+    static __device__ __forceinline__ double y_of(const SysDev &g, const uint4 &a) {
+        return ((double)DSMC_VOX_J(a.x) + (double)__uint_as_float(a.z)) * g.vox_len[1];
     }
     static __device__ __forceinline__ void stage_load(const uint4 *, const float4 *B, size_t i, float v[3],
                                                       uint32_t &id) {
@@ -690,6 +731,7 @@ struct Fp64 {
         b.z = p.v[2];
         b.w = 0.0;
     }
+    static __device__ __forceinline__ double y_of(const SysDev &, const double4 &a) { return a.y; }
     static __device__ __forceinline__ void stage_load(const double4 *A, const double4 *B, size_t i, double v[3],
                                                       uint32_t &id) {
         const double4 b = B[i];
@@ -1218,6 +1260,19 @@ __global__ void __launch_bounds__(256) pass_kernel(PassParams P) {
         }
         if (sample) {
             double m[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            for (int r0 = 0; r0 < n; r0 += 32) {  // y-binned profiles, member by member
+                const int r = r0 + lane;
+                const bool ok = r < n;
+                int bin = 0;
+                double vz = 0;
+                if (ok) {
+                    const int s = st.perm[r];
+                    vz = (double)st.vz[s];
+                    bin = profile_bin(g, Prec::y_of(g, Ain[cell_slot(meta.x, meta.y, nb, nt, s)]));
+                }
+                profile_add_warp(g, ok, bin, 1.0, vz, 0.5 * g.mass * vz * vz);
+                if (ok) profile_vx(g, (double)st.vx[st.perm[r]]);
+            }
             for (int r = lane; r < n; r += 32) {
                 const int s = st.perm[r];
                 const double x = (double)st.vx[s], y = (double)st.vy[s], z = (double)st.vz[s];

@@ -31,6 +31,7 @@ Units::Units() {
     m0 = 1.66053886e-27;
     L0 = 1e-6;
     E0 = 1.65088e-21;
+    E0ev = 1.0318e-2;
     kb = 1.3806503e-23;
     t0 = L0 * std::sqrt(m0 / E0);
     T0 = E0 / kb;
@@ -682,3 +683,32 @@ int dsmc_tocontinue_write(const char *path, double t, uint64_t steps, uint64_t c
 }
 
 }  // extern "C"
+
+int dsmc_profiles_finish(const dsmc_settings *s, double volume_global, int bins, const double *sums, double *count,
+                         double *velocity_z, double *temperature, double *pressure, double *vx_center,
+                         double *vx_count) {
+    if (!s || !sums || bins < 1 || !(s->mass > 0)) return DSMC_ERR_ARG;
+    const dsmc::Units u;
+    // The average of a bin divides by max(count, 1)
+    // (MeasureVelocityDistributionPoiseuille / MeasureTemperatureDistribution
+    // ::get_average, dsmc/statisticalproperty.cpp:280-301, 341-362).
+    const double volume_per_bin = volume_global / bins;
+    for (int b = 0; b < bins; ++b) {
+        const double c = sums[3 * b], norm = c > 1 ? c : 1.0;
+        const double t_red = sums[3 * b + 2] / norm * (2.0 / 3.0);
+        if (count) count[b] = c;
+        if (velocity_z) velocity_z[b] = u.velocity_to_SI(sums[3 * b + 1] / norm);
+        if (temperature) temperature[b] = u.temperature_to_SI(t_red);
+        // MeasurePressureDistribution::get_average (:393-417): the summed count
+        // over the bin's volume times the bin temperature, as the reference has it
+        if (pressure) pressure[b] = u.pressure_to_SI(c / volume_per_bin * t_red);
+    }
+    // MeasureVelocityDistribution::finalize (:462-478): bin centres and counts
+    const double sd = std::sqrt(u.temperature_from_SI(s->temperature) / s->mass);
+    const double v_min = -4 * sd, width = (4 * sd - v_min) / bins;
+    for (int b = 0; b < bins; ++b) {
+        if (vx_center) vx_center[b] = u.velocity_to_SI(v_min + (b + 0.5) * width);
+        if (vx_count) vx_count[b] = sums[3 * bins + b];
+    }
+    return DSMC_OK;
+}

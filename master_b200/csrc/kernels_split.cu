@@ -2,6 +2,7 @@
 // in-voxel offset, fp32 velocities, fp64 cell bookkeeping and tallies.
 #define DSMC_PREC Split32
 #define DSMC_PREC_NS split32
+#include <algorithm>
 #include "kernels_impl.cuh"
 
 #include "split_pass.cuh"
@@ -62,7 +63,8 @@ int fused_grids(int smem_cap, int num_sms, int grids[4]) {
         DSMC_MOVE_RINGS(X)
 #undef X
     }
-    const int bc = static_blocks(pass3::collide_cells_kernel, 32 * pass3::C_WARPS);
+    const int bc = std::min(static_blocks(pass3::collide_cells_kernel<false>, 32 * pass3::C_WARPS),
+                            static_blocks(pass3::collide_cells_kernel<true>, 32 * pass3::C_WARPS));
     const int bp = static_blocks(pass3::place_movers_kernel, 32 * pass3::P_WARPS);
     const int bw = static_blocks(pass3::place_walls_kernel, 32 * pass3::W_WARPS);
     if (bm <= 0 || bc <= 0 || bp <= 0 || bw <= 0) return 0;
@@ -76,7 +78,10 @@ int fused_grids(int smem_cap, int num_sms, int grids[4]) {
 cudaError_t launch_fused(const PassParams &P, const int grids[4], cudaStream_t st, cudaEvent_t *ev) {
     if (ev) cudaEventRecord(ev[0], st);
     if (P.do_collide || P.do_sample) {
-        pass3::collide_cells_kernel<<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
+        if (P.do_sample)
+            pass3::collide_cells_kernel<true><<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
+        else
+            pass3::collide_cells_kernel<false><<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }

@@ -170,6 +170,62 @@ __device__ __forceinline__ void publish_collide(const PassParams &P, int sys, un
     }
 }
 
+// The sampler's pass over one cell (lane-per-cell): fp64 cell moments and the
+// y-binned profiles, on the cadence of StatisticsSampler::sample.  Kept out of
+// line: it runs on sampled steps only and would otherwise raise the register
+// pressure of the collide loop.
+__device__ __noinline__ void sample_cell(const PassParams &P, const SysDev &g, int a, int4 m, unsigned nb,
+                                         unsigned nt, int n) {
+    const float4 *Bin = reinterpret_cast<const float4 *>(P.parts.B[P.cur]);
+    const uint4 *Ain = reinterpret_cast<const uint4 *>(P.parts.A[P.cur]);
+    double m1[3] = {0, 0, 0}, m2[3] = {0, 0, 0};
+    // y-binned profile: a run per bin, flushed when the bin changes
+    int pbin = -1;
+    double pc = 0, ps = 0, pe = 0;
+    for (int q = 0; q < n; ++q) {
+        const int sl = member_slot(m.x, m.y, (int)nb, (int)nt, q);
+        const float4 b = Bin[sl];
+        const double x = b.x, y = b.y, z = b.z;
+        const int bin = profile_bin(g, Split32::y_of(g, Ain[sl]));
+        if (bin != pbin) {
+            if (pbin >= 0) {
+                atomicAdd(g.prof + 3 * pbin, pc);
+                atomicAdd(g.prof + 3 * pbin + 1, ps);
+                atomicAdd(g.prof + 3 * pbin + 2, pe);
+            }
+            pbin = bin;
+            pc = ps = pe = 0;
+        }
+        pc += 1.0;
+        ps += z;
+        pe += 0.5 * g.mass * z * z;
+        profile_vx(g, x);
+        m1[0] += x;
+        m1[1] += y;
+        m1[2] += z;
+        m2[0] += x * x;
+        m2[1] += y * y;
+        m2[2] += z * z;
+    }
+    if (pbin >= 0) {
+        atomicAdd(g.prof + 3 * pbin, pc);
+        atomicAdd(g.prof + 3 * pbin + 1, ps);
+        atomicAdd(g.prof + 3 * pbin + 2, pe);
+    }
+    double *M = P.cells.mom + 8 * (size_t)a;
+    M[0] += (double)n;
+    M[1] += m1[0];
+    M[2] += m1[1];
+    M[3] += m1[2];
+    M[4] += m2[0];
+    M[5] += m2[1];
+    M[6] += m2[2];
+    M[7] += m2[0] + m2[1] + m2[2];
+}
+
+// SAMPLE: the instance launched on steps where some system samples; the host
+// picks it, so the sampler costs the other steps nothing.
+template <bool SAMPLE>
 __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __grid_constant__ PassParams P) {
     __shared__ CollideSmem smem[C_WARPS];
     const int lane = threadIdx.x & 31;
@@ -384,30 +440,11 @@ __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __gri
             *reinterpret_cast<double2 *>(&P.cells.state[a]) = make_double2(vr, rest);
 
         // Sampling on the reference's cadence: cell moments in fp64.
-        if (mine && P.do_sample) {
+        if (SAMPLE && mine && P.do_sample) {
             const SysDev &g = P.sys[sys];
             if (g.sample_interval > 0 && step > 0 && (step % (uint32_t)g.sample_interval) == 0 &&
                 step >= (uint32_t)g.sample_begin) {
-                double m1[3] = {0, 0, 0}, m2[3] = {0, 0, 0};
-                for (int q = 0; q < n; ++q) {
-                    const float4 b = Bin[member_slot(m.x, m.y, (int)nb, (int)nt, q)];
-                    const double x = b.x, y = b.y, z = b.z;
-                    m1[0] += x;
-                    m1[1] += y;
-                    m1[2] += z;
-                    m2[0] += x * x;
-                    m2[1] += y * y;
-                    m2[2] += z * z;
-                }
-                double *M = P.cells.mom + 8 * (size_t)a;
-                M[0] += (double)n;
-                M[1] += m1[0];
-                M[2] += m1[1];
-                M[3] += m1[2];
-                M[4] += m2[0];
-                M[5] += m2[1];
-                M[6] += m2[2];
-                M[7] += m2[0] + m2[1] + m2[2];
+                sample_cell(P, g, a, m, nb, nt, n);
                 if (a == g.active_begin) ++smp;
             }
         }

@@ -183,6 +183,23 @@ def write_tocontinue(path, t: float, steps: int, collisions: int, wall_collision
     check(capi.load().dsmc_tocontinue_write(str(path).encode(), t, steps, collisions, wall_collisions))
 
 
+def finish_profiles(settings: Settings, volume_global: float, sums: np.ndarray, *, lib=None) -> dict:
+    """Finishes raw sampler sums (shape (4, bins), e.g. summed over ranks) by
+    dsmc_profiles_finish."""
+    lib = lib or capi.load()
+    sums = np.asarray(sums, np.float64)
+    b = sums.shape[1]
+    flat = np.ascontiguousarray(np.concatenate([sums[:3].T.reshape(-1), sums[3]]))
+    out = {k: np.empty(b) for k in ("count", "velocity_z", "temperature", "pressure", "vx_center", "vx_count")}
+    raw = settings.raw if isinstance(settings, Settings) else settings
+    rc = lib.dsmc_profiles_finish(C.byref(raw), volume_global, b, ptr(flat, C.c_double),
+                                  *(ptr(out[k], C.c_double) for k in ("count", "velocity_z", "temperature",
+                                                                      "pressure", "vx_center", "vx_count")))
+    if rc:
+        raise capi.DsmcError(rc, "dsmc_profiles_finish")
+    return out
+
+
 class Context:
     """One GPU context holding any number of systems (geometry + gas)."""
 
@@ -322,8 +339,37 @@ class System:
         self.ctx.check(self.ctx.lib.dsmc_tallies_get(self.ctx.handle, self.id, C.byref(t)))
         return t
 
+    def measures(self) -> capi.Measures:
+        """The sampler's scalar measurements now (energy, temperature, flow
+        rates, pressure, permeability), as StatisticsSampler::sample records them."""
+        m = capi.Measures()
+        self.ctx.check(self.ctx.lib.dsmc_measures_get(self.ctx.handle, self.id, C.byref(m)))
+        return m
+
     def reset_tallies(self) -> None:
+        """Zeroes the tallies, the cell moments and the sampler profiles."""
         self.ctx.check(self.ctx.lib.dsmc_tallies_reset(self.ctx.handle, self.id))
+
+    def profile_sums(self) -> np.ndarray:
+        """Raw sampler sums, shape (4, bins): per y bin the count, sum v_z and
+        sum 1/2 m v_z^2, then the v_x histogram (reduced units).  Sums of
+        several runs add before finish_profiles."""
+        bins = C.c_int()
+        self.ctx.check(self.ctx.lib.dsmc_profile_sums_get(self.ctx.handle, self.id, 0, ptr(None, C.c_double),
+                                                          C.byref(bins)))
+        flat = np.empty(4 * bins.value)
+        self.ctx.check(self.ctx.lib.dsmc_profile_sums_get(self.ctx.handle, self.id, flat.size,
+                                                          ptr(flat, C.c_double), C.byref(bins)))
+        b = bins.value
+        y = flat[:3 * b].reshape(b, 3)
+        return np.stack([y[:, 0], y[:, 1], y[:, 2], flat[3 * b:]])
+
+    def profiles(self) -> dict:
+        """The sampler's profiles finished as the reference's finalize()
+        writes them (dsmc/statisticalproperty.cpp:303-309, 364-371, 419-426,
+        462-478): y-binned count, v_z (m/s), temperature (K), pressure (Pa),
+        and the v_x histogram (bin centres in m/s, counts)."""
+        return finish_profiles(self.settings, self.info().volume_global, self.profile_sums(), lib=self.ctx.lib)
 
     # ---- the timestep ------------------------------------------------------
     def step(self, n: int = 1) -> None:

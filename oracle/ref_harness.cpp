@@ -15,6 +15,7 @@
  *   refh_collide         -> Cell::prepare + Cell::collide (dsmc/cell.cpp:42-111)
  *                           per active cell, as System::collide
  *                           (dsmc/system.cpp:122-131) does
+ *   refh_sample          -> StatisticsSampler::sample (dsmc/statisticssampler.cpp:45-66)
  *
  * The only departures from System::step are the draw source (one stream per
  * particle / per cell, selected with tape_select before each call) and
@@ -42,6 +43,9 @@
 #include <random.h>
 #include <cvector.h>
 #include <topology.h>
+#include <statisticssampler.h>
+#include <statisticalproperty.h>
+#include <unitconverter.h>
 #undef private
 #undef protected
 
@@ -241,6 +245,73 @@ void refh_reset_counters(void *h) {
     for (int a = 0; a < 3; ++a) s->mover->count_periodic[a] = 0;
     s->collisions = 0;
     s->mover->surface_collider->num_collisions = 0;
+}
+
+// The reference's StatisticsSampler (dsmc/statisticssampler.cpp:13-42) over
+// the harness's System.  refh_sample advances System::steps and t to `step`
+// as System::step does (steps += 1; t += dt, dsmc/system.cpp:24-26) and runs
+// StatisticsSampler::sample as dsmc/main.cpp:57-64 does after each step.
+void *refh_sampler_create(void *h) { return new StatisticsSampler(sys_of(h)); }
+void refh_sample(void *h, void *smp, uint32_t step) {
+    System *s = sys_of(h);
+    while ((uint32_t)s->steps < step) {
+        s->steps += 1;
+        s->t += s->dt;
+    }
+    static_cast<StatisticsSampler *>(smp)->sample();
+}
+// The current values of the scalar measurements, in the units their file
+// lines use: energy (eV), temperature (K), number and volumetric flow rate
+// (reduced), pressure (Pa), permeability (darcy).
+void refh_measures(void *h, void *smp, double *out6) {
+    StatisticsSampler *S = static_cast<StatisticsSampler *>(smp);
+    UnitConverter *u = sys_of(h)->unit_converter;
+    out6[0] = u->energy_to_eV(S->energy->get_current_value());
+    out6[1] = u->temperature_to_SI(S->temperature->get_current_value());
+    out6[2] = S->number_flow_rate->get_current_value();
+    out6[3] = S->volumetric_flow_rate->get_current_value();
+    out6[4] = u->pressure_to_SI(S->pressure->get_current_value());
+    out6[5] = u->permeability_to_darcy(S->permeability->get_current_value());
+}
+// Profile sums: per y bin {MeasureCount, MeasureVelocityDistributionPoiseuille,
+// MeasureTemperatureDistribution} sums, then MeasureVelocityDistribution's
+// histogram; 4*bins doubles.  Returns bins (negative when cap is short).
+int refh_profile_sums(void *smp, int cap, double *out) {
+    StatisticsSampler *S = static_cast<StatisticsSampler *>(smp);
+    const int b = S->count->value.number_of_bins;
+    if (cap < 4 * b) return -b;
+    std::vector<unsigned long> c = S->count->get_sum();
+    std::vector<double> vz = S->velocity->value.get_sum();
+    std::vector<double> e = S->temperature_distribution->value.get_sum();
+    std::vector<long> hx = S->velocity_distribution->value.get_sum();
+    for (int i = 0; i < b; ++i) {
+        out[3 * i] = (double)c[i];
+        out[3 * i + 1] = vz[i];
+        out[3 * i + 2] = e[i];
+        out[3 * b + i] = (double)hx[i];
+    }
+    return b;
+}
+// The finished profiles in SI units as each finalize() prints them
+// (dsmc/statisticalproperty.cpp:303-309, 364-371, 419-426, 462-478), at full
+// precision: v_z, temperature and pressure per y bin, v_x bin centres.
+int refh_profiles_finish(void *h, void *smp, int cap, double *vz, double *T, double *P, double *vx_center) {
+    System *sys = sys_of(h);
+    StatisticsSampler *S = static_cast<StatisticsSampler *>(smp);
+    UnitConverter *u = sys->unit_converter;
+    const int b = S->count->value.number_of_bins;
+    if (cap < b) return -b;
+    std::vector<double> a = S->velocity->get_average();
+    std::vector<double> t = S->temperature_distribution->get_average();
+    std::vector<double> p = S->pressure_distribution->get_average(sys);
+    MeasureVelocityDistribution *vd = S->velocity_distribution;
+    for (int i = 0; i < b; ++i) {
+        vz[i] = u->velocity_to_SI(a[i]);
+        T[i] = u->temperature_to_SI(t[i]);
+        P[i] = u->pressure_to_SI(p[i]);
+        vx_center[i] = u->velocity_to_SI(vd->v_min + (i + 0.5) * vd->bin_size);
+    }
+    return b;
 }
 
 int refh_voxel_index(void *h, const double *r3) { return sys_of(h)->world_grid->get_index_of_voxel(r3); }

@@ -10,7 +10,8 @@ System::setup_molecules with per-particle draw streams, the state after one
 accelerate + move (+ periodic wrap) and cell re-binning, the velocities and
 cell bookkeeping after one NTC collide, and the state after several full
 steps (every collide on id-ordered cell members), with the reference's
-counters at each point.  It also records sha256 digests of the reference
+counters at each point, and the reference sampler's profiles over those
+steps (sampled after every step).  It also records sha256 digests of the reference
 geometry tool's world arrays for the config-1 geometry.
 """
 from __future__ import annotations
@@ -78,6 +79,7 @@ def make_case(name, c):
     cnt_move = R.counters()
     R.canonicalize()
     R.collide(seed, 1)
+    R.sample(1)
     _, v1c, _ = R.get_particles()
     cells1 = R.cells()
     cnt_col = R.counters()
@@ -88,16 +90,23 @@ def make_case(name, c):
         R.update_cells()
         R.canonicalize()
         R.collide(seed, step)
+        R.sample(step)  # statistics_interval = 1: every step
     rK, vK, cellK = R.get_particles()
+    # the sampler's profiles over steps 1..K (dsmc/statisticalproperty.cpp:229-478)
+    prof = R.profile_sums()
+    fin = R.profiles()
+    measures = R.measures()
     cellsK = R.cells()
     cntK = R.counters()
     meta = dict(case=name, params=c, settings=s, n=n, counters_move=cnt_move, counters_collide=cnt_col,
-                counters_final=cntK, porosity=float(g.porosity))
+                counters_final=cntK, porosity=float(g.porosity), measures_final=measures)
     np.savez_compressed(OUT / f"{name}.npz", r0=r0, v0=v0, cell0=cell0, r1=r1, v1=v1, cell1=cell1, v1c=v1c,
                         vr_max1=cells1["vr_max"], rest1=cells1["rest"], count1=cells1["count"], rK=rK, vK=vK,
                         cellK=cellK, vr_maxK=cellsK["vr_max"], restK=cellsK["rest"], countK=cellsK["count"],
                         cell_global=cells0["global_index"], cell_volume=cells0["volume"], cell_coeff=cells0["coeff"],
                         cell_pixels=cells0["pixels"], cell_total_pixels=cells0["total_pixels"],
+                        prof_sumsK=prof, prof_vzK=fin["velocity_z"], prof_TK=fin["temperature"],
+                        prof_PK=fin["pressure"], prof_vx_center=fin["vx_center"],
                         vr_max0=cells0["vr_max"], meta=np.array(json.dumps(meta)))
     print(name, "n", n, "move", cnt_move, "final", cntK)
 

@@ -103,6 +103,13 @@ class RefSystem:
                                      C.POINTER(C.c_float)]
         L.refh_voxel_index.argtypes = [C.c_void_p, _D]
         L.refh_cell_index_of.argtypes = [C.c_void_p, C.c_long]
+        L.refh_sampler_create.restype = C.c_void_p
+        L.refh_sampler_create.argtypes = [C.c_void_p]
+        L.refh_sample.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+        L.refh_profile_sums.argtypes = [C.c_void_p, C.c_int, _D]
+        L.refh_profiles_finish.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _D, _D, _D, _D]
+        L.refh_measures.argtypes = [C.c_void_p, C.c_void_p, _D]
+        self._sampler = None
         cwd = os.getcwd()
         os.chdir(workdir)
         try:
@@ -181,6 +188,39 @@ class RefSystem:
 
     def reset_counters(self):
         self.lib.refh_reset_counters(self.h)
+
+    def sample(self, step: int) -> None:
+        """StatisticsSampler::sample at System::steps = step (the sampler is
+        created on first use, as dsmc/main.cpp:30 does before the loop)."""
+        if self._sampler is None:
+            self._sampler = self.lib.refh_sampler_create(self.h)
+        self.lib.refh_sample(self.h, self._sampler, step)
+
+    def profile_sums(self) -> np.ndarray:
+        """(4, bins): y-binned count, sum v_z, sum 1/2 m v_z^2; v_x histogram."""
+        buf = np.zeros(4 * 4096)
+        b = self.lib.refh_profile_sums(self._sampler, buf.size, _p(buf, C.c_double))
+        assert b > 0
+        y = buf[:3 * b].reshape(b, 3)
+        return np.stack([y[:, 0], y[:, 1], y[:, 2], buf[3 * b:4 * b]])
+
+    MEASURES = ("energy_eV", "temperature_K", "number_flow_rate", "volumetric_flow_rate", "pressure_Pa",
+                "permeability_darcy")
+
+    def measures(self) -> dict:
+        """The sampler's scalar measurements at the last sample."""
+        out = np.zeros(6)
+        self.lib.refh_measures(self.h, self._sampler, _p(out, C.c_double))
+        return dict(zip(self.MEASURES, out.tolist()))
+
+    def profiles(self) -> dict:
+        """The reference's finished profiles in SI units (full precision)."""
+        out = {k: np.zeros(4096) for k in ("velocity_z", "temperature", "pressure", "vx_center")}
+        b = self.lib.refh_profiles_finish(self.h, self._sampler, 4096, *(_p(out[k], C.c_double) for k in
+                                                                       ("velocity_z", "temperature", "pressure",
+                                                                        "vx_center")))
+        assert b > 0
+        return {k: v[:b].copy() for k, v in out.items()}
 
     def voxel_index(self, r3) -> int:
         r3 = np.ascontiguousarray(r3, np.float64)

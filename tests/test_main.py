@@ -61,6 +61,21 @@ def test_executable_runs_like_reference_main(tmp_path):
     assert "Time analysis" in r.stdout and "atom-timesteps / second" in r.stdout
     t, steps, collisions, walls = (tmp_path / "Tocontinue").read_text().split()
     assert int(steps) == 6 and int(walls) > 0 and float(t) > 0
+    # the sampler's files (dsmc/dsmc_io.cpp:33-47): a line per sample (steps
+    # 2, 4, 6) and the profiles at the end
+    st = tmp_path / "statistics"
+    for name in ("energy", "temperature", "pressure", "number_flow_rate", "volumetric_flow_rate"):
+        rows = [line.split() for line in (st / f"{name}.txt").read_text().splitlines()]
+        assert len(rows) == 3 and all(len(r) == 2 for r in rows), name
+        assert float(rows[0][0]) < float(rows[1][0]) < float(rows[2][0])
+    T = [float(r.split()[1]) for r in (st / "temperature.txt").read_text().splitlines()]
+    assert all(250 < x < 350 for x in T)
+    for name in ("velocity", "linear_temperature", "linear_pressure"):
+        assert len((st / f"{name}.txt").read_text().split()) == 16, name
+    hist = [line.split() for line in (st / "velocity_distribution.txt").read_text().splitlines()]
+    assert len(hist) == 16 and sum(int(c) for _, c in hist) > 0
+    assert len((st / "permeability.txt").read_text().split()) == 1
+    assert sum("Molecules:" in line for line in r.stdout.splitlines()) == 3
 
 
 @pytest.mark.gpu
