@@ -85,6 +85,21 @@ def gather_tallies(pg, num_systems: int, local: Mapping[int, object]) -> np.ndar
     return t.cpu().numpy()
 
 
+def reduce_profile_sums(pg, sums: np.ndarray) -> np.ndarray:
+    """Sampler profile sums (System.profile_sums, shape (4, bins)) added over
+    ranks: replicas of one system pool their samples, as the reference's
+    get_average reduces count and sums over ranks before normalising
+    (dsmc/statisticalproperty.cpp:287-288, 348-349).  Finish the result with
+    system.finish_profiles."""
+    sums = np.ascontiguousarray(sums, np.float64)
+    if pg is None:
+        return sums.copy()
+    import torch
+    t = torch.from_numpy(sums.copy()).to(_device(pg))
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return t.cpu().numpy()
+
+
 def totals(table: np.ndarray, systems: Iterable[int] | None = None) -> dict:
     """Sums over systems of a gathered table, by field name."""
     rows = table if systems is None else table[list(systems)]
@@ -97,4 +112,4 @@ def barrier(pg) -> None:
 
 
 __all__: Sequence[str] = ("assign", "reduce_max", "reduce_sum", "gather_tallies", "tally_row", "totals", "barrier",
-                          "TALLY_FIELDS")
+                          "reduce_profile_sums", "TALLY_FIELDS")

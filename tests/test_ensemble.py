@@ -27,6 +27,14 @@ def fake_tallies(sid: int) -> dict:
             "kinetic_energy": 0.5 * sid, "stranded": 0}
 
 
+def fake_profile(rank: int) -> np.ndarray:
+    p = np.zeros((4, 6))
+    p[0] = np.arange(6) + 10 * rank
+    p[1] = 0.25 * (rank + 1)
+    p[3, rank] = 3
+    return p
+
+
 def _rank(rank: int, world: int, port: int, out):
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
@@ -36,8 +44,9 @@ def _rank(rank: int, world: int, port: int, out):
         table = ensemble.gather_tallies(dist, 5, {s: fake_tallies(s) for s in mine})
         slowest = ensemble.reduce_max(dist, 10.0 + rank)
         total = ensemble.reduce_sum(dist, float(len(mine)))
+        prof = ensemble.reduce_profile_sums(dist, fake_profile(rank))
         ensemble.barrier(dist)
-        out.put((rank, table, slowest, total))
+        out.put((rank, table, slowest, total, prof))
     finally:
         dist.destroy_process_group()
 
@@ -60,9 +69,10 @@ def test_two_gloo_ranks_gather_every_systems_tallies():
         p.join(timeout=60)
         assert p.exitcode == 0
     expect = np.stack([ensemble.tally_row(fake_tallies(s)) for s in range(5)])
-    for rank, table, slowest, total in res:
+    for rank, table, slowest, total, prof in res:
         assert np.array_equal(table, expect)
         assert slowest == 11.0 and total == 5.0
+        assert np.array_equal(prof, fake_profile(0) + fake_profile(1))
     tot = ensemble.totals(expect)
     assert tot["collisions"] == sum(1000 + s for s in range(5))
     assert tot["count_periodic_y"] == -sum(range(5))
