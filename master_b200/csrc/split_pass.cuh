@@ -599,6 +599,69 @@ __device__ __forceinline__ unsigned place_sorted(const FlightConst &fc, const Mo
     return nfs;
 }
 
+// Two consecutive cells of at most 32 members each with sorted bottom
+// segments and one system: place_sorted<R, 1> for both, written as one
+// straight-line body so that the two cells' dependency chains interleave.
+// nfs[k]: stayers of cell k.  All lanes call.
+template <int R>
+__device__ __forceinline__ void place_pair(const FlightConst &fc, const MoveSmem<R> &W, int tail, const int base[2],
+                                          const int n[2], const int nb[2], uint4 *Aout, float4 *Bout, int lane,
+                                          unsigned nfs[2]) {
+    const unsigned below = (1u << lane) - 1u;
+    uint4 ra[2];
+    float4 rb[2];
+    bool stay[2];
+    uint32_t id[2];
+    unsigned fast[2], slow[2], bm[2], add[2], pb[2];
+    int t1 = tail + n[0];
+    if (t1 >= R) t1 -= R;
+    const int tl[2] = {tail, t1};
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const bool valid = lane < n[k];
+        stay[k] = false;
+        if (valid) {
+            int r = tl[k] + lane;
+            if (r >= R) r -= R;
+            ra[k] = W.A[r];
+            rb[k] = W.B[r];
+            stay[k] = first_flight_raw(fc, ra[k], rb[k]);
+        }
+        id[k] = valid ? __float_as_uint(rb[k].w) : 0xffffffffu;
+        fast[k] = __ballot_sync(0xffffffffu, valid && stay[k]);
+        slow[k] = __ballot_sync(0xffffffffu, valid && !stay[k]);
+        bm[k] = nb[k] >= 32 ? 0xffffffffu : (1u << nb[k]) - 1u;
+        add[k] = pb[k] = 0;
+    }
+    // arrival j of each cell: staying arrivals below every member, bottom
+    // stayers below the arrival (both cells in every iteration)
+    const int nt0 = n[0] - nb[0], nt1 = n[1] - nb[1];
+    const int ntmax = max(nt0, nt1);
+    for (int j = 0; j < ntmax; ++j) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const bool has = j < (k ? nt1 : nt0);
+            const int li = (nb[k] + j) & 31;
+            const uint32_t t = __shfl_sync(0xffffffffu, id[k], li);
+            const unsigned ts = has ? (fast[k] >> li) & 1u : 0u;
+            add[k] += ts && t < id[k];
+            const unsigned bl = (unsigned)__popc(fast[k] & bm[k] & __ballot_sync(0xffffffffu, id[k] < t));
+            if (has && lane == li) pb[k] = bl;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        if (lane < n[k]) {
+            const unsigned dst =
+                stay[k] ? (unsigned)base[k] + (lane < nb[k] ? (unsigned)__popc(fast[k] & bm[k] & below) : pb[k]) + add[k]
+                        : (unsigned)(base[k] + n[k]) - 1u - (unsigned)__popc(slow[k] & below);
+            Aout[dst] = ra[k];
+            Bout[dst] = rb[k];
+        }
+        nfs[k] = (unsigned)__popc(fast[k]);
+    }
+}
+
 template <int R>
 __global__ void __launch_bounds__(32 * M_WARPS) move_cells_kernel(const __grid_constant__ PassParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -709,6 +772,28 @@ __global__ void __launch_bounds__(32 * M_WARPS) move_cells_kernel(const __grid_c
             continue;
         }
         stage_ahead();  // the cell in work is staged once this returns
+        // Two small cells of one system with sorted bottoms go together.
+        if (P.sorted_in && ahead >= 2 && ci + 1 < T.ncell && T.sys[ci + 1] == T.sys[ci] &&
+            T.sys[ci] == tsys && T.nb[ci] + T.nt[ci] <= 32u && T.nb[ci + 1] + T.nt[ci + 1] <= 32u) {
+            cp_async_wait(ahead - 2);
+            __syncwarp();
+            const int pn[2] = {(int)(T.nb[ci] + T.nt[ci]), (int)(T.nb[ci + 1] + T.nt[ci + 1])};
+            const int pnb[2] = {(int)T.nb[ci], (int)T.nb[ci + 1]};
+            const int pbase[2] = {T.base[ci], T.base[ci + 1]};
+            unsigned nfs[2];
+            place_pair<R>(fc, W, tail, pbase, pn, pnb, Aout, Bout, lane, nfs);
+            if (lane == ci) nfs_mine = nfs[0];
+            if (lane == ci + 1) nfs_mine = nfs[1];
+            const int m = pn[0] + pn[1];
+            moved += (unsigned)m;
+            __syncwarp();  // every lane is done with the cells' ring slots
+            tail += m;
+            if (tail >= R) tail -= R;
+            used -= m;
+            ahead -= 2;
+            ci += 2;
+            continue;
+        }
         cp_async_wait(ahead - 1);
         __syncwarp();
 
