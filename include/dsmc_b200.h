@@ -199,6 +199,32 @@ typedef struct dsmc_system_info {
 } dsmc_system_info;
 int dsmc_system_info_get(dsmc_ctx *ctx, int sys_id, dsmc_system_info *info);
 
+/* One x-slab of a geometry, for a run over several GPUs (the reference's
+ * domain decomposition, dsmc/topology.cpp + System::mpi_move,
+ * dsmc/system.cpp:49-105, along x): the system owns the active cells with
+ * cell x index in [cell_x0, cell_x1) and holds the whole geometry for the
+ * mover.  Particle init and dsmc_particles_set keep the particles of the
+ * slab's cells (ids stay the geometry-wide indices).  A slab is its
+ * context's only system, runs in split precision, and advances one step per
+ * dsmc_step; after each step dsmc_exchange_take hands out the particles that
+ * ended in another slab's cell and dsmc_exchange_put takes in those that
+ * ended in this one, before the next step.  dsmc_particles_get on a slab
+ * needs buffers for every id of the geometry and marks the ids it does not
+ * hold with cell = -1. */
+int dsmc_system_add_slab(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t ny, uint32_t nz,
+                         const uint8_t *voxels, const float *normals, const float *tangents1, const float *tangents2,
+                         float porosity_global, int cell_x0, int cell_x1, int *sys_id);
+/* Exchange records are 32 bytes: uint32 voxel (i | j << 11 | k << 22),
+ * uint32 x offset (float bits; the top bit flags a non-empty voxel), float y
+ * and z offsets in voxel units; float vx, vy, vz, uint32 id.  The owner of a
+ * record is the slab holding cell x index i / (nx / cells_x).
+ * take: moves the outgoing records into `records` (host memory, or device
+ * memory of the context's GPU when device != 0) and sets *n;
+ * DSMC_ERR_CAPACITY, with *n set and nothing taken, when cap < *n.
+ * put: inserts n records, each in a cell of system sys_id. */
+int dsmc_exchange_take(dsmc_ctx *ctx, int64_t cap, void *records, int device, int64_t *n);
+int dsmc_exchange_put(dsmc_ctx *ctx, int sys_id, int64_t n, const void *records, int device);
+
 /* Maxwellian velocities and uniform positions in empty voxels, as
  * System::setup_molecules (dsmc/system.cpp:398-430); draws come from one
  * counter-based stream per particle.  n < 0: the reference's count. */

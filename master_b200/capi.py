@@ -40,6 +40,7 @@ EXPORTED = [
     "dsmc_pass_times_get", "dsmc_state_file_read", "dsmc_state_file_write", "dsmc_tocontinue_read",
     "dsmc_tocontinue_write", "dsmc_continue_from", "dsmc_checkpoint_save", "dsmc_checkpoint_load",
     "dsmc_profile_sums_get", "dsmc_profiles_finish", "dsmc_profiles_get", "dsmc_measures_get",
+    "dsmc_system_add_slab", "dsmc_exchange_take", "dsmc_exchange_put",
 ]
 
 
@@ -167,6 +168,10 @@ def load() -> C.CDLL:
         "dsmc_checkpoint_load": [_P, C.c_char_p],
         "dsmc_profile_sums_get": [_P, C.c_int, C.c_int, _D, C.POINTER(C.c_int)],
         "dsmc_measures_get": [_P, C.c_int, C.POINTER(Measures)],
+        "dsmc_system_add_slab": [_P, C.POINTER(Settings), C.c_uint32, C.c_uint32, C.c_uint32, _U8, _F, _F, _F,
+                                 C.c_float, C.c_int, C.c_int, C.POINTER(C.c_int)],
+        "dsmc_exchange_take": [_P, C.c_int64, C.c_void_p, C.c_int, C.POINTER(C.c_int64)],
+        "dsmc_exchange_put": [_P, C.c_int, C.c_int64, C.c_void_p, C.c_int],
         "dsmc_profiles_finish": [C.POINTER(Settings), C.c_double, C.c_int, _D, _D, _D, _D, _D, _D, _D],
         "dsmc_profiles_get": [_P, C.c_int, C.c_int, _D, _D, _D, _D, _D, _D, C.POINTER(C.c_int)],
         "dsmc_cells_layout": [C.POINTER(Settings), C.c_uint32, C.c_uint32, C.c_uint32, _U8, C.c_int, _I32, _I32,

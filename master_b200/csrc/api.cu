@@ -65,6 +65,8 @@ struct SysHost {
     double volume_global = 0;         // L_x L_y L_z * porosity_global (dsmc/system.cpp:314)
     int prof_bins = 0;
     DevBuf<double> prof;              // sampler profiles: 3*bins y-binned sums, then the v_x histogram
+    bool slab = false;                // owns only the cells with x index in [slab_x0, slab_x1)
+    int slab_x0 = 0, slab_x1 = 0;
 };
 
 }  // namespace dsmc
@@ -99,6 +101,9 @@ struct dsmc_ctx {
     DevBuf<SpillRec> spill;
     unsigned spill_cap = 1u << 16;
     DevBuf<int2> walls;       // wall-flight list of the production pass (one entry per slot at most)
+    DevBuf<uint4> out;        // outgoing list of a slab: particles that ended in another slab's cell
+    unsigned out_cap = 0;
+    bool slab = false;        // the context holds a slab system (its only system)
     int cur = 0;
     int cphase = 0;           // occupancy set the next pass reads
     bool sorted = false;      // every bottom segment is sorted by id (a production pass ran last)
@@ -172,6 +177,8 @@ ParticleArrays particle_arrays(dsmc_ctx *ctx) {
     p.spill_cap = ctx->spill_cap;
     p.walls = ctx->walls.p;
     p.walls_cap = (unsigned)std::min<size_t>(ctx->slots, 0xffffffffu);
+    p.out = ctx->out.p;
+    p.out_cap = ctx->out.p ? ctx->out_cap : 0u;
     return p;
 }
 
@@ -442,7 +449,8 @@ int rebuild_cells(dsmc_ctx *ctx) {
         s.dev.active_begin = s.active_begin;
         s.dev.active_end = s.active_end;
         std::vector<int> map_abs(s.cell_map.size());
-        for (size_t g = 0; g < s.cell_map.size(); ++g) map_abs[g] = s.cell_map[g] < 0 ? -1 : s.cell_map[g] + s.active_begin;
+        for (size_t g = 0; g < s.cell_map.size(); ++g)
+            map_abs[g] = s.cell_map[g] < 0 ? s.cell_map[g] : s.cell_map[g] + s.active_begin;
         CK(s.cell_map_dev.ensure(map_abs.size()));
         CK(cudaMemcpyAsync(s.cell_map_dev.p, map_abs.data(), map_abs.size() * sizeof(int), cudaMemcpyHostToDevice,
                            ctx->stream));
@@ -531,10 +539,20 @@ int dsmc_sync(dsmc_ctx *ctx) {
     return DSMC_OK;
 }
 
-int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t ny, uint32_t nz,
-                    const uint8_t *voxels, const float *normals, const float *tangents1, const float *tangents2,
-                    float porosity_global, int *sys_id) {
+// A system over the whole geometry, or (cx1 >= 0) an x-slab that owns the
+// active cells with cell x index in [cx0, cx1).
+static int system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t ny, uint32_t nz,
+                      const uint8_t *voxels, const float *normals, const float *tangents1, const float *tangents2,
+                      float porosity_global, int cx0, int cx1, int *sys_id) {
     if (!ctx || !s || !voxels || !normals || !tangents1 || !tangents2 || !sys_id) return DSMC_ERR_ARG;
+    const bool slab = cx1 >= 0;
+    if (ctx->slab) return fail(ctx, DSMC_ERR_CONFIG, "a slab is its context's only system");
+    if (slab) {
+        if (!ctx->systems.empty()) return fail(ctx, DSMC_ERR_CONFIG, "a slab is its context's only system");
+        if (is_fp64(ctx)) return fail(ctx, DSMC_ERR_CONFIG, "slabs run in split precision");
+        if (cx0 < 0 || cx0 >= cx1 || cx1 > s->cells_x)
+            return fail(ctx, DSMC_ERR_CONFIG, "slab cell range must satisfy 0 <= x0 < x1 <= cells_x");
+    }
     cudaSetDevice(ctx->device);
     if (nx == 0 || ny == 0 || nz == 0 || nx > 2048 || ny > 2048 || nz > 1024)
         return fail(ctx, DSMC_ERR_CAPACITY, "voxel grid limited to 2048 x 2048 x 1024");
@@ -596,7 +614,34 @@ int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t
         rc2 = dsmc_cells_layout(s, nx, ny, nz, voxels, nc, h->cell_global.data(), h->pixels.data(),
                                 h->total_pixels.data(), h->volume_cell.data(), h->coeff.data(), &nc);
         if (rc2) return fail(ctx, rc2, thread_error());
-        h->cell_map.assign(s->cells_x * s->cells_y * s->cells_z, -1);
+        h->cell_map.assign(s->cells_x * s->cells_y * s->cells_z, DSMC_CELL_SOLID);
+        if (slab) {
+            // keep the slab's cells; the other active cells are foreign
+            const int yz = s->cells_y * s->cells_z;
+            int k = 0;
+            for (int c = 0; c < nc; ++c) {
+                const int cg = h->cell_global[c], x = cg / yz;
+                if (x < cx0 || x >= cx1) {
+                    h->cell_map[cg] = DSMC_CELL_FOREIGN;
+                    continue;
+                }
+                h->cell_global[k] = cg;
+                h->pixels[k] = h->pixels[c];
+                h->total_pixels[k] = h->total_pixels[c];
+                h->volume_cell[k] = h->volume_cell[c];
+                h->coeff[k] = h->coeff[c];
+                ++k;
+            }
+            nc = k;
+            h->cell_global.resize(nc);
+            h->pixels.resize(nc);
+            h->total_pixels.resize(nc);
+            h->volume_cell.resize(nc);
+            h->coeff.resize(nc);
+            h->slab = true;
+            h->slab_x0 = cx0;
+            h->slab_x1 = cx1;
+        }
         for (int c = 0; c < nc; ++c) h->cell_map[h->cell_global[c]] = c;
     }
     // Device geometry.
@@ -663,6 +708,13 @@ int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t
         d.vx_bin = (4 * sd - d.vx_min) / h->prof_bins;
     }
 
+    if (slab) {
+        // outgoing records: a quarter of the geometry's particles at most
+        // per step (an overflow is reported, never written past the end)
+        ctx->out_cap = (unsigned)std::min<int64_t>(std::max<int64_t>(h->expected / 4, 1 << 16), 1 << 28);
+        CK(ctx->out.alloc(2 * (size_t)ctx->out_cap));
+        ctx->slab = true;
+    }
     ctx->systems.push_back(std::move(h));
     *sys_id = (int)ctx->systems.size() - 1;
     // The staged keys index the old cell numbering; rebuild with the new
@@ -682,6 +734,20 @@ int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t
         CK(cudaMemcpyAsync(ctx->hist.p, hc.data(), hc.size() * sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
     }
     return relayout(ctx, staged);
+}
+
+int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t ny, uint32_t nz,
+                    const uint8_t *voxels, const float *normals, const float *tangents1, const float *tangents2,
+                    float porosity_global, int *sys_id) {
+    return system_add(ctx, s, nx, ny, nz, voxels, normals, tangents1, tangents2, porosity_global, 0, -1, sys_id);
+}
+
+int dsmc_system_add_slab(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t ny, uint32_t nz,
+                         const uint8_t *voxels, const float *normals, const float *tangents1, const float *tangents2,
+                         float porosity_global, int cell_x0, int cell_x1, int *sys_id) {
+    if (cell_x1 < 0) return DSMC_ERR_ARG;
+    return system_add(ctx, s, nx, ny, nz, voxels, normals, tangents1, tangents2, porosity_global, cell_x0, cell_x1,
+                      sys_id);
 }
 
 int dsmc_cells_layout(const dsmc_settings *s, uint32_t nx, uint32_t ny, uint32_t nz, const uint8_t *voxels, int cap,
@@ -805,6 +871,20 @@ static int place_particles(dsmc_ctx *ctx, int sys_id, long long n, const double 
     }
     h.num_particles = n;
     h.id_count = (uint32_t)n;
+    if (h.slab) {
+        // the slab keeps the particles in its own cells (ids are the global indices)
+        const int C = h.active_end - h.active_begin;
+        std::vector<unsigned> counts(std::max(C, 1), 0u);
+        if (C)
+            CK(cudaMemcpyAsync(counts.data(), ctx->hist.p + h.active_begin, C * sizeof(unsigned),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        long long kept = 0;
+        for (int c = 0; c < C; ++c) kept += counts[c];
+        h.num_particles = kept;
+        if (h.settings.max_molecules_per_node > 0 && kept > h.settings.max_molecules_per_node)
+            return fail(ctx, DSMC_ERR_CAPACITY, "the slab holds more than max_molecules_per_node particles");
+    }
     return relayout(ctx, staged + n);
 }
 
@@ -818,7 +898,7 @@ int dsmc_particles_init(dsmc_ctx *ctx, int sys_id, int64_t n) {
     if (!ctx || sys_id < 0 || sys_id >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
     SysHost &h = *ctx->systems[sys_id];
     if (n < 0) n = h.expected;
-    if (n > h.settings.max_molecules_per_node && h.settings.max_molecules_per_node > 0) {
+    if (n > h.settings.max_molecules_per_node && h.settings.max_molecules_per_node > 0 && !h.slab) {
         char buf[200];
         std::snprintf(buf, sizeof(buf), "Node 0 wants to create %lld molecules (MAX_MOLECULE_NUM=%d)", (long long)n,
                       h.settings.max_molecules_per_node);
@@ -904,6 +984,7 @@ int dsmc_checkpoint_save(dsmc_ctx *ctx, const char *path) {
     cudaError_t e;
     Status st = read_status(ctx, &e);
     CK(e);
+    if (st.nout) return fail(ctx, DSMC_ERR_STATE, "take the outgoing records of the slab before a checkpoint");
     CkptHeader hd;
     std::memset(&hd, 0, sizeof(hd));
     std::memcpy(hd.magic, kCkptMagic, 8);
@@ -1046,12 +1127,18 @@ int dsmc_particles_get(dsmc_ctx *ctx, int sys_id, int64_t cap, double *r, double
     if (rc) return rc;
     SysHost &h = *ctx->systems[sys_id];
     *n = h.num_particles;
-    if (cap < h.num_particles) return fail(ctx, DSMC_ERR_CAPACITY, "output buffers smaller than the particle count");
-    const long long N = h.num_particles;
+    // a slab holds some of the geometry's ids: entries run over every id and
+    // cell[i] = -1 marks the ids it does not hold
+    const long long N = h.slab ? (long long)h.id_count : h.num_particles;
+    if (h.slab && !cell) return fail(ctx, DSMC_ERR_ARG, "a slab reports which ids it holds through cell");
+    if (cap < N)
+        return fail(ctx, DSMC_ERR_CAPACITY, h.slab ? "output buffers smaller than the geometry's id count"
+                                                   : "output buffers smaller than the particle count");
     CK(ctx->io_r.ensure(3 * std::max<long long>(N, 1)));
     CK(ctx->io_v.ensure(3 * std::max<long long>(N, 1)));
     CK(ctx->io_cell.ensure(std::max<long long>(N, 1)));
     if (N == 0) return DSMC_OK;
+    if (h.slab) CK(cudaMemsetAsync(ctx->io_cell.p, 0xff, N * sizeof(int), ctx->stream));
     cudaError_t e = is_fp64(ctx)
                         ? fp64::launch_to_fp64(ctx->sys_dev.p, sys_id, cell_arrays(ctx), particle_arrays(ctx), ctx->cur,
                                                ctx->cphase, 0, N, ctx->io_r.p, ctx->io_v.p, ctx->io_cell.p, &ctx->status.p->error,
@@ -1071,6 +1158,11 @@ int dsmc_step(dsmc_ctx *ctx, int nsteps) {
     if (!ctx || nsteps < 0) return DSMC_ERR_ARG;
     if (ctx->systems.empty() || nsteps == 0) return DSMC_OK;
     cudaSetDevice(ctx->device);
+    if (ctx->slab) {
+        if (nsteps != 1) return fail(ctx, DSMC_ERR_ARG, "a slab advances one step between exchanges");
+        if (!(ctx->use_pipelined && ctx->fused_grids[1] > 0))
+            return fail(ctx, DSMC_ERR_CONFIG, "a slab needs the production pass (cells too large for it)");
+    }
     ctx->keys_valid = false;
     int left = nsteps;
     while (left > 0) {
@@ -1101,8 +1193,64 @@ int dsmc_step(dsmc_ctx *ctx, int nsteps) {
     return DSMC_OK;
 }
 
+int dsmc_exchange_take(dsmc_ctx *ctx, int64_t cap, void *records, int device, int64_t *n) {
+    if (!ctx || !n || cap < 0 || (cap > 0 && !records)) return DSMC_ERR_ARG;
+    *n = 0;
+    if (!ctx->slab) return DSMC_OK;
+    cudaSetDevice(ctx->device);
+    cudaError_t e;
+    Status st = read_status(ctx, &e);
+    CK(e);
+    if (st.nout > ctx->out_cap)
+        return fail(ctx, DSMC_ERR_STATE, "more particles left the slab in one step than its outgoing list holds");
+    *n = st.nout;
+    if ((int64_t)st.nout > cap) return fail(ctx, DSMC_ERR_CAPACITY, "record buffer smaller than the outgoing count");
+    if (st.nout) {
+        CK(cudaMemcpyAsync(records, ctx->out.p, 2 * sizeof(uint4) * st.nout,
+                           device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
+        const unsigned zero = 0;
+        CK(cudaMemcpyAsync(&ctx->status.p->nout, &zero, sizeof(zero), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        ctx->systems[0]->num_particles -= st.nout;
+    }
+    return DSMC_OK;
+}
+
+int dsmc_exchange_put(dsmc_ctx *ctx, int sys_id, int64_t n, const void *records, int device) {
+    if (!ctx || sys_id < 0 || sys_id >= (int)ctx->systems.size() || n < 0 || (n > 0 && !records))
+        return DSMC_ERR_ARG;
+    if (!ctx->slab) return fail(ctx, DSMC_ERR_CONFIG, "records enter a slab system only");
+    if (n == 0) return DSMC_OK;
+    cudaSetDevice(ctx->device);
+    SysHost &h = *ctx->systems[sys_id];
+    const uint4 *src = static_cast<const uint4 *>(records);
+    DevBuf<uint4> staged;
+    if (!device) {
+        CK(staged.alloc(2 * (size_t)n));
+        CK(cudaMemcpyAsync(staged.p, records, 2 * sizeof(uint4) * n, cudaMemcpyHostToDevice, ctx->stream));
+        src = staged.p;
+    }
+    CK(split32::launch_put(ctx->sys_dev.p, sys_id, cell_arrays(ctx), particle_arrays(ctx), ctx->cur, ctx->cphase, n,
+                           src, ctx->status.p, ctx->stream));
+    cudaError_t e;
+    Status st = read_status(ctx, &e);
+    CK(e);
+    h.num_particles += n;
+    if (st.error & DSMC_EBIT_CELL) return fail(ctx, DSMC_ERR_STATE, "a record lies outside the slab's cells");
+    if (st.error & DSMC_EBIT_FATAL) return fail(ctx, DSMC_ERR_STATE, "records could not be placed");
+    if (st.spill) {
+        // cells without room: repack with the overflow records
+        long long staged_n = 0;
+        int rc = stage_present(ctx, 0, -1, &staged_n);
+        if (rc) return rc;
+        return relayout(ctx, staged_n);
+    }
+    return DSMC_OK;
+}
+
 int dsmc_stage_move(dsmc_ctx *ctx) {
     if (!ctx) return DSMC_ERR_ARG;
+    if (ctx->slab) return fail(ctx, DSMC_ERR_CONFIG, "a slab moves through dsmc_step and the exchange");
     cudaSetDevice(ctx->device);
     int rc = flush_pending(ctx);
     if (rc) return rc;
@@ -1114,6 +1262,7 @@ int dsmc_stage_move(dsmc_ctx *ctx) {
 
 int dsmc_stage_sort(dsmc_ctx *ctx) {
     if (!ctx) return DSMC_ERR_ARG;
+    if (ctx->slab) return fail(ctx, DSMC_ERR_CONFIG, "a slab moves through dsmc_step and the exchange");
     cudaSetDevice(ctx->device);
     int rc = flush_pending(ctx);
     if (rc) return rc;

@@ -52,6 +52,10 @@
     (DSMC_EBIT_CELL | DSMC_EBIT_RESEED | DSMC_EBIT_SPILL_FULL | DSMC_EBIT_SMEM | DSMC_EBIT_NAN | DSMC_EBIT_TIMEOUT | \
      DSMC_EBIT_ALIGN | DSMC_EBIT_WALL)
 
+// cell_map values of cells that are not this system's active cells
+#define DSMC_CELL_SOLID (-1)    // no free volume
+#define DSMC_CELL_FOREIGN (-2)  // owned by another slab of the geometry
+
 #define DSMC_VOX_PACK(i, j, k) ((uint32_t)(i) | ((uint32_t)(j) << 11) | ((uint32_t)(k) << 22))
 #define DSMC_VOX_I(p) ((int)((p)&0x7FFu))
 #define DSMC_VOX_J(p) ((int)(((p) >> 11) & 0x7FFu))
@@ -131,7 +135,8 @@ struct Status {
     unsigned int blocks_done;  // end-of-pass counter used to advance `step`
     unsigned int halted;       // non-zero: a pass saw spill/error; later passes do nothing
     unsigned int walls;        // entries in the wall-flight list this pass (production pass)
-    unsigned int pad[2];
+    unsigned int nout;         // records in the outgoing list (particles that left a slab)
+    unsigned int pad;
 };
 
 struct SpillRec {
@@ -163,8 +168,10 @@ struct ParticleArrays {
     void *B[2];
     SpillRec *spill;
     unsigned spill_cap;
-    int2 *walls;               // production pass: {output slot, system} of flights that meet a wall
+    int2 *walls;               // production pass: {output slot, source cell} of flights that meet a wall
     unsigned walls_cap;
+    uint4 *out;                // outgoing list: record k is {A, B} at out[2k], out[2k + 1]
+    unsigned out_cap;
 };
 
 struct PassParams {

@@ -45,6 +45,10 @@ int fused_block();                  // threads per block of the production kerne
 int fused_grids(int smem_cap, int num_sms, int grids[4]);
 // ev: null, or five events recorded before each kernel and after the last
 cudaError_t launch_fused(const PassParams &P, const int grids[4], cudaStream_t st, cudaEvent_t *ev = nullptr);
+// Records from another slab into system s's cells (occupancy set cin of buffer
+// cur): top segments, or the overflow list when a cell is full.
+cudaError_t launch_put(const SysDev *sys, int s, const CellArrays &cells, const ParticleArrays &parts, int cur, int cin,
+                       long long n, const uint4 *rec, Status *status, cudaStream_t st);
 }  // namespace split32
 
 // Pass modes (engine.cuh PassMode).

@@ -53,8 +53,8 @@ template <> struct Maker<Fp64> {
 __device__ __forceinline__ int particle_cell(const SysDev &g, const Particle &p, unsigned *err) {
     const int cg = Prec::cell_global(g, p);
     const int ac = __ldg(g.cell_map + cg);
-    if (ac < 0) atomicOr(err, DSMC_EBIT_CELL);
-    return ac;
+    if (ac == DSMC_CELL_SOLID) atomicOr(err, DSMC_EBIT_CELL);
+    return ac;  // DSMC_CELL_FOREIGN: another slab's cell, the particle is left out
 }
 
 // Flat fp64 state (the reference's state-file layout) -> flat records + cell keys.

@@ -105,5 +105,13 @@ cudaError_t launch_fused(const PassParams &P, const int grids[4], cudaStream_t s
     return e;
 }
 
+cudaError_t launch_put(const SysDev *sys, int s, const CellArrays &cells, const ParticleArrays &parts, int cur, int cin,
+                       long long n, const uint4 *rec, Status *status, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    const int grid = (int)std::min<long long>((n + 255) / 256, 148LL * 8);
+    pass3::put_records_kernel<<<grid, 256, 0, st>>>(sys, s, cells, parts, cur, cin, n, rec, status);
+    return cudaGetLastError();
+}
+
 }  // namespace split32
 }  // namespace dsmc

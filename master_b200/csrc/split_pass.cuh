@@ -990,12 +990,45 @@ __device__ __forceinline__ void insert_top(const PassParams &P, const Split32::P
     if (valid && lane == leader && over) atomicSub(&top_out[key], (unsigned)__popc(over));
 }
 
-// New active cell of a particle that completed its flight; false when the
-// particle ended in a cell without free volume (stranded: it stays out).
-__device__ __forceinline__ bool new_cell(const SysDev &g, const Split32::Particle &p, unsigned &key) {
+// Where a particle that completed its flight goes: its new active cell; or,
+// when it ended inside solid whose cell has no free volume, its source cell
+// (the reference aborts there, dsmc/system.h:134-142; the particle's next
+// move re-seeds it, dsmc/moleculemover.cpp:57-60); or, in another slab's
+// cell, the outgoing list (`leave`).  False only for the outgoing list.
+__device__ __forceinline__ bool new_cell(const SysDev &g, const Split32::Particle &p, int src, unsigned &key,
+                                         bool &leave, MoveCounts &cnt, unsigned &err) {
     const int ac = __ldg(g.cell_map + Split32::cell_global(g, p));
-    key = (unsigned)ac;
-    return ac >= 0;
+    leave = ac == DSMC_CELL_FOREIGN;
+    if (ac >= 0) {
+        key = (unsigned)ac;
+    } else if (!leave) {
+        err |= DSMC_EBIT_STRANDED;
+        ++cnt.stranded;
+        key = (unsigned)src;
+    }
+    return !leave;
+}
+
+// Appends the particles of the valid lanes to the outgoing list (one atomic
+// per warp).  All lanes call.
+__device__ __forceinline__ void leave_slab(const PassParams &P, const Split32::Particle &p, bool valid, unsigned &err) {
+    const int lane = threadIdx.x & 31;
+    const unsigned vm = __ballot_sync(0xffffffffu, valid);
+    if (!vm) return;
+    unsigned at = 0;
+    if (lane == __ffs(vm) - 1) at = atomicAdd(&P.status->nout, (unsigned)__popc(vm));
+    at = __shfl_sync(0xffffffffu, at, __ffs(vm) - 1) + (unsigned)__popc(vm & ((1u << lane) - 1u));
+    if (valid) {
+        if (at < P.parts.out_cap) {
+            uint4 ra;
+            float4 rb;
+            Split32::pack(p, ra, rb);
+            P.parts.out[2 * (size_t)at] = ra;
+            P.parts.out[2 * (size_t)at + 1] = *reinterpret_cast<const uint4 *>(&rb);
+        } else {
+            err |= DSMC_EBIT_SPILL_FULL;
+        }
+    }
 }
 
 // Appends the warp's collected wall flights to the list (one atomic per
@@ -1068,6 +1101,7 @@ __global__ void __launch_bounds__(32 * P_WARPS, 8) place_movers_kernel(const __g
             }
             const int slot = __shfl_sync(0xffffffffu, gap, c) + (f - __shfl_sync(0xffffffffu, pre, c));
             const int psys = __shfl_sync(0xffffffffu, sys, c);
+            const int src = first + c;  // the mover's cell
             const int csys = common_system(valid, psys);
             if (csys != tsys) {
                 counts_publish(P, tsys, cnt, false);
@@ -1078,30 +1112,25 @@ __global__ void __launch_bounds__(32 * P_WARPS, 8) place_movers_kernel(const __g
             mt.wall_hits = mt.reseeds = 0;
             mt.cross[0] = mt.cross[1] = mt.cross[2] = 0;
             mt.err = 0;
-            bool done = false, place = false;
+            bool done = false, place = false, leave = false;
             unsigned key = 0;
             if (valid) {
                 Split32::unpack(Aout[slot], Bout[slot], p);
                 const SysDev &g = P.sys[psys];
                 done = Split32::move_open(g, p, mt);
-                if (done) {
-                    place = new_cell(g, p, key);
-                    if (!place) {
-                        mt.err |= DSMC_EBIT_STRANDED;
-                        ++cnt.stranded;
-                    }
-                }
+                if (done) place = new_cell(g, p, src, key, leave, cnt, mt.err);
             }
             // flights that meet a wall stay in their slot for place_walls
             const unsigned wall = __ballot_sync(0xffffffffu, valid && !done);
             if (wall) {
                 if (W.qn + __popc(wall) > WQ) flush_walls(P, W);
-                if (valid && !done) W.q[W.qn + __popc(wall & ((1u << lane) - 1u))] = make_int2(slot, psys);
+                if (valid && !done) W.q[W.qn + __popc(wall & ((1u << lane) - 1u))] = make_int2(slot, src);
                 __syncwarp();
                 if (lane == 0) W.qn += __popc(wall);
                 __syncwarp();
             }
             insert_top(P, p, place, key, mt.err);
+            leave_slab(P, p, leave, mt.err);
             counts_add(cnt, mt);
             if (tsys == -2) counts_publish(P, psys, cnt, true);
         }
@@ -1128,8 +1157,9 @@ __global__ void __launch_bounds__(32 * W_WARPS) place_walls_kernel(const __grid_
     for (unsigned i0 = (blockIdx.x * W_WARPS + (threadIdx.x >> 5)) * 32u; i0 < nwalls; i0 += wstride) {
         const unsigned i = i0 + lane;
         const bool valid = i < nwalls;
-        const int2 e = valid ? P.parts.walls[i] : make_int2(0, -1);
-        const int csys = common_system(valid, e.y);
+        const int2 e = valid ? P.parts.walls[i] : make_int2(0, -1);  // {slot, source cell}
+        const int esys = valid ? P.cells.meta[e.y].w : -1;
+        const int csys = common_system(valid, esys);
         if (csys != tsys) {
             counts_publish(P, tsys, cnt, false);
             tsys = csys;
@@ -1140,10 +1170,10 @@ __global__ void __launch_bounds__(32 * W_WARPS) place_walls_kernel(const __grid_
         mt.cross[0] = mt.cross[1] = mt.cross[2] = 0;
         mt.err = 0;
         unsigned key = 0;
-        bool place = false;
+        bool place = false, leave = false;
         // the lanes of a warp share their system unless it is mixed; a mixed
         // warp moves its lanes one system at a time
-        const int s0 = valid ? e.y : -1;
+        const int s0 = esys;
         if (valid) Split32::unpack(Aout[e.x], Bout[e.x], p);
         for (unsigned todo = __ballot_sync(0xffffffffu, valid); todo;) {
             const int sys = __shfl_sync(0xffffffffu, s0, __ffs(todo) - 1);
@@ -1151,16 +1181,11 @@ __global__ void __launch_bounds__(32 * W_WARPS) place_walls_kernel(const __grid_
             Split32::move_general_warp(P.sys[sys], p, move_step, mt, mine);
             todo &= ~__ballot_sync(0xffffffffu, mine);
         }
-        if (valid) {
-            place = new_cell(P.sys[e.y], p, key);
-            if (!place) {
-                mt.err |= DSMC_EBIT_STRANDED;
-                ++cnt.stranded;
-            }
-        }
+        if (valid) place = new_cell(P.sys[esys], p, e.y, key, leave, cnt, mt.err);
         insert_top(P, p, place, key, mt.err);
+        leave_slab(P, p, leave, mt.err);
         counts_add(cnt, mt);
-        if (tsys == -2) counts_publish(P, e.y, cnt, true);
+        if (tsys == -2) counts_publish(P, esys, cnt, true);
     }
     counts_publish(P, tsys, cnt, false);
 
@@ -1175,6 +1200,54 @@ __global__ void __launch_bounds__(32 * W_WARPS) place_walls_kernel(const __grid_
                 atomicExch(&P.status->halted, 1u);
             atomicExch(&P.status->walls, 0u);
             atomicExch(&P.status->blocks_done, 0u);
+        }
+    }
+}
+
+// ---- slab exchange ----------------------------------------------------------
+
+// Records that arrive from another slab (the receiving side of the
+// reference's mpi_move, dsmc/system.cpp:49-105): each goes into the top
+// segment of its cell, above the bottom segment, or into the overflow list
+// (the host then repacks).  A record outside this system's cells is an error.
+__global__ void put_records_kernel(const SysDev *sys, int s, const CellArrays cells, const ParticleArrays parts,
+                                   int cur, int cin, long long n, const uint4 *rec, Status *status) {
+    const SysDev &g = sys[s];
+    uint4 *A = reinterpret_cast<uint4 *>(parts.A[cur]);
+    float4 *B = reinterpret_cast<float4 *>(parts.B[cur]);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const uint4 ra = rec[2 * i];
+        const uint4 rbits = rec[2 * i + 1];
+        const float4 rb = *reinterpret_cast<const float4 *>(&rbits);
+        Split32::Particle p;
+        Split32::unpack(ra, rb, p);
+        if (p.c[0] < 0 || p.c[0] >= g.n[0] || p.c[1] >= g.n[1] || p.c[2] >= g.n[2]) {
+            atomicOr(&status->error, DSMC_EBIT_CELL);
+            continue;
+        }
+        const int ac = __ldg(g.cell_map + Split32::cell_global(g, p));
+        if (ac < 0) {
+            atomicOr(&status->error, DSMC_EBIT_CELL);
+            continue;
+        }
+        const int4 m = cells.meta[ac];
+        const unsigned nb = min(cells.bot[cin][ac], (unsigned)m.y);
+        const unsigned j = atomicAdd(&cells.top[cin][ac], 1u);
+        if (nb + j < (unsigned)m.y) {
+            const unsigned dst = (unsigned)(m.x + m.y) - 1u - j;
+            A[dst] = ra;
+            B[dst] = rb;
+        } else {
+            atomicSub(&cells.top[cin][ac], 1u);
+            const unsigned si = atomicAdd(&status->spill, 1u);
+            if (si < parts.spill_cap) {
+                SpillRec &sr = parts.spill[si];
+                sr.a = ra;
+                sr.b = rbits;
+                sr.cell = ac;
+            } else {
+                atomicOr(&status->error, DSMC_EBIT_SPILL_FULL);
+            }
         }
     }
 }

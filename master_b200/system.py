@@ -233,6 +233,58 @@ class Context:
                                             C.c_float(geometry.porosity_global), C.byref(sid)))
         return sid.value
 
+    def add_slab(self, settings: Settings, geometry: Geometry, cell_x0: int, cell_x1: int) -> int:
+        """The x-slab of the geometry holding cells with x index in
+        [cell_x0, cell_x1): the context's only system (master_b200.slab)."""
+        sid = C.c_int()
+        nx, ny, nz = geometry.shape
+        self.check(self.lib.dsmc_system_add_slab(self.handle, C.byref(settings.raw), nx, ny, nz,
+                                                 ptr(geometry.voxels, C.c_uint8), ptr(geometry.normals, C.c_float),
+                                                 ptr(geometry.tangents1, C.c_float),
+                                                 ptr(geometry.tangents2, C.c_float),
+                                                 C.c_float(geometry.porosity_global), cell_x0, cell_x1,
+                                                 C.byref(sid)))
+        return sid.value
+
+    def exchange_take(self) -> np.ndarray:
+        """The records that left the slab in the last step, shape (n, 8)
+        uint32 (dsmc_exchange_take's layout), now removed from the slab."""
+        n = C.c_int64()
+        rc = self.lib.dsmc_exchange_take(self.handle, 0, None, 0, C.byref(n))
+        if rc not in (0, capi.DSMC_ERR_CAPACITY):
+            self.check(rc)
+        out = np.empty((n.value, 8), np.uint32)
+        if n.value:
+            self.check(self.lib.dsmc_exchange_take(self.handle, n.value, out.ctypes.data, 0, C.byref(n)))
+        return out[:n.value]
+
+    def exchange_take_device(self, torch_device):
+        """exchange_take into a tensor on the context's GPU (int32 view of the records)."""
+        import torch
+        n = C.c_int64()
+        rc = self.lib.dsmc_exchange_take(self.handle, 0, None, 1, C.byref(n))
+        if rc not in (0, capi.DSMC_ERR_CAPACITY):
+            self.check(rc)
+        out = torch.empty((n.value, 8), dtype=torch.int32, device=torch_device)
+        if n.value:
+            torch.cuda.synchronize(torch_device)
+            self.check(self.lib.dsmc_exchange_take(self.handle, n.value, C.c_void_p(out.data_ptr()), 1, C.byref(n)))
+        return out
+
+    def exchange_put(self, sys_id: int, records) -> None:
+        """Records (n, 8) from other slabs into system sys_id: a numpy array
+        on the host, or a tensor on the context's GPU."""
+        if hasattr(records, "data_ptr") and getattr(records, "is_cuda", False):
+            if records.shape[0]:
+                import torch
+                torch.cuda.synchronize(records.device)
+                self.check(self.lib.dsmc_exchange_put(self.handle, sys_id, records.shape[0],
+                                                      C.c_void_p(records.contiguous().data_ptr()), 1))
+            return
+        rec = np.ascontiguousarray(np.asarray(records).view(np.uint32).reshape(-1, 8))
+        if rec.shape[0]:
+            self.check(self.lib.dsmc_exchange_put(self.handle, sys_id, rec.shape[0], rec.ctypes.data, 0))
+
     def step(self, n: int = 1):
         self.check(self.lib.dsmc_step(self.handle, n))
 
