@@ -136,7 +136,7 @@ struct Status {
     unsigned int halted;       // non-zero: a pass saw spill/error; later passes do nothing
     unsigned int walls;        // entries in the wall-flight list this pass (production pass)
     unsigned int nout;         // records in the outgoing list (particles that left a slab)
-    unsigned int pad;
+    unsigned int walls_taken;  // wall-flight entries claimed by place_walls' warps this pass
 };
 
 struct SpillRec {

@@ -313,11 +313,20 @@ __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __gri
                 const int k = f - __shfl_sync(0xffffffffu, start, c);
                 const int cb = __shfl_sync(0xffffffffu, m.x, c), cc = __shfl_sync(0xffffffffu, m.y, c);
                 const int cnb = (int)__shfl_sync(0xffffffffu, nb, c), cnt = __shfl_sync(0xffffffffu, n, c) - cnb;
-                if (f < total) {
-                    const int sl = member_slot(cb, cc, cnb, cnt, k);
-                    W.slot[f] = sl;
-                    W.ids[f] = __float_as_uint(Bin[sl].w);
+                if (f < total) W.slot[f] = member_slot(cb, cc, cnb, cnt, k);
+            }
+            __syncwarp();
+            // the members' ids, four loads in flight per lane
+            for (int f0 = lane; f0 < total; f0 += 128) {
+                uint32_t v[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int f = f0 + 32 * u;
+                    v[u] = f < total ? __float_as_uint(Bin[W.slot[f]].w) : 0u;
                 }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (f0 + 32 * u < total) W.ids[f0 + 32 * u] = v[u];
             }
             __syncwarp();
             // Cells with a sorted bottom and few arrivals: each lane sorts its
@@ -1153,8 +1162,13 @@ __global__ void __launch_bounds__(32 * W_WARPS) place_walls_kernel(const __grid_
     MoveCounts cnt;
     counts_reset(cnt);
     int tsys = -1;
-    const unsigned wstride = gridDim.x * W_WARPS * 32u;
-    for (unsigned i0 = (blockIdx.x * W_WARPS + (threadIdx.x >> 5)) * 32u; i0 < nwalls; i0 += wstride) {
+    // warps claim 32 entries at a time: flights differ widely in length, so
+    // a warp that finishes early takes more
+    for (;;) {
+        unsigned i0 = 0;
+        if (lane == 0) i0 = atomicAdd(&P.status->walls_taken, 32u);
+        i0 = __shfl_sync(0xffffffffu, i0, 0);
+        if (i0 >= nwalls) break;
         const unsigned i = i0 + lane;
         const bool valid = i < nwalls;
         const int2 e = valid ? P.parts.walls[i] : make_int2(0, -1);  // {slot, source cell}
@@ -1199,6 +1213,7 @@ __global__ void __launch_bounds__(32 * W_WARPS) place_walls_kernel(const __grid_
             if (atomicAdd(&P.status->spill, 0u) != 0u || (atomicAdd(&P.status->error, 0u) & DSMC_EBIT_FATAL) != 0u)
                 atomicExch(&P.status->halted, 1u);
             atomicExch(&P.status->walls, 0u);
+            atomicExch(&P.status->walls_taken, 0u);
             atomicExch(&P.status->blocks_done, 0u);
         }
     }
