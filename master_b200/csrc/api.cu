@@ -39,6 +39,9 @@ template <class T> struct DevBuf {
         return e;
     }
     cudaError_t ensure(size_t count) { return count <= n && p ? cudaSuccess : alloc(count); }
+    // ensure with 1/16 headroom on growth, so that capacities that drift up
+    // between repacks do not reallocate every time
+    cudaError_t ensure_grow(size_t count) { return count <= n && p ? cudaSuccess : alloc(count + count / 16); }
 };
 
 struct SysHost {
@@ -232,12 +235,12 @@ int relayout(dsmc_ctx *ctx, long long total) {
     ctx->smem_cap = (int)((maxcap + 31u) & ~31u);
     ctx->slots = slots;
     const size_t half = ctx->rec_half();
-    CK(ctx->A0.ensure(slots * half));
-    CK(ctx->A1.ensure(slots * half));
-    CK(ctx->B0.ensure(slots * half));
-    CK(ctx->B1.ensure(slots * half));
-    CK(ctx->key.ensure(slots));
-    CK(ctx->walls.ensure(std::max<size_t>(slots, 1)));
+    CK(ctx->A0.ensure_grow(slots * half));
+    CK(ctx->A1.ensure_grow(slots * half));
+    CK(ctx->B0.ensure_grow(slots * half));
+    CK(ctx->B1.ensure_grow(slots * half));
+    CK(ctx->key.ensure_grow(slots));
+    CK(ctx->walls.ensure_grow(std::max<size_t>(slots, 1)));
     CK(ctx->meta.ensure(std::max(C, 1)));
     if (C) {
         CK(cudaMemcpyAsync(ctx->meta.p, ctx->h_meta.data(), C * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
