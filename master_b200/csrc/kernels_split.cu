@@ -44,7 +44,7 @@ template <class K> static int static_blocks(K kernel, int threads) {
 // Ring slots per warp of move_cells for cells of at most `smem_cap` slots
 // (0: no ring is large enough, or a cell could exceed the collide batch).
 int fused_capacity(int smem_cap) {
-    static const int rings[] = {64, 96, 128, 160, 192, 224, 256};
+    static const int rings[] = {64, 96, 128, 160, 192, 224, 256, 320, 384, 448, 512};
     if (smem_cap > pass3::PCAP) return 0;
     for (int r : rings)
         if (smem_cap <= r) return r;
@@ -53,7 +53,7 @@ int fused_capacity(int smem_cap) {
 
 int fused_block() { return 32 * pass3::M_WARPS; }
 
-#define DSMC_MOVE_RINGS(X) X(64) X(96) X(128) X(160) X(192) X(224) X(256)
+#define DSMC_MOVE_RINGS(X) X(64) X(96) X(128) X(160) X(192) X(224) X(256) X(320) X(384) X(448) X(512)
 
 int fused_grids(int smem_cap, int num_sms, int grids[4]) {
     int bm = 0;
