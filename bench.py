@@ -140,6 +140,7 @@ def cpu_reference(steps: int, replicas: int | None = None):
     mol = res["reports"][0].get("molecules")
     return {
         "value": res["particle_steps_per_s"], "unit": UNIT, "cores": cores, "kind": "reference",
+        "particles_per_replica": mol,
         "sample": (f"{cores} independent single-rank runs of the reference solver (oracle/_ref/dsmc_ref, g++ -O3) on "
                    f"a 64^3 box of the same voxel size, sphere radius, porosity, gas and simulator weight "
                    f"({mol} particles each), {steps} timesteps; its own stage timers (moving+colliding+"
@@ -157,11 +158,19 @@ def run_reference_arm(args, world, rank, pg):
     except Exception as e:  # noqa: BLE001
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU solver could not run: {e}"}))
         return 0
+    from master_b200 import workloads
+    W = workloads.WORKLOADS[args.workload]
+    per_replica = cb.get("particles_per_replica")
+    # a step of one replica: its particles over its share of the throughput
+    ms = (1e3 * per_replica * cb["cores"] / cb["value"]) if per_replica and cb["value"] else None
     line = {
         "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": min(steps, 200),
-        "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "warmup": 0, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": "packed_256 (bounded 64^3 sample on host cores)", "parallelism": "replicas"},
+        # the reference's timers cover every step of its run: no warm-up to leave out
+        "config": {"workload": W.name, "voxels": W.n, "cells": W.cells, "atoms_per_molecule": W.atoms_per_molecule,
+                   "parallelism": f"{cb['cores']} replicas on host cores",
+                   "sample": "bounded 64^3 sample of the workload per replica (cpu_baseline.sample)"},
         "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": time.time() - t0,
     }
