@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -131,6 +132,15 @@ struct dsmc_ctx {
     long long tpasses = 0;
     double cap_factor = 2.0;
     int cap_pad = 24;
+    // The production pass as CUDA graphs, one per pass configuration (buffer
+    // parity, occupancy set, sorted bottoms, collide, sample); every buffer
+    // pointer is baked into the graphs, so any (re)allocation drops them.
+    bool use_graphs = true;
+    std::map<int, cudaGraphExec_t> graphs;
+    void drop_graphs() {
+        for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+        graphs.clear();
+    }
 
     size_t rec_half() const { return precision == DSMC_PREC_FP64 ? 32 : 16; }
 };
@@ -186,6 +196,7 @@ ParticleArrays particle_arrays(dsmc_ctx *ctx) {
 }
 
 int upload_sys_table(dsmc_ctx *ctx) {
+    ctx->drop_graphs();  // the table may move
     std::vector<SysDev> t;
     for (auto &s : ctx->systems) t.push_back(s->dev);
     CK(ctx->sys_dev.ensure(std::max<size_t>(t.size(), 1)));
@@ -205,6 +216,7 @@ Status read_status(dsmc_ctx *ctx, cudaError_t *err) {
 // Rebuilds every cell table and slot buffer from flat staged particles.
 // fA/fB/fkey hold `total` records; hist holds per-cell counts.
 int relayout(dsmc_ctx *ctx, long long total) {
+    ctx->drop_graphs();  // slot buffers and grids may change
     const int C = ctx->num_cells;
     std::vector<unsigned> counts(C);
     if (C) CK(cudaMemcpyAsync(counts.data(), ctx->hist.p, C * sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
@@ -330,6 +342,30 @@ int stage_present(dsmc_ctx *ctx, long long extra, int skip, long long *staged) {
 // Runs the collide + sample of the last step if it is still pending.
 int flush_pending(dsmc_ctx *ctx);
 
+// One production pass from its cached graph, captured on first use.
+cudaError_t launch_fused_graph(dsmc_ctx *ctx, const PassParams &P) {
+    const int key = P.cur | (P.cin << 1) | (P.sorted_in << 3) | (P.do_collide << 4) | (P.do_sample << 5) |
+                    (P.do_move << 6);
+    auto it = ctx->graphs.find(key);
+    if (it == ctx->graphs.end()) {
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        const cudaError_t el = split32::launch_fused(P, ctx->fused_grids, ctx->stream, nullptr);
+        e = cudaStreamEndCapture(ctx->stream, &g);
+        if (el != cudaSuccess || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return el != cudaSuccess ? el : e;
+        }
+        cudaGraphExec_t x = nullptr;
+        e = cudaGraphInstantiate(&x, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return e;
+        it = ctx->graphs.emplace(key, x).first;
+    }
+    return cudaGraphLaunch(it->second, ctx->stream);
+}
+
 int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, int advance) {
     PassParams P;
     P.sys = ctx->sys_dev.p;
@@ -351,7 +387,17 @@ int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, 
     if (mode == PASS_FUSED && ctx->use_pipelined && ctx->fused_grids[1] > 0) {
         P.top_only = 0;
         ctx->sorted = true;  // move_cells leaves every bottom segment sorted
-        e = split32::launch_fused(P, ctx->fused_grids, ctx->stream, ctx->timing ? ctx->tev : nullptr);
+        if (ctx->use_graphs && !ctx->timing && advance) {
+            e = launch_fused_graph(ctx, P);
+            if (e != cudaSuccess) {  // capture refused: plain launches from here on
+                cudaGetLastError();
+                ctx->drop_graphs();
+                ctx->use_graphs = false;
+                e = split32::launch_fused(P, ctx->fused_grids, ctx->stream, nullptr);
+            }
+        } else {
+            e = split32::launch_fused(P, ctx->fused_grids, ctx->stream, ctx->timing ? ctx->tev : nullptr);
+        }
         if (e == cudaSuccess && ctx->timing) {
             CK(cudaEventSynchronize(ctx->tev[4]));
             for (int k = 0; k < 4; ++k) {
@@ -419,6 +465,7 @@ int flush_pending(dsmc_ctx *ctx) {
 }
 
 int rebuild_cells(dsmc_ctx *ctx) {
+    ctx->drop_graphs();
     // Keep the cell state and tallies of the systems already present: a new
     // system's cells are appended after theirs.
     const int C_old = ctx->num_cells;
@@ -529,6 +576,7 @@ void dsmc_ctx_destroy(dsmc_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    ctx->drop_graphs();
     for (cudaEvent_t &e : ctx->tev)
         if (e) cudaEventDestroy(e);
     cudaStream_t s = ctx->stream;
