@@ -67,8 +67,19 @@ struct SysHost {
     double sqrt_t_over_m = 0;
     double vr_max0 = 0;
     double volume_global = 0;         // L_x L_y L_z * porosity_global (dsmc/system.cpp:314)
-    int prof_bins = 0;
-    DevBuf<double> prof;              // sampler profiles: 3*bins y-binned sums, then the v_x histogram
+    int prof_bins = 0, prof_copies = 1;
+    DevBuf<double> prof;              // sampler profiles: copies of {3*bins y-binned sums, v_x histogram}
+    size_t prof_len() const { return (size_t)prof_copies * 4 * (size_t)prof_bins; }
+    // the copies added up: the 4*bins sums
+    cudaError_t prof_sums(std::vector<double> &out, cudaStream_t st) const {
+        std::vector<double> all(prof_len());
+        cudaError_t e = cudaMemcpyAsync(all.data(), prof.p, all.size() * sizeof(double), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        out.assign(4 * (size_t)prof_bins, 0.0);
+        for (int c = 0; c < prof_copies; ++c)
+            for (size_t i = 0; i < out.size(); ++i) out[i] += all[(size_t)c * out.size() + i];
+        return e;
+    }
     bool slab = false;                // owns only the cells with x index in [slab_x0, slab_x1)
     int slab_x0 = 0, slab_x1 = 0;
 };
@@ -747,11 +758,14 @@ static int system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32
     d.sample_begin = s->sample_begin;
     // Sampler profiles (dsmc/statisticssampler.cpp:22-26): sampling_bins bins
     // in y, and a v_x histogram over [-4 sigma, 4 sigma], sigma = sqrt(T/m).
+    // Up to 64 copies, 16 MB at most, so that a sample's atomics spread.
     h->prof_bins = s->sampling_bins;
-    CK(h->prof.alloc(4 * (size_t)h->prof_bins));
-    CK(cudaMemsetAsync(h->prof.p, 0, 4 * (size_t)h->prof_bins * sizeof(double), ctx->stream));
+    h->prof_copies = (int)std::max<size_t>(1, std::min<size_t>(64, ((size_t)1 << 21) / (4 * (size_t)h->prof_bins)));
+    CK(h->prof.alloc(h->prof_len()));
+    CK(cudaMemsetAsync(h->prof.p, 0, h->prof_len() * sizeof(double), ctx->stream));
     d.prof = h->prof.p;
     d.prof_bins = h->prof_bins;
+    d.prof_copies = h->prof_copies;
     d.mass = s->mass;
     {
         const double sd = std::sqrt(temperature / s->mass);
@@ -1026,12 +1040,7 @@ int dsmc_checkpoint_save(dsmc_ctx *ctx, const char *path) {
     }
     if (S) CK(cudaMemcpyAsync(tally.data(), ctx->tally.p, S * sizeof(SysTally), cudaMemcpyDeviceToHost, ctx->stream));
     std::vector<std::vector<double>> prof(S);
-    for (int s = 0; s < S; ++s) {
-        const SysHost &h = *ctx->systems[s];
-        prof[s].resize(4 * (size_t)h.prof_bins);
-        CK(cudaMemcpyAsync(prof[s].data(), h.prof.p, prof[s].size() * sizeof(double), cudaMemcpyDeviceToHost,
-                           ctx->stream));
-    }
+    for (int s = 0; s < S; ++s) CK(ctx->systems[s]->prof_sums(prof[s], ctx->stream));
     cudaError_t e;
     Status st = read_status(ctx, &e);
     CK(e);
@@ -1158,6 +1167,8 @@ int dsmc_checkpoint_load(dsmc_ctx *ctx, const char *path) {
     }
     if (S) CK(cudaMemcpyAsync(ctx->tally.p, tally.data(), S * sizeof(SysTally), cudaMemcpyHostToDevice, ctx->stream));
     for (int s = 0; s < S; ++s)
+        CK(cudaMemsetAsync(ctx->systems[s]->prof.p, 0, ctx->systems[s]->prof_len() * sizeof(double), ctx->stream));
+    for (int s = 0; s < S; ++s)  // the saved sums into the first copy
         CK(cudaMemcpyAsync(ctx->systems[s]->prof.p, prof[s].data(), prof[s].size() * sizeof(double),
                            cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(&ctx->status.p->step, &hd.step, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
@@ -1449,8 +1460,9 @@ int dsmc_profile_sums_get(dsmc_ctx *ctx, int sys_id, int cap, double *sums, int 
     *bins = h.prof_bins;
     if (!sums) return DSMC_OK;
     if (cap < 4 * h.prof_bins) return fail(ctx, DSMC_ERR_CAPACITY, "profile buffer smaller than 4 * sampling_bins");
-    CK(cudaMemcpyAsync(sums, h.prof.p, 4 * (size_t)h.prof_bins * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    std::vector<double> total;
+    CK(h.prof_sums(total, ctx->stream));
+    std::memcpy(sums, total.data(), total.size() * sizeof(double));
     return DSMC_OK;
 }
 
@@ -1477,7 +1489,7 @@ int dsmc_tallies_reset(dsmc_ctx *ctx, int sys_id) {
     CK(cudaMemsetAsync(ctx->tally.p + sys_id, 0, sizeof(SysTally), ctx->stream));
     const int C = h.active_end - h.active_begin;
     if (C > 0) CK(cudaMemsetAsync(ctx->mom.p + 8 * (size_t)h.active_begin, 0, 8 * (size_t)C * sizeof(double), ctx->stream));
-    CK(cudaMemsetAsync(h.prof.p, 0, 4 * (size_t)h.prof_bins * sizeof(double), ctx->stream));
+    CK(cudaMemsetAsync(h.prof.p, 0, h.prof_len() * sizeof(double), ctx->stream));
     cudaError_t e;
     Status st = read_status(ctx, &e);
     CK(e);

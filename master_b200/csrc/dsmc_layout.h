@@ -107,9 +107,12 @@ struct SysDev {
     // y-binned profiles of the sampler (dsmc/statisticalproperty.cpp:229-362):
     // per bin {particle count, sum v_z, sum 1/2 m v_z^2} over the samples
     // and the v_x histogram of MeasureVelocityDistribution (bins of width
-    // vx_bin from vx_min = -4 sqrt(T/m)), stored after the 3*bins sums
+    // vx_bin from vx_min = -4 sqrt(T/m)), stored after the 3*bins sums;
+    // prof_copies copies of these 4*bins sums, each warp adding to one of
+    // them (every particle of a sample lands in one of a few bins: with one
+    // copy the atomics queue on those few addresses); the host adds them up
     double *prof;
-    int prof_bins;
+    int prof_bins, prof_copies;
     double mass, vx_min, vx_bin;
 };
 

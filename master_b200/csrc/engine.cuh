@@ -114,6 +114,11 @@ __device__ __forceinline__ bool cl_normal(real v_norm_in, real factor, real max_
 }
 
 // ---- sampler profiles -------------------------------------------------------
+// The calling warp's copy of the system's profile sums.
+__device__ __forceinline__ double *profile_copy(const SysDev &g) {
+    const unsigned w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    return g.prof + (size_t)(w % (unsigned)g.prof_copies) * 4 * (size_t)g.prof_bins;
+}
 // Bin of a y position as MeasureCount and friends take it
 // (dsmc/statisticalproperty.cpp:236): int(r_y * (1/L_y) * bins), kept in range.
 __device__ __forceinline__ int profile_bin(const SysDev &g, double y) {
@@ -135,9 +140,10 @@ __device__ __forceinline__ void profile_add_warp(const SysDev &g, bool valid, in
             ee += __shfl_xor_sync(0xffffffffu, ee, o);
         }
         if ((threadIdx.x & 31) == 0) {
-            atomicAdd(g.prof + 3 * b, cc);
-            atomicAdd(g.prof + 3 * b + 1, ss);
-            atomicAdd(g.prof + 3 * b + 2, ee);
+            double *pr = profile_copy(g);
+            atomicAdd(pr + 3 * b, cc);
+            atomicAdd(pr + 3 * b + 1, ss);
+            atomicAdd(pr + 3 * b + 2, ee);
         }
         todo &= ~__ballot_sync(0xffffffffu, in);
     }
@@ -147,7 +153,7 @@ __device__ __forceinline__ void profile_add_warp(const SysDev &g, bool valid, in
 // bin int((v_x - v_min) / width), truncated toward zero, counted when in range.
 __device__ __forceinline__ void profile_vx(const SysDev &g, double vx) {
     const int b = (int)((vx - g.vx_min) / g.vx_bin);
-    if (b >= 0 && b < g.prof_bins) atomicAdd(g.prof + 3 * g.prof_bins + b, 1.0);
+    if (b >= 0 && b < g.prof_bins) atomicAdd(profile_copy(g) + 3 * g.prof_bins + b, 1.0);
 }
 
 struct Split32 {

@@ -178,6 +178,7 @@ __device__ __noinline__ void sample_cell(const PassParams &P, const SysDev &g, i
                                          unsigned nt, int n) {
     const float4 *Bin = reinterpret_cast<const float4 *>(P.parts.B[P.cur]);
     const uint4 *Ain = reinterpret_cast<const uint4 *>(P.parts.A[P.cur]);
+    double *pr = profile_copy(g);
     double m1[3] = {0, 0, 0}, m2[3] = {0, 0, 0};
     // y-binned profile: a run per bin, flushed when the bin changes
     int pbin = -1;
@@ -189,9 +190,9 @@ __device__ __noinline__ void sample_cell(const PassParams &P, const SysDev &g, i
         const int bin = profile_bin(g, Split32::y_of(g, Ain[sl]));
         if (bin != pbin) {
             if (pbin >= 0) {
-                atomicAdd(g.prof + 3 * pbin, pc);
-                atomicAdd(g.prof + 3 * pbin + 1, ps);
-                atomicAdd(g.prof + 3 * pbin + 2, pe);
+                atomicAdd(pr + 3 * pbin, pc);
+                atomicAdd(pr + 3 * pbin + 1, ps);
+                atomicAdd(pr + 3 * pbin + 2, pe);
             }
             pbin = bin;
             pc = ps = pe = 0;
@@ -208,9 +209,9 @@ __device__ __noinline__ void sample_cell(const PassParams &P, const SysDev &g, i
         m2[2] += z * z;
     }
     if (pbin >= 0) {
-        atomicAdd(g.prof + 3 * pbin, pc);
-        atomicAdd(g.prof + 3 * pbin + 1, ps);
-        atomicAdd(g.prof + 3 * pbin + 2, pe);
+        atomicAdd(pr + 3 * pbin, pc);
+        atomicAdd(pr + 3 * pbin + 1, ps);
+        atomicAdd(pr + 3 * pbin + 2, pe);
     }
     double *M = P.cells.mom + 8 * (size_t)a;
     M[0] += (double)n;
