@@ -171,3 +171,35 @@ def test_two_processes_exchange_over_gloo():
     assert sum(x[4] for x in res) == t1.collisions
     assert sum(x[5] for x in res) == t1.wall_collisions
     assert [sum(x[6][d] for x in res) for d in range(3)] == list(t1.count_periodic)
+
+
+def test_device_records_path_equals_host_path():
+    """The exchange through device buffers (the nccl transport's path:
+    exchange_take_device / exchange_put of CUDA tensors) moves the same
+    records as the host path."""
+    import torch
+    case, K, world = "small_dt5", 6, 2
+    z, meta, s, g = load_case(case)
+    host = [Slab(s, g, r, world, init_particles=False) for r in range(world)]
+    dev = [Slab(s, g, r, world, init_particles=False) for r in range(world)]
+    for sl in host + dev:
+        sl.set_particles(z["r0"], z["v0"])
+    step_local(host, K)
+    cuda = torch.device("cuda", 0)
+    for _ in range(K):
+        for sl in dev:
+            sl.ctx.step(1)
+        outs = [sl.ctx.exchange_take_device(cuda) for sl in dev]
+        for sl in dev:
+            parts = []
+            for o, src in zip(outs, dev):
+                if o.shape[0]:
+                    d = torch.from_numpy(src.destinations(o.cpu().numpy())).to(cuda)
+                    parts.append(o[d == sl.rank])
+            if parts:
+                sl.ctx.exchange_put(sl.id, torch.cat(parts).contiguous())
+    N = z["r0"].shape[0]
+    for a, b in zip(host, dev):
+        ra, va, ca = a.get_particles(N)
+        rb, vb, cb = b.get_particles(N)
+        assert np.array_equal(ca, cb) and np.array_equal(ra, rb) and np.array_equal(va, vb)
