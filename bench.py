@@ -322,8 +322,11 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48 * N / k_e2e,
                 "d2h_bytes_per_step": (48 * N + 64 * k_e2e) / k_e2e, "steps": k_e2e},
         # collide_cells + move_cells + place_movers + place_walls per step
-        # (production pass), one pass kernel per step otherwise
-        "gpu_launches": args.steps * (4 if pipelined else 1),
+        # (production pass) and sample_cells on the sampled steps the timed
+        # passes collide; one pass kernel per step otherwise
+        "gpu_launches": args.steps * (4 if pipelined else 1) + (sum(
+            1 for st in range(args.warmup, args.warmup + args.steps)
+            if st > 0 and st % settings.statistics_interval == 0) if pipelined else 0),
         "clocks": clocks,
         "device_status": {"error_bits": err, "spill": spill},
         "pass": system.ctx.pass_info(),

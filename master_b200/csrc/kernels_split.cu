@@ -63,8 +63,7 @@ int fused_grids(int smem_cap, int num_sms, int grids[4]) {
         DSMC_MOVE_RINGS(X)
 #undef X
     }
-    const int bc = std::min(static_blocks(pass3::collide_cells_kernel<false>, 32 * pass3::C_WARPS),
-                            static_blocks(pass3::collide_cells_kernel<true>, 32 * pass3::C_WARPS));
+    const int bc = static_blocks(pass3::collide_cells_kernel, 32 * pass3::C_WARPS);
     const int bp = static_blocks(pass3::place_movers_kernel, 32 * pass3::P_WARPS);
     const int bw = static_blocks(pass3::place_walls_kernel, 32 * pass3::W_WARPS);
     if (bm <= 0 || bc <= 0 || bp <= 0 || bw <= 0) return 0;
@@ -78,12 +77,14 @@ int fused_grids(int smem_cap, int num_sms, int grids[4]) {
 cudaError_t launch_fused(const PassParams &P, const int grids[4], cudaStream_t st, cudaEvent_t *ev) {
     if (ev) cudaEventRecord(ev[0], st);
     if (P.do_collide || P.do_sample) {
-        if (P.do_sample)
-            pass3::collide_cells_kernel<true><<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
-        else
-            pass3::collide_cells_kernel<false><<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
-        const cudaError_t e = cudaGetLastError();
+        pass3::collide_cells_kernel<<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
+        cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
+        if (P.do_sample) {  // sampled steps only: the host knows the cadence
+            pass3::sample_cells_kernel<<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+        }
     }
     if (ev) cudaEventRecord(ev[1], st);
     cudaError_t e = cudaErrorInvalidValue;

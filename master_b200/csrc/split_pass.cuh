@@ -153,80 +153,21 @@ struct PickPerm {
 };
 
 __device__ __forceinline__ void publish_collide(const PassParams &P, int sys, unsigned col, unsigned cand,
-                                                unsigned smp, bool per_lane) {
+                                                bool per_lane) {
     if (per_lane) {
         if (sys >= 0) {
             if (col) atomicAdd(&P.tally[sys].collisions, (unsigned long long)col);
             if (cand) atomicAdd(&P.tally[sys].candidates, (unsigned long long)cand);
-            if (smp) atomicAdd(&P.tally[sys].samples, (unsigned long long)smp);
         }
         return;
     }
-    const unsigned c = warp_sum(col), d = warp_sum(cand), s = warp_sum(smp);
+    const unsigned c = warp_sum(col), d = warp_sum(cand);
     if ((threadIdx.x & 31) == 0 && sys >= 0) {
         if (c) atomicAdd(&P.tally[sys].collisions, (unsigned long long)c);
         if (d) atomicAdd(&P.tally[sys].candidates, (unsigned long long)d);
-        if (s) atomicAdd(&P.tally[sys].samples, (unsigned long long)s);
     }
 }
 
-// The sampler's pass over one cell (lane-per-cell): fp64 cell moments and the
-// y-binned profiles, on the cadence of StatisticsSampler::sample.  Kept out of
-// line: it runs on sampled steps only and would otherwise raise the register
-// pressure of the collide loop.
-__device__ __noinline__ void sample_cell(const PassParams &P, const SysDev &g, int a, int4 m, unsigned nb,
-                                         unsigned nt, int n) {
-    const float4 *Bin = reinterpret_cast<const float4 *>(P.parts.B[P.cur]);
-    const uint4 *Ain = reinterpret_cast<const uint4 *>(P.parts.A[P.cur]);
-    double *pr = profile_copy(g);
-    double m1[3] = {0, 0, 0}, m2[3] = {0, 0, 0};
-    // y-binned profile: a run per bin, flushed when the bin changes
-    int pbin = -1;
-    double pc = 0, ps = 0, pe = 0;
-    for (int q = 0; q < n; ++q) {
-        const int sl = member_slot(m.x, m.y, (int)nb, (int)nt, q);
-        const float4 b = Bin[sl];
-        const double x = b.x, y = b.y, z = b.z;
-        const int bin = profile_bin(g, Split32::y_of(g, Ain[sl]));
-        if (bin != pbin) {
-            if (pbin >= 0) {
-                atomicAdd(pr + 3 * pbin, pc);
-                atomicAdd(pr + 3 * pbin + 1, ps);
-                atomicAdd(pr + 3 * pbin + 2, pe);
-            }
-            pbin = bin;
-            pc = ps = pe = 0;
-        }
-        pc += 1.0;
-        ps += z;
-        pe += 0.5 * g.mass * z * z;
-        profile_vx(g, x);
-        m1[0] += x;
-        m1[1] += y;
-        m1[2] += z;
-        m2[0] += x * x;
-        m2[1] += y * y;
-        m2[2] += z * z;
-    }
-    if (pbin >= 0) {
-        atomicAdd(pr + 3 * pbin, pc);
-        atomicAdd(pr + 3 * pbin + 1, ps);
-        atomicAdd(pr + 3 * pbin + 2, pe);
-    }
-    double *M = P.cells.mom + 8 * (size_t)a;
-    M[0] += (double)n;
-    M[1] += m1[0];
-    M[2] += m1[1];
-    M[3] += m1[2];
-    M[4] += m2[0];
-    M[5] += m2[1];
-    M[6] += m2[2];
-    M[7] += m2[0] + m2[1] + m2[2];
-}
-
-// SAMPLE: the instance launched on steps where some system samples; the host
-// picks it, so the sampler costs the other steps nothing.
-template <bool SAMPLE>
 __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __grid_constant__ PassParams P) {
     __shared__ CollideSmem smem[C_WARPS];
     const int lane = threadIdx.x & 31;
@@ -238,7 +179,7 @@ __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __gri
 
     const int C = P.cells.num_cells;
     const int nchunks = (C + 31) >> 5;
-    unsigned col = 0, cand = 0, smp = 0;  // this lane's counts for system tsys
+    unsigned col = 0, cand = 0;  // this lane's counts for system tsys
     int tsys = -1;
 
     for (int ch = blockIdx.x * C_WARPS + (threadIdx.x >> 5); ch < nchunks; ch += gridDim.x * C_WARPS) {
@@ -268,8 +209,8 @@ __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __gri
         const int sys = m.w;
         const int csys = common_system(mine, sys);
         if (csys != tsys) {
-            publish_collide(P, tsys, col, cand, smp, false);
-            col = cand = smp = 0;
+            publish_collide(P, tsys, col, cand, false);
+            col = cand = 0;
             tsys = csys;
         }
 
@@ -449,21 +390,76 @@ __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __gri
         if (mine && P.do_collide)
             *reinterpret_cast<double2 *>(&P.cells.state[a]) = make_double2(vr, rest);
 
-        // Sampling on the reference's cadence: cell moments in fp64.
-        if (SAMPLE && mine && P.do_sample) {
-            const SysDev &g = P.sys[sys];
-            if (g.sample_interval > 0 && step > 0 && (step % (uint32_t)g.sample_interval) == 0 &&
-                step >= (uint32_t)g.sample_begin) {
-                sample_cell(P, g, a, m, nb, nt, n);
-                if (a == g.active_begin) ++smp;
-            }
-        }
         if (tsys == -2) {  // a chunk that spans systems: per-lane counts
-            publish_collide(P, sys, col, cand, smp, true);
-            col = cand = smp = 0;
+            publish_collide(P, sys, col, cand, true);
+            col = cand = 0;
         }
     }
-    publish_collide(P, tsys, col, cand, smp, false);
+    publish_collide(P, tsys, col, cand, false);
+}
+
+// ---- sample_cells -----------------------------------------------------------
+
+// The sampler on the reference's cadence (StatisticsSampler::sample,
+// dsmc/statisticssampler.cpp:45-66): every cell's fp64 moments and the
+// y-binned profiles, one warp per cell with its members over the lanes,
+// after collide_cells on sampled steps only.
+__global__ void __launch_bounds__(32 * C_WARPS) sample_cells_kernel(const __grid_constant__ PassParams P) {
+    const int lane = threadIdx.x & 31;
+    const volatile Status *vs = P.status;
+    if (vs->halted) return;
+    const uint32_t step = vs->step;
+    const float4 *Bin = reinterpret_cast<const float4 *>(P.parts.B[P.cur]);
+    const uint4 *Ain = reinterpret_cast<const uint4 *>(P.parts.A[P.cur]);
+    const int C = P.cells.num_cells;
+    const int nwarps = gridDim.x * C_WARPS;
+    for (int a = blockIdx.x * C_WARPS + (threadIdx.x >> 5); a < C; a += nwarps) {
+        const int4 m = P.cells.meta[a];
+        const SysDev &g = P.sys[m.w];
+        if (!(g.sample_interval > 0 && step > 0 && (step % (uint32_t)g.sample_interval) == 0 &&
+              step >= (uint32_t)g.sample_begin))
+            continue;
+        unsigned nb, nt;
+        input_counts(P, a, m, nb, nt);
+        const int n = (int)(nb + nt);
+        double mo[6] = {0, 0, 0, 0, 0, 0};  // sum v, sum v^2 per axis
+        for (int q0 = 0; q0 < n; q0 += 32) {
+            const int q = q0 + lane;
+            const bool ok = q < n;
+            int bin = 0;
+            double x = 0, y = 0, z = 0;
+            if (ok) {
+                const int sl = member_slot(m.x, m.y, (int)nb, (int)nt, q);
+                const float4 b = Bin[sl];
+                x = b.x;
+                y = b.y;
+                z = b.z;
+                bin = profile_bin(g, Split32::y_of(g, Ain[sl]));
+                mo[0] += x;
+                mo[1] += y;
+                mo[2] += z;
+                mo[3] += x * x;
+                mo[4] += y * y;
+                mo[5] += z * z;
+            }
+            profile_add_warp(g, ok, bin, 1.0, z, 0.5 * g.mass * z * z);
+            if (ok) profile_vx(g, x);
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) mo[k] = warp_sum_f64(mo[k]);
+        if (lane == 0) {
+            double *M = P.cells.mom + 8 * (size_t)a;
+            M[0] += (double)n;
+            M[1] += mo[0];
+            M[2] += mo[1];
+            M[3] += mo[2];
+            M[4] += mo[3];
+            M[5] += mo[4];
+            M[6] += mo[5];
+            M[7] += mo[3] + mo[4] + mo[5];
+            if (a == g.active_begin) atomicAdd(&P.tally[m.w].samples, 1ull);
+        }
+    }
 }
 
 // ---- move_cells -------------------------------------------------------------
