@@ -134,7 +134,7 @@ struct dsmc_ctx {
     // launch shape of the cell pass
     int block = 256;
     int grid = 0;
-    int fused_grids[4] = {0, 0, 0, 0};  // production split-precision pass (collide, move, place, walls); 0 = not usable
+    int fused_grids[5] = {0, 0, 0, 0, 0};  // production pass (collide, move, place, walls, sample); 0 = not usable
     bool use_pipelined = true;
     // per-kernel timers of the production pass (dsmc_ctx_set_timing)
     bool timing = false;
@@ -296,7 +296,7 @@ int relayout(dsmc_ctx *ctx, long long total) {
                                     : split32::pass_blocks_per_sm(PASS_SORT, ctx->block, ctx->smem_cap);
     if (bps_in <= 0 || bps_so <= 0) return fail(ctx, DSMC_ERR_CUDA, "stage passes cannot be resident (shared memory)");
     ctx->grid = bps * ctx->num_sms;
-    ctx->fused_grids[0] = ctx->fused_grids[1] = ctx->fused_grids[2] = ctx->fused_grids[3] = 0;
+    for (int &gsz : ctx->fused_grids) gsz = 0;
     if (!is_fp64(ctx) && split32::fused_capacity(ctx->smem_cap) > 0)
         split32::fused_grids(ctx->smem_cap, ctx->num_sms, ctx->fused_grids);
     Status st;

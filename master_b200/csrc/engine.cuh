@@ -151,9 +151,13 @@ __device__ __forceinline__ void profile_add_warp(const SysDev &g, bool valid, in
 
 // MeasureVelocityDistribution::update (dsmc/statisticalproperty.cpp:441-458):
 // bin int((v_x - v_min) / width), truncated toward zero, counted when in range.
-__device__ __forceinline__ void profile_vx(const SysDev &g, double vx) {
+__device__ __forceinline__ int profile_vx_bin(const SysDev &g, double vx) {
     const int b = (int)((vx - g.vx_min) / g.vx_bin);
-    if (b >= 0 && b < g.prof_bins) atomicAdd(profile_copy(g) + 3 * g.prof_bins + b, 1.0);
+    return b >= 0 && b < g.prof_bins ? b : -1;
+}
+__device__ __forceinline__ void profile_vx(const SysDev &g, double vx) {
+    const int b = profile_vx_bin(g, vx);
+    if (b >= 0) atomicAdd(profile_copy(g) + 3 * g.prof_bins + b, 1.0);
 }
 
 struct Split32 {

@@ -40,11 +40,12 @@ namespace split32 {
 // the production pass (split_pass.cuh)
 int fused_capacity(int smem_cap);   // move_cells ring slots per warp; 0: the production pass cannot run
 int fused_block();                  // threads per block of the production kernels
-// Persistent grids of collide_cells, move_cells, place_movers and
-// place_walls; 0 when one of them cannot be resident.
-int fused_grids(int smem_cap, int num_sms, int grids[4]);
+// Persistent grids of collide_cells, move_cells, place_movers, place_walls
+// and sample_cells; 0 when one of them cannot be resident.
+int fused_grids(int smem_cap, int num_sms, int grids[5]);
 // ev: null, or five events recorded before each kernel and after the last
-cudaError_t launch_fused(const PassParams &P, const int grids[4], cudaStream_t st, cudaEvent_t *ev = nullptr);
+// (the sampler, on sampled steps, falls in the collide interval)
+cudaError_t launch_fused(const PassParams &P, const int grids[5], cudaStream_t st, cudaEvent_t *ev = nullptr);
 // Records from another slab into system s's cells (occupancy set cin of buffer
 // cur): top segments, or the overflow list when a cell is full.
 cudaError_t launch_put(const SysDev *sys, int s, const CellArrays &cells, const ParticleArrays &parts, int cur, int cin,

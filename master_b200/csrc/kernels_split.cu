@@ -55,7 +55,7 @@ int fused_block() { return 32 * pass3::M_WARPS; }
 
 #define DSMC_MOVE_RINGS(X) X(64) X(96) X(128) X(160) X(192) X(224) X(256) X(320) X(384) X(448) X(512)
 
-int fused_grids(int smem_cap, int num_sms, int grids[4]) {
+int fused_grids(int smem_cap, int num_sms, int grids[5]) {
     int bm = 0;
     switch (fused_capacity(smem_cap)) {
 #define X(r) \
@@ -66,22 +66,24 @@ int fused_grids(int smem_cap, int num_sms, int grids[4]) {
     const int bc = static_blocks(pass3::collide_cells_kernel, 32 * pass3::C_WARPS);
     const int bp = static_blocks(pass3::place_movers_kernel, 32 * pass3::P_WARPS);
     const int bw = static_blocks(pass3::place_walls_kernel, 32 * pass3::W_WARPS);
-    if (bm <= 0 || bc <= 0 || bp <= 0 || bw <= 0) return 0;
+    const int bs = static_blocks(pass3::sample_cells_kernel, 32 * pass3::C_WARPS);
+    if (bm <= 0 || bc <= 0 || bp <= 0 || bw <= 0 || bs <= 0) return 0;
     grids[0] = bc * num_sms;
     grids[1] = bm * num_sms;
     grids[2] = bp * num_sms;
     grids[3] = bw * num_sms;
+    grids[4] = bs * num_sms;
     return 1;
 }
 
-cudaError_t launch_fused(const PassParams &P, const int grids[4], cudaStream_t st, cudaEvent_t *ev) {
+cudaError_t launch_fused(const PassParams &P, const int grids[5], cudaStream_t st, cudaEvent_t *ev) {
     if (ev) cudaEventRecord(ev[0], st);
     if (P.do_collide || P.do_sample) {
         pass3::collide_cells_kernel<<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         if (P.do_sample) {  // sampled steps only: the host knows the cadence
-            pass3::sample_cells_kernel<<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
+            pass3::sample_cells_kernel<<<grids[4], 32 * pass3::C_WARPS, 0, st>>>(P);
             e = cudaGetLastError();
             if (e != cudaSuccess) return e;
         }

@@ -400,66 +400,118 @@ __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __gri
 
 // ---- sample_cells -----------------------------------------------------------
 
+constexpr int SHIST = 1024;  // v_x histogram bins a warp counts in shared memory
+
 // The sampler on the reference's cadence (StatisticsSampler::sample,
-// dsmc/statisticssampler.cpp:45-66): every cell's fp64 moments and the
-// y-binned profiles, one warp per cell with its members over the lanes,
-// after collide_cells on sampled steps only.
+// dsmc/statisticssampler.cpp:45-66), after collide_cells on sampled steps
+// only: every cell's fp64 moments and the y-binned profiles.  A warp takes a
+// chunk of 32 cells: their headers one per lane, then each sampled cell with
+// its members over the lanes, and at the end each lane adds its own cell's
+// moments.  Each warp counts the v_x histogram in shared memory and adds it to
+// its copy of the sums once per system (every particle lands in one of a few
+// bins: one global atomic per particle queued on those addresses).
 __global__ void __launch_bounds__(32 * C_WARPS) sample_cells_kernel(const __grid_constant__ PassParams P) {
+    __shared__ unsigned hist[C_WARPS][SHIST];
     const int lane = threadIdx.x & 31;
     const volatile Status *vs = P.status;
     if (vs->halted) return;
     const uint32_t step = vs->step;
     const float4 *Bin = reinterpret_cast<const float4 *>(P.parts.B[P.cur]);
     const uint4 *Ain = reinterpret_cast<const uint4 *>(P.parts.A[P.cur]);
-    const int C = P.cells.num_cells;
-    const int nwarps = gridDim.x * C_WARPS;
-    for (int a = blockIdx.x * C_WARPS + (threadIdx.x >> 5); a < C; a += nwarps) {
-        const int4 m = P.cells.meta[a];
-        const SysDev &g = P.sys[m.w];
-        if (!(g.sample_interval > 0 && step > 0 && (step % (uint32_t)g.sample_interval) == 0 &&
-              step >= (uint32_t)g.sample_begin))
-            continue;
-        unsigned nb, nt;
-        input_counts(P, a, m, nb, nt);
-        const int n = (int)(nb + nt);
-        double mo[6] = {0, 0, 0, 0, 0, 0};  // sum v, sum v^2 per axis
-        for (int q0 = 0; q0 < n; q0 += 32) {
-            const int q = q0 + lane;
-            const bool ok = q < n;
-            int bin = 0;
-            double x = 0, y = 0, z = 0;
-            if (ok) {
-                const int sl = member_slot(m.x, m.y, (int)nb, (int)nt, q);
-                const float4 b = Bin[sl];
-                x = b.x;
-                y = b.y;
-                z = b.z;
-                bin = profile_bin(g, Split32::y_of(g, Ain[sl]));
-                mo[0] += x;
-                mo[1] += y;
-                mo[2] += z;
-                mo[3] += x * x;
-                mo[4] += y * y;
-                mo[5] += z * z;
-            }
-            profile_add_warp(g, ok, bin, 1.0, z, 0.5 * g.mass * z * z);
-            if (ok) profile_vx(g, x);
+    unsigned *H = hist[threadIdx.x >> 5];
+    for (int b = lane; b < SHIST; b += 32) H[b] = 0;
+    __syncwarp();
+    int hsys = -1;  // the system whose histogram H holds
+    auto flush = [&]() {
+        if (hsys >= 0) {
+            const SysDev &gh = P.sys[hsys];
+            double *pr = profile_copy(gh) + 3 * (size_t)gh.prof_bins;
+            for (int b = lane; b < gh.prof_bins; b += 32)
+                if (H[b]) {
+                    atomicAdd(pr + b, (double)H[b]);
+                    H[b] = 0;
+                }
+            __syncwarp();
         }
+    };
+    const int C = P.cells.num_cells;
+    const int nchunks = (C + 31) >> 5;
+    const int nwarps = gridDim.x * C_WARPS;
+    for (int ch = blockIdx.x * C_WARPS + (threadIdx.x >> 5); ch < nchunks; ch += nwarps) {
+        const int a = ch * 32 + lane;
+        int4 m = make_int4(0, 0, 0, -1);
+        unsigned nb = 0, nt = 0;
+        bool smp = false;
+        if (a < C) {
+            m = P.cells.meta[a];
+            input_counts(P, a, m, nb, nt);
+            const SysDev &g = P.sys[m.w];
+            smp = g.sample_interval > 0 && step > 0 && (step % (uint32_t)g.sample_interval) == 0 &&
+                  step >= (uint32_t)g.sample_begin;
+        }
+        double own[6] = {0, 0, 0, 0, 0, 0};  // this lane's cell: sum v, sum v^2 per axis
+        for (unsigned todo = __ballot_sync(0xffffffffu, smp); todo; todo &= todo - 1u) {
+            const int c = __ffs(todo) - 1;
+            const int sys = __shfl_sync(0xffffffffu, m.w, c);
+            const int cb = __shfl_sync(0xffffffffu, m.x, c), cc = __shfl_sync(0xffffffffu, m.y, c);
+            const int cnb = (int)__shfl_sync(0xffffffffu, nb, c), cnt = (int)__shfl_sync(0xffffffffu, nt, c);
+            const int n = cnb + cnt;
+            const SysDev &g = P.sys[sys];
+            const bool local = g.prof_bins <= SHIST;
+            if (local && sys != hsys) {
+                flush();
+                hsys = sys;
+            }
+            double mo[6] = {0, 0, 0, 0, 0, 0};
+            for (int q0 = 0; q0 < n; q0 += 32) {
+                const int q = q0 + lane;
+                const bool ok = q < n;
+                int bin = 0;
+                double x = 0, y = 0, z = 0;
+                if (ok) {
+                    const int sl = member_slot(cb, cc, cnb, cnt, q);
+                    const float4 b = Bin[sl];
+                    x = b.x;
+                    y = b.y;
+                    z = b.z;
+                    bin = profile_bin(g, Split32::y_of(g, Ain[sl]));
+                    mo[0] += x;
+                    mo[1] += y;
+                    mo[2] += z;
+                    mo[3] += x * x;
+                    mo[4] += y * y;
+                    mo[5] += z * z;
+                }
+                profile_add_warp(g, ok, bin, 1.0, z, 0.5 * g.mass * z * z);
+                if (ok) {
+                    if (local) {
+                        const int hb = profile_vx_bin(g, x);
+                        if (hb >= 0) atomicAdd(&H[hb], 1u);
+                    } else {
+                        profile_vx(g, x);
+                    }
+                }
+            }
 #pragma unroll
-        for (int k = 0; k < 6; ++k) mo[k] = warp_sum_f64(mo[k]);
-        if (lane == 0) {
+            for (int k = 0; k < 6; ++k) {
+                mo[k] = warp_sum_f64(mo[k]);
+                if (lane == c) own[k] = mo[k];
+            }
+        }
+        if (smp) {
             double *M = P.cells.mom + 8 * (size_t)a;
-            M[0] += (double)n;
-            M[1] += mo[0];
-            M[2] += mo[1];
-            M[3] += mo[2];
-            M[4] += mo[3];
-            M[5] += mo[4];
-            M[6] += mo[5];
-            M[7] += mo[3] + mo[4] + mo[5];
-            if (a == g.active_begin) atomicAdd(&P.tally[m.w].samples, 1ull);
+            M[0] += (double)(nb + nt);
+            M[1] += own[0];
+            M[2] += own[1];
+            M[3] += own[2];
+            M[4] += own[3];
+            M[5] += own[4];
+            M[6] += own[5];
+            M[7] += own[3] + own[4] + own[5];
+            if (a == P.sys[m.w].active_begin) atomicAdd(&P.tally[m.w].samples, 1ull);
         }
     }
+    flush();
 }
 
 // ---- move_cells -------------------------------------------------------------
