@@ -402,14 +402,37 @@ __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __gri
 
 constexpr int SHIST = 1024;  // v_x histogram bins a warp counts in shared memory
 
+// Eight per-lane values summed over the warp, transposed: lane l returns the
+// sum of slot l >> 2 (lanes 4j..4j+3 hold the sum of slot j).  Each exchange
+// halves the slots a lane carries (4, 2, 1, then two plain steps): 9 fp64
+// shuffles where eight separate reductions take 40.  All lanes call.
+__device__ __forceinline__ double warp_transpose_sum8(const double (&v)[8], int lane) {
+    const bool b4 = lane & 16, b3 = lane & 8, b2 = lane & 4;
+    double w[4], u[2];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+        w[i] = (b4 ? v[i + 4] : v[i]) + __shfl_xor_sync(0xffffffffu, b4 ? v[i] : v[i + 4], 16);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+        u[i] = (b3 ? w[i + 2] : w[i]) + __shfl_xor_sync(0xffffffffu, b3 ? w[i] : w[i + 2], 8);
+    double t = (b2 ? u[1] : u[0]) + __shfl_xor_sync(0xffffffffu, b2 ? u[0] : u[1], 4);
+    t += __shfl_xor_sync(0xffffffffu, t, 2);
+    t += __shfl_xor_sync(0xffffffffu, t, 1);
+    return t;
+}
+
 // The sampler on the reference's cadence (StatisticsSampler::sample,
 // dsmc/statisticssampler.cpp:45-66), after collide_cells on sampled steps
 // only: every cell's fp64 moments and the y-binned profiles.  A warp takes a
-// chunk of 32 cells: their headers one per lane, then each sampled cell with
-// its members over the lanes, and at the end each lane adds its own cell's
-// moments.  Each warp counts the v_x histogram in shared memory and adds it to
-// its copy of the sums once per system (every particle lands in one of a few
-// bins: one global atomic per particle queued on those addresses).
+// chunk of 32 cells, their headers one per lane, then each sampled cell with
+// its members over the lanes.  Per cell one transposing butterfly sums the
+// six velocity moments and the cell's profile sums {v_z, 1/2 m v_z^2} in the
+// bin of its first member (members in another bin, rare when the bins are
+// no finer than the cells, add their own); lanes 4j then add slot j to the
+// cell's moment row or the profile.  Each warp counts the v_x histogram in
+// shared memory and adds it to its copy of the sums once per system (every
+// particle lands in one of a few bins: one global atomic per particle queued
+// on those addresses).
 __global__ void __launch_bounds__(32 * C_WARPS) sample_cells_kernel(const __grid_constant__ PassParams P) {
     __shared__ unsigned hist[C_WARPS][SHIST];
     const int lane = threadIdx.x & 31;
@@ -434,6 +457,11 @@ __global__ void __launch_bounds__(32 * C_WARPS) sample_cells_kernel(const __grid
             __syncwarp();
         }
     };
+    // moment row entry this lane adds: slot j of the butterfly to M[1 + j]
+    // (j < 6), lane 1 the count to M[0]; lane 12 also M[7] = the three sums
+    // of squares
+    const int slot = lane >> 2;
+    const int mcol = (lane & 3) == 0 && slot < 6 ? 1 + slot : lane == 1 ? 0 : -1;
     const int C = P.cells.num_cells;
     const int nchunks = (C + 31) >> 5;
     const int nwarps = gridDim.x * C_WARPS;
@@ -449,20 +477,26 @@ __global__ void __launch_bounds__(32 * C_WARPS) sample_cells_kernel(const __grid
             smp = g.sample_interval > 0 && step > 0 && (step % (uint32_t)g.sample_interval) == 0 &&
                   step >= (uint32_t)g.sample_begin;
         }
-        double own[6] = {0, 0, 0, 0, 0, 0};  // this lane's cell: sum v, sum v^2 per axis
         for (unsigned todo = __ballot_sync(0xffffffffu, smp); todo; todo &= todo - 1u) {
             const int c = __ffs(todo) - 1;
+            const int ac = ch * 32 + c;
             const int sys = __shfl_sync(0xffffffffu, m.w, c);
             const int cb = __shfl_sync(0xffffffffu, m.x, c), cc = __shfl_sync(0xffffffffu, m.y, c);
             const int cnb = (int)__shfl_sync(0xffffffffu, nb, c), cnt = (int)__shfl_sync(0xffffffffu, nt, c);
             const int n = cnb + cnt;
             const SysDev &g = P.sys[sys];
+            double *M = P.cells.mom + 8 * (size_t)ac;
+            const double mold = mcol >= 0 ? M[mcol] : 0.0;  // in flight with the members' loads
+            const double m7 = lane == 12 ? M[7] : 0.0;
             const bool local = g.prof_bins <= SHIST;
             if (local && sys != hsys) {
                 flush();
                 hsys = sys;
             }
-            double mo[6] = {0, 0, 0, 0, 0, 0};
+            // Σv_x Σv_y Σv_z Σv_x² Σv_y² Σv_z², then Σv_z and Σ 1/2 m v_z² in bin b0
+            double v[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            int b0 = 0;
+            unsigned in0 = 0;  // members in bin b0
             for (int q0 = 0; q0 < n; q0 += 32) {
                 const int q = q0 + lane;
                 const bool ok = q < n;
@@ -475,14 +509,22 @@ __global__ void __launch_bounds__(32 * C_WARPS) sample_cells_kernel(const __grid
                     y = b.y;
                     z = b.z;
                     bin = profile_bin(g, Split32::y_of(g, Ain[sl]));
-                    mo[0] += x;
-                    mo[1] += y;
-                    mo[2] += z;
-                    mo[3] += x * x;
-                    mo[4] += y * y;
-                    mo[5] += z * z;
+                    v[0] += x;
+                    v[1] += y;
+                    v[2] += z;
+                    v[3] += x * x;
+                    v[4] += y * y;
+                    v[5] += z * z;
                 }
-                profile_add_warp(g, ok, bin, 1.0, z, 0.5 * g.mass * z * z);
+                if (q0 == 0) b0 = __shfl_sync(0xffffffffu, bin, 0);
+                const bool here = ok && bin == b0;
+                const double e = 0.5 * g.mass * z * z;
+                if (here) {
+                    v[6] += z;
+                    v[7] += e;
+                }
+                in0 += (unsigned)__popc(__ballot_sync(0xffffffffu, here));
+                profile_add_warp(g, ok && !here, bin, 1.0, z, e);
                 if (ok) {
                     if (local) {
                         const int hb = profile_vx_bin(g, x);
@@ -492,23 +534,18 @@ __global__ void __launch_bounds__(32 * C_WARPS) sample_cells_kernel(const __grid
                     }
                 }
             }
-#pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                mo[k] = warp_sum_f64(mo[k]);
-                if (lane == c) own[k] = mo[k];
+            const double t = warp_transpose_sum8(v, lane);
+            const double sq = __shfl_sync(0xffffffffu, t, 12) + __shfl_sync(0xffffffffu, t, 16) +
+                              __shfl_sync(0xffffffffu, t, 20);
+            if (mcol >= 0) M[mcol] = mold + (mcol == 0 ? (double)n : t);
+            if (lane == 12) M[7] = m7 + sq;
+            if (in0) {
+                double *pr = profile_copy(g) + 3 * b0;
+                if (lane == 2) atomicAdd(pr, (double)in0);
+                if (lane == 24) atomicAdd(pr + 1, t);
+                if (lane == 28) atomicAdd(pr + 2, t);
             }
-        }
-        if (smp) {
-            double *M = P.cells.mom + 8 * (size_t)a;
-            M[0] += (double)(nb + nt);
-            M[1] += own[0];
-            M[2] += own[1];
-            M[3] += own[2];
-            M[4] += own[3];
-            M[5] += own[4];
-            M[6] += own[5];
-            M[7] += own[3] + own[4] + own[5];
-            if (a == P.sys[m.w].active_begin) atomicAdd(&P.tally[m.w].samples, 1ull);
+            if (lane == 0 && ac == g.active_begin) atomicAdd(&P.tally[sys].samples, 1ull);
         }
     }
     flush();

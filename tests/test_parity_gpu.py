@@ -156,7 +156,7 @@ def run_pair(case, capacity=None):
 
 @pytest.mark.parametrize("case", CASES)
 def test_fused_pass_equals_stage_calls(case):
-    """The production fused pass (bulk-copy pipelined kernel) and the four
+    """The production pass (collide, move, place and wall kernels) and the four
     stand-alone stage kernels give bit-identical trajectories."""
     A, z, meta = run_pair(case)
     B, _, _ = run_pair(case)
