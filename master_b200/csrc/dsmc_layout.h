@@ -140,6 +140,7 @@ struct Status {
     unsigned int walls;        // entries in the wall-flight list this pass (production pass)
     unsigned int nout;         // records in the outgoing list (particles that left a slab)
     unsigned int walls_taken;  // wall-flight entries claimed by place_walls' warps this pass
+    unsigned int collide_taken;  // cell chunks claimed by collide_cells' warps this pass
 };
 
 struct SpillRec {

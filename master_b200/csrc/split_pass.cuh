@@ -85,6 +85,17 @@ __device__ __forceinline__ int common_system(bool valid, int sys) {
     return __all_sync(0xffffffffu, !valid || sys == s0) ? s0 : -2;
 }
 
+// collide_cells' chunks of 32 cells go to warps from a pass-wide counter, so
+// that a warp that finishes early takes more (a chunk's cost varies with its
+// cells' collisions); place_walls' last block zeroes the counter for the next
+// pass.  (move_cells, place_movers and sample_cells keep a fixed stride: a
+// counter made them no faster or slower.)  claim_issue starts a claim (lane 0), claim_take hands its chunk to
+// every lane: issued a chunk ahead, the atomic's latency is hidden.
+__device__ __forceinline__ unsigned claim_issue(unsigned *counter, int lane) {
+    return lane == 0 ? atomicAdd(counter, 1u) : 0u;
+}
+__device__ __forceinline__ int claim_take(unsigned claimed) { return (int)__shfl_sync(0xffffffffu, claimed, 0); }
+
 // ---- collide_cells ----------------------------------------------------------
 
 constexpr int C_WARPS = 4;
@@ -182,7 +193,9 @@ __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __gri
     unsigned col = 0, cand = 0;  // this lane's counts for system tsys
     int tsys = -1;
 
-    for (int ch = blockIdx.x * C_WARPS + (threadIdx.x >> 5); ch < nchunks; ch += gridDim.x * C_WARPS) {
+    unsigned nxt = claim_issue(&P.status->collide_taken, lane);
+    for (int ch = claim_take(nxt); ch < nchunks; ch = claim_take(nxt)) {
+        nxt = claim_issue(&P.status->collide_taken, lane);  // the next chunk, in flight meanwhile
         const int first = ch * 32;
         const bool mine = lane < C - first;
         const int a = first + lane;
@@ -1300,6 +1313,7 @@ __global__ void __launch_bounds__(32 * W_WARPS) place_walls_kernel(const __grid_
                 atomicExch(&P.status->halted, 1u);
             atomicExch(&P.status->walls, 0u);
             atomicExch(&P.status->walls_taken, 0u);
+            atomicExch(&P.status->collide_taken, 0u);
             atomicExch(&P.status->blocks_done, 0u);
         }
     }
