@@ -32,6 +32,7 @@ CUDA_SOURCES = {
     # the reference's fp64 arithmetic: no fused multiply-add
     "kernels_fp64.cu": ["-fmad=false"],
     "api.cu": [],
+    "cell_layout.cu": [],
     # must round exactly as the CPU geometry path
     "geometry_gpu.cu": ["-fmad=false"],
 }

@@ -56,6 +56,7 @@ struct SysHost {
     int active_begin = 0, active_end = 0;
     std::vector<int> cell_global;     // per active cell
     std::vector<int> pixels, total_pixels;
+    double pixel_sum = 0;             // free voxels over the active cells
     std::vector<double> volume_cell, coeff;
     std::vector<int> cell_map;        // global -> local active index
     DevBuf<uint8_t> vox;
@@ -108,7 +109,9 @@ struct dsmc_ctx {
     DevBuf<unsigned> bot[3], top[3], key;  // occupancy sets, rotating per re-binning pass
     DevBuf<int2> room;                      // per cell: top-slot room of the pass in flight
     DevBuf<double> mom;
-    std::vector<int4> h_meta;   // {base, cap, global, sys}
+    DevBuf<int> pix;                 // per cell: free voxels (the capacity's expected share)
+    DevBuf<double2> cap_np;          // per system: {particles, free voxels} at the last layout
+    DevBuf<unsigned long long> cap_bsum, cap_out;  // layout scan: block sums; {total slots, largest capacity}
     size_t slots = 0;
     int smem_cap = 32;
     // particles
@@ -139,6 +142,10 @@ struct dsmc_ctx {
     // per-kernel timers of the production pass (dsmc_ctx_set_timing)
     bool timing = false;
     cudaEvent_t tev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    // dsmc_particles_get: positions are copied out on io_stream while the
+    // velocities are converted on `stream`
+    cudaStream_t io_stream = nullptr;
+    cudaEvent_t io_event = nullptr;
     double tms[4] = {0, 0, 0, 0};
     long long tpasses = 0;
     double cap_factor = 2.0;
@@ -229,30 +236,25 @@ Status read_status(dsmc_ctx *ctx, cudaError_t *err) {
 int relayout(dsmc_ctx *ctx, long long total) {
     ctx->drop_graphs();  // slot buffers and grids may change
     const int C = ctx->num_cells;
-    std::vector<unsigned> counts(C);
-    if (C) CK(cudaMemcpyAsync(counts.data(), ctx->hist.p, C * sizeof(unsigned), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
     // Capacity per cell: twice the larger of the expected and the present
-    // occupancy plus 24 slots, a multiple of 4 (Poisson tails beyond it are
-    // below 1e-12 per cell and step; an overflow spills and the host repacks).
-    size_t slots = 0;
-    unsigned maxcap = 4;
-    for (auto &sp : ctx->systems) {
-        SysHost &s = *sp;
-        double total_pixels = 0;
-        for (int p : s.pixels) total_pixels += p;
-        const double nsys = (double)s.num_particles;
-        for (int a = s.active_begin; a < s.active_end; ++a) {
-            const double expect = total_pixels > 0 ? nsys * s.pixels[a - s.active_begin] / total_pixels : 0;
-            const double want = std::max(expect, (double)counts[a]);
-            unsigned cap = (unsigned)std::ceil(ctx->cap_factor * want + ctx->cap_pad);
-            if (cap < 1) cap = 1;
-            ctx->h_meta[a].x = (int)slots;
-            ctx->h_meta[a].y = (int)cap;
-            slots += cap;
-            maxcap = std::max(maxcap, cap);
-        }
-    }
+    // occupancy plus 24 slots by default (Poisson tails beyond it are below
+    // 1e-12 per cell and step; an overflow spills and the host repacks).
+    // Computed on the device with the cells' first slots (cell_layout.cu).
+    const size_t S = std::max<size_t>(ctx->systems.size(), 1);
+    std::vector<double2> np(S, double2{0.0, 0.0});
+    for (size_t q = 0; q < ctx->systems.size(); ++q)
+        np[q] = double2{(double)ctx->systems[q]->num_particles, ctx->systems[q]->pixel_sum};
+    CK(ctx->cap_np.ensure(S));
+    CK(ctx->cap_bsum.ensure(std::max(cell_layout_blocks(C), 1)));
+    CK(ctx->cap_out.ensure(2));
+    CK(cudaMemcpyAsync(ctx->cap_np.p, np.data(), S * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+    CK(launch_cell_layout(ctx->meta.p, ctx->pix.p, ctx->hist.p, ctx->cap_np.p, ctx->cap_factor, (double)ctx->cap_pad, C,
+                          ctx->cap_bsum.p, ctx->cap_out.p, ctx->stream));
+    unsigned long long lay[2] = {0, 0};
+    CK(cudaMemcpyAsync(lay, ctx->cap_out.p, sizeof(lay), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const size_t slots = (size_t)lay[0];
+    const unsigned maxcap = (unsigned)std::max<unsigned long long>(4, lay[1]);
     if (slots >= (size_t)0x7fffffffu) return fail(ctx, DSMC_ERR_CAPACITY, "more than 2^31 particle slots");
     if (maxcap > 4096) return fail(ctx, DSMC_ERR_CAPACITY, "a cell needs more than 4096 slots");
     ctx->smem_cap = (int)((maxcap + 31u) & ~31u);
@@ -264,9 +266,7 @@ int relayout(dsmc_ctx *ctx, long long total) {
     CK(ctx->B1.ensure_grow(slots * half));
     CK(ctx->key.ensure_grow(slots));
     CK(ctx->walls.ensure_grow(std::max<size_t>(slots, 1)));
-    CK(ctx->meta.ensure(std::max(C, 1)));
     if (C) {
-        CK(cudaMemcpyAsync(ctx->meta.p, ctx->h_meta.data(), C * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
         for (int q = 0; q < 3; ++q) {
             CK(cudaMemsetAsync(ctx->bot[q].p, 0, C * sizeof(unsigned), ctx->stream));
             CK(cudaMemsetAsync(ctx->top[q].p, 0, C * sizeof(unsigned), ctx->stream));
@@ -377,7 +377,7 @@ cudaError_t launch_fused_graph(dsmc_ctx *ctx, const PassParams &P) {
     return cudaGraphLaunch(it->second, ctx->stream);
 }
 
-int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, int advance) {
+PassParams pass_params(dsmc_ctx *ctx, int do_collide, int do_move, int do_sample, int advance) {
     PassParams P;
     P.sys = ctx->sys_dev.p;
     P.tally = ctx->tally.p;
@@ -394,6 +394,11 @@ int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, 
     P.do_sample = do_sample;
     P.smem_cap = ctx->smem_cap;
     P.advance_step = advance;
+    return P;
+}
+
+int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, int advance) {
+    PassParams P = pass_params(ctx, do_collide, do_move, do_sample, advance);
     cudaError_t e;
     if (mode == PASS_FUSED && ctx->use_pipelined && ctx->fused_grids[1] > 0) {
         P.top_only = 0;
@@ -469,8 +474,19 @@ int settle(dsmc_ctx *ctx, unsigned step_before, int cur_before, int cphase_befor
 
 int flush_pending(dsmc_ctx *ctx) {
     if (!ctx->pending) return DSMC_OK;
-    int rc = launch(ctx, PASS_INPLACE, 1, 0, 1, 0);
-    if (rc) return rc;
+    if (!is_fp64(ctx) && ctx->use_pipelined && ctx->fused_grids[1] > 0) {
+        // the production pass's own collide (and, on a sampled step, sampler)
+        // kernels, in place: the pending step is the device's step counter
+        cudaError_t e;
+        const Status st = read_status(ctx, &e);
+        CK(e);
+        PassParams P = pass_params(ctx, 1, 0, samples_at(ctx, st.step) ? 1 : 0, 0);
+        P.top_only = 0;
+        CK(split32::launch_collide(P, ctx->fused_grids, ctx->stream));
+    } else {
+        int rc = launch(ctx, PASS_INPLACE, 1, 0, 1, 0);
+        if (rc) return rc;
+    }
     ctx->pending = false;
     return DSMC_OK;
 }
@@ -494,15 +510,19 @@ int rebuild_cells(dsmc_ctx *ctx) {
     // Concatenate the active cells of all systems.
     int C = 0;
     for (auto &s : ctx->systems) C += (int)s->cell_global.size();
-    ctx->h_meta.assign(C, int4{0, 0, 0, 0});
+    std::vector<int4> h_meta(C, int4{0, 0, 0, 0});  // {base, cap: set by each layout; global, sys}
+    std::vector<int> pix(C);
     std::vector<double4> state(C);
     int a = 0;
     for (size_t si = 0; si < ctx->systems.size(); ++si) {
         SysHost &s = *ctx->systems[si];
         s.active_begin = a;
+        s.pixel_sum = 0;
         for (size_t c = 0; c < s.cell_global.size(); ++c, ++a) {
-            ctx->h_meta[a].z = s.cell_global[c];
-            ctx->h_meta[a].w = (int)si;
+            h_meta[a].z = s.cell_global[c];
+            h_meta[a].w = (int)si;
+            pix[a] = s.pixels[c];
+            s.pixel_sum += s.pixels[c];
             // Cell::vr_max starts at 3*sqrt(T) (dsmc/system.cpp:451,477)
             state[a] = double4{s.vr_max0, 0.0, s.coeff[c], 0.0};
         }
@@ -521,6 +541,7 @@ int rebuild_cells(dsmc_ctx *ctx) {
     ctx->num_cells = C;
     const size_t Cn = std::max(C, 1);
     CK(ctx->meta.alloc(Cn));
+    CK(ctx->pix.alloc(Cn));
     CK(ctx->state.alloc(Cn));
     for (int q = 0; q < 3; ++q) {
         CK(ctx->bot[q].alloc(Cn));
@@ -532,6 +553,8 @@ int rebuild_cells(dsmc_ctx *ctx) {
     if (C) {
         if (C_old > 0 && C_old <= C)
             for (int q = 0; q < C_old; ++q) state[q] = old_state[q];
+        CK(cudaMemcpyAsync(ctx->meta.p, h_meta.data(), C * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->pix.p, pix.data(), C * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaMemcpyAsync(ctx->state.p, state.data(), C * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
         CK(cudaMemsetAsync(ctx->mom.p, 0, 8 * C * sizeof(double), ctx->stream));
         for (int q = 0; q < 3; ++q) {
@@ -590,6 +613,8 @@ void dsmc_ctx_destroy(dsmc_ctx *ctx) {
     ctx->drop_graphs();
     for (cudaEvent_t &e : ctx->tev)
         if (e) cudaEventDestroy(e);
+    if (ctx->io_event) cudaEventDestroy(ctx->io_event);
+    if (ctx->io_stream) cudaStreamDestroy(ctx->io_stream);
     cudaStream_t s = ctx->stream;
     delete ctx;
     cudaStreamDestroy(s);
@@ -1201,18 +1226,36 @@ int dsmc_particles_get(dsmc_ctx *ctx, int sys_id, int64_t cap, double *r, double
     CK(ctx->io_cell.ensure(std::max<long long>(N, 1)));
     if (N == 0) return DSMC_OK;
     if (h.slab) CK(cudaMemsetAsync(ctx->io_cell.p, 0xff, N * sizeof(int), ctx->stream));
-    cudaError_t e = is_fp64(ctx)
-                        ? fp64::launch_to_fp64(ctx->sys_dev.p, sys_id, cell_arrays(ctx), particle_arrays(ctx), ctx->cur,
-                                               ctx->cphase, 0, N, ctx->io_r.p, ctx->io_v.p, ctx->io_cell.p, &ctx->status.p->error,
-                                               ctx->stream)
-                        : split32::launch_to_fp64(ctx->sys_dev.p, sys_id, cell_arrays(ctx), particle_arrays(ctx),
-                                                  ctx->cur, ctx->cphase, 0, N, ctx->io_r.p, ctx->io_v.p, ctx->io_cell.p,
-                                                  &ctx->status.p->error, ctx->stream);
+    if (!ctx->io_stream) {
+        CK(cudaStreamCreateWithFlags(&ctx->io_stream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->io_event, cudaEventDisableTiming));
+    }
+    // Each record's values go to its id's place, a scatter: the positions
+    // (and cells) first, copied out on io_stream while the velocities are
+    // converted, so that one conversion overlaps the other's copy.
+    auto to_fp64 = [&](double *ro, double *vo, int *co) {
+        return is_fp64(ctx) ? fp64::launch_to_fp64(ctx->sys_dev.p, sys_id, cell_arrays(ctx), particle_arrays(ctx),
+                                                   ctx->cur, ctx->cphase, 0, N, ro, vo, co, &ctx->status.p->error,
+                                                   ctx->stream)
+                            : split32::launch_to_fp64(ctx->sys_dev.p, sys_id, cell_arrays(ctx), particle_arrays(ctx),
+                                                      ctx->cur, ctx->cphase, 0, N, ro, vo, co, &ctx->status.p->error,
+                                                      ctx->stream);
+    };
+    CK(to_fp64(ctx->io_r.p, nullptr, ctx->io_cell.p));
+    CK(cudaEventRecord(ctx->io_event, ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->io_stream, ctx->io_event, 0));
+    cudaError_t e = cudaMemcpyAsync(r, ctx->io_r.p, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->io_stream);
+    if (e == cudaSuccess && cell)
+        e = cudaMemcpyAsync(cell, ctx->io_cell.p, N * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->io_stream);
+    if (e == cudaSuccess) e = to_fp64(nullptr, ctx->io_v.p, nullptr);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(v, ctx->io_v.p, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream);
+    // both streams are done with the caller's buffers before this returns
+    const cudaError_t e1 = cudaStreamSynchronize(ctx->io_stream);
+    const cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
     CK(e);
-    CK(cudaMemcpyAsync(r, ctx->io_r.p, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaMemcpyAsync(v, ctx->io_v.p, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    if (cell) CK(cudaMemcpyAsync(cell, ctx->io_cell.p, N * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK(e1);
+    CK(e2);
     return DSMC_OK;
 }
 
@@ -1521,6 +1564,8 @@ int dsmc_cells_get(dsmc_ctx *ctx, int sys_id, int cap, int32_t *global_index, in
                            ctx->stream));
     }
     std::vector<double4> st(C);
+    std::vector<int4> mt(count ? C : 0);
+    if (count) CK(cudaMemcpyAsync(mt.data(), ctx->meta.p + a0, C * sizeof(int4), cudaMemcpyDeviceToHost, ctx->stream));
     if (vr_max || rest)
         CK(cudaMemcpyAsync(st.data(), ctx->state.p + a0, C * sizeof(double4), cudaMemcpyDeviceToHost, ctx->stream));
     if (moments)
@@ -1531,7 +1576,7 @@ int dsmc_cells_get(dsmc_ctx *ctx, int sys_id, int cap, int32_t *global_index, in
         if (vr_max) vr_max[q] = st[q].x;
         if (rest) rest[q] = st[q].y;
         if (count) {
-            const unsigned cap = (unsigned)ctx->h_meta[a0 + q].y;
+            const unsigned cap = (unsigned)mt[q].y;
             const unsigned b = std::min(nb[q], cap);
             count[q] = (int32_t)(b + std::min(nt[q], cap - b));
         }

@@ -46,11 +46,23 @@ int fused_grids(int smem_cap, int num_sms, int grids[5]);
 // ev: null, or five events recorded before each kernel and after the last
 // (the sampler, on sampled steps, falls in the collide interval)
 cudaError_t launch_fused(const PassParams &P, const int grids[5], cudaStream_t st, cudaEvent_t *ev = nullptr);
+// collide_cells (and sample_cells when P.do_sample) alone, in place: the
+// collide of a step whose move has not started
+cudaError_t launch_collide(const PassParams &P, const int grids[5], cudaStream_t st);
 // Records from another slab into system s's cells (occupancy set cin of buffer
 // cur): top segments, or the overflow list when a cell is full.
 cudaError_t launch_put(const SysDev *sys, int s, const CellArrays &cells, const ParticleArrays &parts, int cur, int cin,
                        long long n, const uint4 *rec, Status *status, cudaStream_t st);
 }  // namespace split32
+
+// Slot layout of the cells (cell_layout.cu): meta[a].y = capacity of cell a
+// from its free voxels pix[a], its present occupancy and np[system] =
+// {particles, free voxels of the system}; meta[a].x = its first slot (the
+// capacities of the cells before it).  out = {total slots, largest capacity};
+// bsum holds cell_layout_blocks(C) entries.
+int cell_layout_blocks(int C);
+cudaError_t launch_cell_layout(int4 *meta, const int *pix, const unsigned *present, const double2 *np, double factor,
+                               double pad, int C, unsigned long long *bsum, unsigned long long *out, cudaStream_t st);
 
 // Pass modes (engine.cuh PassMode).
 enum { PASS_FUSED = 0, PASS_INPLACE = 1, PASS_SORT = 2 };

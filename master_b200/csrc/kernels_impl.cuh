@@ -175,7 +175,8 @@ __global__ void k_insert(const CellArrays cells, const ParticleArrays parts, int
     }
 }
 
-// Slots of one system -> fp64 state ordered by id (dsmc/dsmc_io.cpp:98-113 layout).
+// Slots of one system -> fp64 state ordered by id (dsmc/dsmc_io.cpp:98-113
+// layout); r, v and cell may each be null (not written).
 __global__ void k_to_fp64(const SysDev *sys, int s, const CellArrays cells, const ParticleArrays parts, int cur,
                           int cin, uint32_t id_base, long long cap, double *r, double *v, int *cell, unsigned *err) {
     const SysDev &g = sys[s];
@@ -197,12 +198,13 @@ __global__ void k_to_fp64(const SysDev *sys, int s, const CellArrays cells, cons
                 atomicOr(err, DSMC_EBIT_CELL);
                 continue;
             }
-            double rr[3];
-            Maker<Prec>::position(g, p, rr);
-            for (int d = 0; d < 3; ++d) {
-                r[3 * i + d] = rr[d];
-                v[3 * i + d] = (double)p.v[d];
+            if (r) {
+                double rr[3];
+                Maker<Prec>::position(g, p, rr);
+                for (int d = 0; d < 3; ++d) r[3 * i + d] = rr[d];
             }
+            if (v)
+                for (int d = 0; d < 3; ++d) v[3 * i + d] = (double)p.v[d];
             if (cell) cell[i] = m.z;
         }
     }

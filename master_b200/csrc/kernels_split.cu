@@ -108,6 +108,20 @@ cudaError_t launch_fused(const PassParams &P, const int grids[5], cudaStream_t s
     return e;
 }
 
+cudaError_t launch_collide(const PassParams &P, const int grids[5], cudaStream_t st) {
+    pass3::collide_cells_kernel<<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (P.do_sample) {
+        pass3::sample_cells_kernel<<<grids[4], 32 * pass3::C_WARPS, 0, st>>>(P);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    // place_walls, whose last block zeroes collide_cells' chunk counter at the
+    // end of a full pass, does not run here
+    return cudaMemsetAsync(&P.status->collide_taken, 0, sizeof(unsigned), st);
+}
+
 cudaError_t launch_put(const SysDev *sys, int s, const CellArrays &cells, const ParticleArrays &parts, int cur, int cin,
                        long long n, const uint4 *rec, Status *status, cudaStream_t st) {
     if (n <= 0) return cudaSuccess;
