@@ -127,6 +127,10 @@ struct dsmc_ctx {
     bool sorted = false;      // every bottom segment is sorted by id (a production pass ran last)
     bool pending = false;     // the last step's collide/sample has not run yet
     bool keys_valid = false;  // a stand-alone move stage left new cell keys
+    // the device step counter as the last settle read it, while no pass and
+    // no host write has touched it since (dsmc_step then skips its read)
+    bool step_known = false;
+    unsigned known_step = 0;
     // staging
     DevBuf<unsigned char> fA, fB;
     DevBuf<int> fkey;
@@ -398,6 +402,7 @@ PassParams pass_params(dsmc_ctx *ctx, int do_collide, int do_move, int do_sample
 }
 
 int launch(dsmc_ctx *ctx, int mode, int do_collide, int do_move, int do_sample, int advance) {
+    ctx->step_known = false;
     PassParams P = pass_params(ctx, do_collide, do_move, do_sample, advance);
     cudaError_t e;
     if (mode == PASS_FUSED && ctx->use_pipelined && ctx->fused_grids[1] > 0) {
@@ -467,8 +472,11 @@ int settle(dsmc_ctx *ctx, unsigned step_before, int cur_before, int cphase_befor
         long long staged = 0;
         int rc = stage_present(ctx, 0, -1, &staged);
         if (rc) return rc;
-        return relayout(ctx, staged);
+        rc = relayout(ctx, staged);  // leaves the step counter as it is
+        if (rc) return rc;
     }
+    ctx->step_known = true;
+    ctx->known_step = st.step;
     return DSMC_OK;
 }
 
@@ -1014,6 +1022,7 @@ int dsmc_continue_from(dsmc_ctx *ctx, int sys_id, double t, uint64_t steps, uint
     T.wall_hits = wall_collisions;
     CK(cudaMemcpyAsync(ctx->tally.p + sys_id, &T, sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
     const unsigned st = (unsigned)steps;
+    ctx->step_known = false;
     CK(cudaMemcpyAsync(&ctx->status.p->step, &st, sizeof(st), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     h.t0_reduced = t;
@@ -1196,6 +1205,7 @@ int dsmc_checkpoint_load(dsmc_ctx *ctx, const char *path) {
     for (int s = 0; s < S; ++s)  // the saved sums into the first copy
         CK(cudaMemcpyAsync(ctx->systems[s]->prof.p, prof[s].data(), prof[s].size() * sizeof(double),
                            cudaMemcpyHostToDevice, ctx->stream));
+    ctx->step_known = false;
     CK(cudaMemcpyAsync(&ctx->status.p->step, &hd.step, sizeof(unsigned), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return DSMC_OK;
@@ -1271,10 +1281,13 @@ int dsmc_step(dsmc_ctx *ctx, int nsteps) {
     ctx->keys_valid = false;
     int left = nsteps;
     while (left > 0) {
-        cudaError_t e;
-        Status st = read_status(ctx, &e);
-        CK(e);
-        const unsigned step0 = st.step;
+        unsigned step0 = ctx->known_step;
+        if (!ctx->step_known) {
+            cudaError_t e;
+            const Status st = read_status(ctx, &e);
+            CK(e);
+            step0 = st.step;
+        }
         const int cur0 = ctx->cur;
         const int cphase0 = ctx->cphase;
         const bool pending0 = ctx->pending;

@@ -124,3 +124,28 @@ def test_graph_replay_equals_plain_launches():
     assert np.array_equal(ra, rb) and np.array_equal(va, vb) and np.array_equal(ca, cb)
     assert A.tallies().collisions == B.tallies().collisions
     assert B.ctx.pass_times()["passes"] > 0
+
+
+@pytest.mark.parametrize("capacity", [None, (1.5, 3), (1.0, 0)])
+def test_device_layout_follows_the_capacity_rule(capacity):
+    """Cell capacities are computed on the device whenever the buffers are
+    laid out: ceil(factor * max(expected, present) + pad) per active cell,
+    expected = particles * free voxels of the cell / free voxels of the
+    system (rounded without fused multiply-add), and the slots total their
+    sum.  The counts come back through the device table as well."""
+    from master_b200.system import cells_layout
+    z, meta, s, g = load_case("small_dt5")
+    S = System(s, g, init_particles=False)
+    factor, pad = capacity or (2.0, 24)
+    if capacity:
+        S.ctx.check(S.ctx.lib.dsmc_ctx_set_capacity(S.ctx.handle, factor, pad))
+    S.set_particles(z["r0"], z["v0"])
+    cells = S.cells()
+    lay = cells_layout(s, g)
+    assert np.array_equal(cells["global_index"], lay["global_index"])
+    present = cells["count"].astype(np.float64)
+    assert present.sum() == z["r0"].shape[0]
+    pix = lay["pixels"].astype(np.float64)
+    expect = (z["r0"].shape[0] * pix) / pix.sum()
+    cap = np.maximum(np.ceil(factor * np.maximum(expect, present) + pad), 1.0)
+    assert S.info().slots == int(cap.sum())
