@@ -770,8 +770,11 @@ __device__ __forceinline__ void place_pair(const FlightConst &fc, const MoveSmem
     }
 }
 
+// At most 128 registers (four blocks per SM): the compiler then keeps both
+// cells of a pair in flight; left to itself it may pick 96 and five blocks,
+// which measured slower.
 template <int R>
-__global__ void __launch_bounds__(32 * M_WARPS) move_cells_kernel(const __grid_constant__ PassParams P) {
+__global__ void __launch_bounds__(32 * M_WARPS, 4) move_cells_kernel(const __grid_constant__ PassParams P) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     typedef Split32::Particle Particle;
     const int lane = threadIdx.x & 31;
