@@ -1159,7 +1159,7 @@ __device__ __forceinline__ void flush_walls(const PassParams &P, PlaceSmem &W) {
     __syncwarp();
 }
 
-__global__ void __launch_bounds__(32 * P_WARPS, 8) place_movers_kernel(const __grid_constant__ PassParams P) {
+__global__ void __launch_bounds__(32 * P_WARPS, 5) place_movers_kernel(const __grid_constant__ PassParams P) {
     __shared__ PlaceSmem smem[P_WARPS];
     const int lane = threadIdx.x & 31;
     const volatile Status *vs = P.status;
