@@ -804,6 +804,7 @@ static int system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32
         const double sd = std::sqrt(temperature / s->mass);
         d.vx_min = -4 * sd;
         d.vx_bin = (4 * sd - d.vx_min) / h->prof_bins;
+        d.vx_inv_bin = 1.0 / d.vx_bin;
     }
 
     if (slab) {

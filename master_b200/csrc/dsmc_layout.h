@@ -113,7 +113,7 @@ struct SysDev {
     // copy the atomics queue on those few addresses); the host adds them up
     double *prof;
     int prof_bins, prof_copies;
-    double mass, vx_min, vx_bin;
+    double mass, vx_min, vx_bin, vx_inv_bin;
 };
 
 #define DSMC_WALL_THERMAL 0    // diffuse reflection at the wall temperature

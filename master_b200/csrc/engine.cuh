@@ -151,8 +151,15 @@ __device__ __forceinline__ void profile_add_warp(const SysDev &g, bool valid, in
 
 // MeasureVelocityDistribution::update (dsmc/statisticalproperty.cpp:441-458):
 // bin int((v_x - v_min) / width), truncated toward zero, counted when in range.
+// The quotient is taken by the reciprocal (within 4.4e-16 of the divided one,
+// relatively) unless it lies within 1e-9 of an integer or beyond 1e6, where
+// the division itself decides: the bin is the one the division gives.
 __device__ __forceinline__ int profile_vx_bin(const SysDev &g, double vx) {
-    const int b = (int)((vx - g.vx_min) / g.vx_bin);
+    const double d = vx - g.vx_min;
+    double q = d * g.vx_inv_bin;
+    const double f = q - floor(q);
+    if (f < 1e-9 || f > 1.0 - 1e-9 || fabs(q) > 1e6) q = d / g.vx_bin;
+    const int b = (int)q;
     return b >= 0 && b < g.prof_bins ? b : -1;
 }
 __device__ __forceinline__ void profile_vx(const SysDev &g, double vx) {
