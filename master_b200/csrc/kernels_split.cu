@@ -63,7 +63,8 @@ int fused_grids(int smem_cap, int num_sms, int grids[5]) {
         DSMC_MOVE_RINGS(X)
 #undef X
     }
-    const int bc = static_blocks(pass3::collide_cells_kernel, 32 * pass3::C_WARPS);
+    const int bc = std::min(static_blocks(pass3::collide_cells_kernel<false>, 32 * pass3::C_WARPS),
+                            static_blocks(pass3::collide_cells_kernel<true>, 32 * pass3::C_WARPS));
     const int bp = static_blocks(pass3::place_movers_kernel, 32 * pass3::P_WARPS);
     const int bw = static_blocks(pass3::place_walls_kernel, 32 * pass3::W_WARPS);
     const int bs = static_blocks(pass3::sample_cells_kernel, 32 * pass3::C_WARPS);
@@ -76,10 +77,19 @@ int fused_grids(int smem_cap, int num_sms, int grids[5]) {
     return 1;
 }
 
+// collide_cells with the chunk counter when each warp has many chunks
+static void launch_collide_cells(const PassParams &P, int grid, cudaStream_t st) {
+    const long long nchunks = (P.cells.num_cells + 31) / 32;
+    if (nchunks >= (long long)pass3::CLAIM_MIN_CHUNKS_PER_WARP * grid * pass3::C_WARPS)
+        pass3::collide_cells_kernel<true><<<grid, 32 * pass3::C_WARPS, 0, st>>>(P);
+    else
+        pass3::collide_cells_kernel<false><<<grid, 32 * pass3::C_WARPS, 0, st>>>(P);
+}
+
 cudaError_t launch_fused(const PassParams &P, const int grids[5], cudaStream_t st, cudaEvent_t *ev) {
     if (ev) cudaEventRecord(ev[0], st);
     if (P.do_collide || P.do_sample) {
-        pass3::collide_cells_kernel<<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
+        launch_collide_cells(P, grids[0], st);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         if (P.do_sample) {  // sampled steps only: the host knows the cadence
@@ -109,7 +119,7 @@ cudaError_t launch_fused(const PassParams &P, const int grids[5], cudaStream_t s
 }
 
 cudaError_t launch_collide(const PassParams &P, const int grids[5], cudaStream_t st) {
-    pass3::collide_cells_kernel<<<grids[0], 32 * pass3::C_WARPS, 0, st>>>(P);
+    launch_collide_cells(P, grids[0], st);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (P.do_sample) {

@@ -85,12 +85,15 @@ __device__ __forceinline__ int common_system(bool valid, int sys) {
     return __all_sync(0xffffffffu, !valid || sys == s0) ? s0 : -2;
 }
 
-// collide_cells' chunks of 32 cells go to warps from a pass-wide counter, so
-// that a warp that finishes early takes more (a chunk's cost varies with its
-// cells' collisions); place_walls' last block zeroes the counter for the next
-// pass.  (move_cells, place_movers and sample_cells keep a fixed stride: a
-// counter made them no faster or slower.)  claim_issue starts a claim (lane 0), claim_take hands its chunk to
-// every lane: issued a chunk ahead, the atomic's latency is hidden.
+// collide_cells' chunks of 32 cells beyond each warp's first go to warps from
+// a pass-wide counter when there are many per warp, so that a warp that
+// finishes early takes more (a chunk's cost varies with its cells'
+// collisions); place_walls' last block zeroes the counter for the next pass.
+// Four chunks per warp or more take the counter.  (move_cells, place_movers
+// and sample_cells keep a fixed stride: a counter made them no faster or
+// slower.)  claim_issue starts a claim (lane 0), claim_take hands its chunk
+// to every lane: issued a chunk ahead, the atomic's latency is hidden.
+constexpr int CLAIM_MIN_CHUNKS_PER_WARP = 4;
 __device__ __forceinline__ unsigned claim_issue(unsigned *counter, int lane) {
     return lane == 0 ? atomicAdd(counter, 1u) : 0u;
 }
@@ -179,6 +182,10 @@ __device__ __forceinline__ void publish_collide(const PassParams &P, int sys, un
     }
 }
 
+// CLAIM: chunks beyond each warp's first come from the counter (chosen by
+// the launcher when there are many chunks per warp; a fixed stride measured
+// faster with few: packed_64 and packed_128).
+template <bool CLAIM>
 __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __grid_constant__ PassParams P) {
     __shared__ CollideSmem smem[C_WARPS];
     const int lane = threadIdx.x & 31;
@@ -193,9 +200,13 @@ __global__ void __launch_bounds__(32 * C_WARPS) collide_cells_kernel(const __gri
     unsigned col = 0, cand = 0;  // this lane's counts for system tsys
     int tsys = -1;
 
-    unsigned nxt = claim_issue(&P.status->collide_taken, lane);
-    for (int ch = claim_take(nxt); ch < nchunks; ch = claim_take(nxt)) {
-        nxt = claim_issue(&P.status->collide_taken, lane);  // the next chunk, in flight meanwhile
+    // A warp's first chunk is its index; with CLAIM the later ones come from
+    // the counter, each claimed while the chunk before is in work.
+    const int nw = gridDim.x * C_WARPS;
+    unsigned nxt = 0;
+    for (int ch = blockIdx.x * C_WARPS + (threadIdx.x >> 5); ch < nchunks;
+         ch = CLAIM ? nw + claim_take(nxt) : ch + nw) {
+        if (CLAIM) nxt = claim_issue(&P.status->collide_taken, lane);  // the next chunk, in flight meanwhile
         const int first = ch * 32;
         const bool mine = lane < C - first;
         const int a = first + lane;
