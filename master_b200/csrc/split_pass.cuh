@@ -1,15 +1,18 @@
-// The production timestep pass for split-precision state: three kernels per
-// step over the active cells, which the previous pass left sorted by cell
-// (bottom segment + top segment of each cell's slots, counts in the `cin`
-// occupancy set).
+// The production timestep pass for split-precision state: four kernels per
+// step (five on sampled steps) over the active cells, which the previous pass
+// left sorted by cell (bottom segment + top segment of each cell's slots,
+// counts in the `cin` occupancy set).
 //
 //   collide_cells  Cell::prepare + Cell::collide (dsmc/cell.cpp:42-111) of
-//                  every cell, and the sampling on the reference's cadence.
+//                  every cell.
 //                  Per chunk of 32 consecutive cells lane i selects for cell
 //                  i; the warp ranks each colliding cell's particles by id
 //                  (the reference's member order) into shared memory, then
 //                  every lane runs the candidate loop of its own cell.
 //                  Velocities are updated in place in the input buffer.
+//   sample_cells   On sampled steps only (the reference's cadence,
+//                  dsmc/statisticssampler.cpp:45-66): every cell's fp64
+//                  moments and the y-binned profiles.
 //   move_cells     System::accelerate + the mover's first flight
 //                  (dsmc/system.cpp:133-144, dsmc/moleculemover.cpp:50-126)
 //                  for every particle.  A particle that stays inside its
@@ -22,7 +25,8 @@
 //   place_movers   A mover whose flight ends in an empty voxel completes it
 //                  and takes a top slot of its new cell (warp-aggregated
 //                  atomics; the spill list when the cell is full).  Flights
-//                  that meet a wall go to a list of (slot, system) pairs.
+//                  that meet a wall go to a list of (slot, source cell)
+//                  pairs.
 //   place_walls    The general mover (bisection, facet, diffuse wall) for
 //                  the listed flights, then the same placement.  The last
 //                  block ends the pass (step counter, halting).
