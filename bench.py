@@ -12,14 +12,18 @@ geometry from the reference's own generator semantics).  Multi-GPU runs are
 independent replicas (different draw seeds), one per rank: weak scaling.
 
 --impl reference runs the reference's own CPU solver (oracle/_ref/dsmc_ref,
-built from the reference sources) on a bounded sample of the same workload
-on the host cores, rank 0 only.
+built from the reference sources) on the same workload, its world written by
+the reference's own geometry tool, as single-rank replicas on the host cores
+(rank 0 only), each timing a bounded number of timesteps (--ref-steps).  It
+imports nothing of the B200 library.  A second leg times the 64^3 sample of
+the workload that the GPU arm's cpu_baseline also runs.
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -128,50 +132,119 @@ def barrier(pg):
     ensemble.barrier(pg)
 
 
-def cpu_reference(steps: int, replicas: int | None = None):
-    """The reference's own CPU solver on the bounded sample of the workload."""
+def _host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_reference_sample(steps: int, replicas: int | None = None):
+    """The reference's own CPU solver on the bounded 64^3 sample of the
+    workload (same voxel size, sphere radius, porosity, gas and simulator
+    weight), its world written by the reference's own geometry tool."""
     from oracle import run_reference
-    from master_b200 import workloads
-    w = workloads.PACKED_256_SAMPLE
-    s = w.settings(statistics_interval=100)
-    g = w.geometry()
-    cores = replicas or max(1, min(os.cpu_count() or 1, 32))
-    res = run_reference.run_replicas(s, g, timesteps=steps, replicas=cores)
+    w = run_reference.PACKED_256_SAMPLE
+    cores = replicas or max(1, min(_host_cores(), 32))
+    res = run_reference.run_replicas(w.settings(statistics_interval=100), w.geometry(), timesteps=steps,
+                                     replicas=cores)
     mol = res["reports"][0].get("molecules")
     return {
         "value": res["particle_steps_per_s"], "unit": UNIT, "cores": cores, "kind": "reference",
-        "particles_per_replica": mol,
+        "particles_per_replica": mol, "workload": w.name, "steps": steps,
         "sample": (f"{cores} independent single-rank runs of the reference solver (oracle/_ref/dsmc_ref, g++ -O3) on "
                    f"a 64^3 box of the same voxel size, sphere radius, porosity, gas and simulator weight "
-                   f"({mol} particles each), {steps} timesteps; its own stage timers (moving+colliding+"
-                   f"accelerating+sampling)"),
+                   f"({mol} particles each; world from the reference's geometry tool), {steps} timesteps; its own "
+                   f"stage timers (moving+colliding+accelerating+sampling)"),
+    }
+
+
+def cpu_reference_full(workload: str, steps: int):
+    """The reference's own CPU solver on the benchmark workload itself: the
+    world written by the reference's geometry tool (a single-rank world file
+    with its 27x periodic halo, 16.8 GB at 256^3), then as many single-rank
+    replicas as the host cores and 70 % of the available host memory hold
+    (about 23 GB each at 256^3), each timing `steps` timesteps with its own
+    stage timers.  Setup (geometry tool, world read, particle creation) is
+    outside the timers, as in the reference's report."""
+    from oracle import run_reference
+    w = run_reference.WORKLOADS[workload]
+    g = w.geometry()
+    need = g.world_bytes()
+    # a scratch folder with room for the world file and every replica's final
+    # state file (48 bytes per particle)
+    replicas = run_reference.replicas_that_fit(w, _host_cores())
+    state_bytes = int(48 * 1.05 * w.expected_particles())
+    cands = [os.environ.get("TMPDIR"), "/tmp", "/var/tmp", "/dev/shm"]
+    base = None
+    for c in cands:
+        if c and os.path.isdir(c):
+            free = shutil.disk_usage(c).free
+            fit = int((free - 1.1 * need) // state_bytes) if free > 1.1 * need else 0
+            if fit >= 1:
+                base, replicas = c, max(1, min(replicas, fit))
+                break
+    if base is None:
+        raise RuntimeError(f"no scratch folder with {need / 1e9:.1f} GB free for the reference's world file")
+    root = Path(tempfile.mkdtemp(prefix="dsmc_ref_full_", dir=base))
+    try:
+        t0 = time.perf_counter()
+        g.write_world(root / "worlds")
+        tool_s = time.perf_counter() - t0
+        res = run_reference.run_replicas(w.settings(statistics_interval=100), g, timesteps=steps, replicas=replicas,
+                                         workdir=root / "runs", world_dir=root / "worlds", timeout=1800)
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+    reps = res["reports"]
+    mol = reps[0].get("molecules")
+    init_s = statistics.median(r.get("initialize", 0.0) for r in reps)
+    return {
+        "value": res["particle_steps_per_s"], "unit": UNIT, "cores": replicas, "kind": "reference",
+        "particles_per_replica": mol, "workload": w.name, "steps": steps,
+        "step_seconds_median": statistics.median(r["step_seconds"] for r in reps),
+        "geometry_tool_s": tool_s, "initialize_s_median": init_s,
+        "host_cores": _host_cores(), "host_mem_available_gb": run_reference.host_memory_available() / 1e9,
+        "sample": (f"{replicas} independent single-rank runs of the reference solver (oracle/_ref/dsmc_ref, g++ -O3) "
+                   f"on the {w.name} workload itself ({w.n}^3 voxels, {mol} particles each; world from the "
+                   f"reference's geometry tool), {steps} timesteps each; replica count limited by host cores "
+                   f"({_host_cores()}) and 70 % of available host memory at ~{w.replica_bytes() / 1e9:.0f} GB per "
+                   f"replica; its own stage timers (moving+colliding+accelerating+sampling)"),
     }
 
 
 def run_reference_arm(args, world, rank, pg):
+    """The reference's own CPU solver on this arm's workload and metric.  Imports
+    nothing of the B200 library: worlds come from the reference's geometry
+    tool, settings from the oracle's own workload table."""
     if rank != 0:
         return 0
-    steps = max(args.steps, 1)
     t0 = time.time()
+    # a bounded sample of the workload per replica: a few of its timesteps
+    steps = max(1, min(args.steps, args.ref_steps))
     try:
-        cb = cpu_reference(steps=min(steps, 200))
+        full = cpu_reference_full(args.workload, steps)
     except Exception as e:  # noqa: BLE001
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU solver could not run: {e}"}))
         return 0
-    from master_b200 import workloads
-    W = workloads.WORKLOADS[args.workload]
-    per_replica = cb.get("particles_per_replica")
-    # a step of one replica: its particles over its share of the throughput
-    ms = (1e3 * per_replica * cb["cores"] / cb["value"]) if per_replica and cb["value"] else None
+    sample = None
+    if not args.no_cpu_baseline:
+        try:
+            sample = cpu_reference_sample(steps=args.cpu_steps)
+        except Exception as e:  # noqa: BLE001
+            sample = {"value": None, "unavailable": str(e)}
+    per_replica = full.get("particles_per_replica")
+    ms = 1e3 * full["step_seconds_median"] / steps if full.get("step_seconds_median") else None
     line = {
-        "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": min(steps, 200),
+        "metric": METRIC, "value": full["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
         "warmup": 0, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic", "impl": "reference",
         # the reference's timers cover every step of its run: no warm-up to leave out
-        "config": {"workload": W.name, "voxels": W.n, "cells": W.cells, "atoms_per_molecule": W.atoms_per_molecule,
-                   "parallelism": f"{cb['cores']} replicas on host cores",
-                   "sample": "bounded 64^3 sample of the workload per replica (cpu_baseline.sample)"},
-        "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "config": {"workload": full["workload"], "particles_per_replica": per_replica,
+                   "parallelism": f"{full['cores']} replicas on host cores",
+                   "sample": f"{steps} timesteps of the workload per replica (cpu_baseline.sample)"},
+        "cpu_baseline": full,
+        "sample_leg_64": sample,
+        "e2e": {"value": full["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": time.time() - t0,
     }
     print(json.dumps(line))
@@ -186,7 +259,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="packed_256")
     ap.add_argument("--e2e-steps", type=int, default=None)
-    ap.add_argument("--cpu-steps", type=int, default=100)
+    ap.add_argument("--cpu-steps", type=int, default=20)
+    ap.add_argument("--ref-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -334,7 +408,7 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_reference(steps=args.cpu_steps)
+            line["cpu_baseline"] = cpu_reference_sample(steps=args.cpu_steps)
         except Exception as e:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
     system.ctx.close()

@@ -149,8 +149,10 @@ int dsmc_geometry_finish_gpu(int device_id, uint32_t nx, uint32_t ny, uint32_t n
  * the reference.  Its device-side working buffers are a file-scope array of
  * the library sized for at most 64^3 voxels (13.1 MB kept by every GPU that
  * loads the library until exit); larger grids return DSMC_ERR_CAPACITY.  The
- * first call on a device looks up the array's device address (make it before
- * any stream capture); calls that overlap on one GPU race on the array. */
+ * first call on a device looks up the array's device address and keeps it
+ * (make that call before any stream capture; after a cudaDeviceReset of the
+ * device the kept address is stale, so do not call it there again); calls
+ * that overlap on one GPU race on the array. */
 int dsmc_geometry_finish_gpu_noalloc(int device_id, uint32_t nx, uint32_t ny, uint32_t nz,
                                      int number_of_neighbor_averages, uint8_t *voxels, float *normals,
                                      float *tangents1, float *tangents2);

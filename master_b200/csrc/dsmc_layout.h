@@ -41,16 +41,13 @@
 #define DSMC_EBIT_SPILL_FULL 8u  // the overflow list itself overflowed
 #define DSMC_EBIT_SMEM 16u       // a cell held more particles than the staging buffer
 #define DSMC_EBIT_NAN 32u        // non-finite position or velocity
-#define DSMC_EBIT_TIMEOUT 128u   // a bounded wait on a bulk copy ran out
-#define DSMC_EBIT_ALIGN 256u     // a bulk copy operand was not 16-byte aligned (copy skipped)
 #define DSMC_EBIT_WALL 512u      // the Cercignani-Lampis sampler accepted nothing within its limit
 #define DSMC_EBIT_STRANDED 64u   // a move ended inside solid whose cell has no free volume; the
                                  // particle stays in its previous cell and is re-seeded next step
 // bits that stop the pipeline (a failed facet search or a stranded particle is
 // re-seeded, counted, and the pipeline goes on)
 #define DSMC_EBIT_FATAL \
-    (DSMC_EBIT_CELL | DSMC_EBIT_RESEED | DSMC_EBIT_SPILL_FULL | DSMC_EBIT_SMEM | DSMC_EBIT_NAN | DSMC_EBIT_TIMEOUT | \
-     DSMC_EBIT_ALIGN | DSMC_EBIT_WALL)
+    (DSMC_EBIT_CELL | DSMC_EBIT_RESEED | DSMC_EBIT_SPILL_FULL | DSMC_EBIT_SMEM | DSMC_EBIT_NAN | DSMC_EBIT_WALL)
 
 // cell_map values of cells that are not this system's active cells
 #define DSMC_CELL_SOLID (-1)    // no free volume

@@ -138,41 +138,36 @@ __global__ void k_frames(uint64_t V, const float *nrm, const float *seed, float 
 
 using namespace dsmc;
 
-extern "C" int dsmc_geometry_finish_gpu(int device_id, uint32_t nx, uint32_t ny, uint32_t nz, int avg, uint8_t *vox,
-                                        float *nrm, float *t1, float *t2) {
-    if (!vox || !nrm || !t1 || !t2 || nx == 0 || ny == 0 || nz == 0 || avg < 0) return DSMC_ERR_ARG;
-    if (cudaSetDevice(device_id) != cudaSuccess) {
-        set_thread_error("no CUDA device for geometry preprocessing");
-        return DSMC_ERR_NO_DEVICE;
-    }
-    const Dims d = {(int)nx, (int)ny, (int)nz, avg};
-    const uint64_t V = (uint64_t)nx * ny * nz;
-    uint8_t *dmask = nullptr, *dcand = nullptr;
-    float *dn = nullptr, *dseed = nullptr, *dt1 = nullptr, *dt2 = nullptr;
-    auto cleanup = [&]() {
-        cudaFree(dmask);
-        cudaFree(dcand);
-        cudaFree(dn);
-        cudaFree(dseed);
-        cudaFree(dt1);
-        cudaFree(dt2);
-    };
+namespace dsmc {
+namespace {
+
+// Device working buffers of the stencil: mask and candidate flags (V bytes
+// each), normals, tangent seeds, tangents1, tangents2 (3 floats per voxel each).
+struct StencilBuffers {
+    uint8_t *mask, *cand;
+    float *normals, *seed, *t1, *t2;
+};
+
+// The preprocessing itself, on buffers the caller provides: the normal
+// stencil on the GPU, the sequential replay of the removals on the host, then
+// the tangent frames and boundary typing on the GPU.  `what` prefixes error
+// messages.  Allocates no device memory.
+int finish_on_device(const Dims &d, uint8_t *vox, float *nrm, float *t1, float *t2, const StencilBuffers &b,
+                     const char *what) {
+    const uint64_t V = (uint64_t)d.X * d.Y * d.Z;
     auto cuda_err = [&](cudaError_t e) {
-        cleanup();
-        set_thread_error(std::string("geometry on the GPU: ") + cudaGetErrorString(e));
+        set_thread_error(std::string(what) + ": " + cudaGetErrorString(e));
         return DSMC_ERR_CUDA;
     };
     cudaError_t e;
-    if ((e = cudaMalloc(&dmask, V)) || (e = cudaMalloc(&dcand, V)) || (e = cudaMalloc(&dn, 12 * V)))
-        return cuda_err(e);
-    if ((e = cudaMemcpy(dmask, vox, V, cudaMemcpyHostToDevice))) return cuda_err(e);
+    if ((e = cudaMemcpy(b.mask, vox, V, cudaMemcpyHostToDevice))) return cuda_err(e);
     const int block = 256;
     const int grid = (int)std::min<uint64_t>((V + block - 1) / block, 148 * 64);
-    k_normals<<<grid, block>>>(d, dmask, dn, dcand);
+    k_normals<<<grid, block>>>(d, b.mask, b.normals, b.cand);
     if ((e = cudaGetLastError())) return cuda_err(e);
     std::vector<uint8_t> cand(V);
-    if ((e = cudaMemcpy(nrm, dn, 12 * V, cudaMemcpyDeviceToHost)) ||
-        (e = cudaMemcpy(cand.data(), dcand, V, cudaMemcpyDeviceToHost)))
+    if ((e = cudaMemcpy(nrm, b.normals, 12 * V, cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(cand.data(), b.cand, V, cudaMemcpyDeviceToHost)))
         return cuda_err(e);
     // Sequential replay of the voxels a removal can reach, in sweep order.
     std::priority_queue<uint64_t, std::vector<uint64_t>, std::greater<uint64_t>> dirty;
@@ -182,11 +177,11 @@ extern "C" int dsmc_geometry_finish_gpu(int device_id, uint32_t nx, uint32_t ny,
             dirty.push(idx);
             queued[idx] = 1;
         }
-    const int reach = std::max(1, avg);
+    const int reach = std::max(1, d.avg);
     while (!dirty.empty()) {
         const uint64_t idx = dirty.top();
         dirty.pop();
-        const int k = (int)(idx % nz), j = (int)((idx / nz) % ny), i = (int)(idx / ((uint64_t)ny * nz));
+        const int k = (int)(idx % d.Z), j = (int)((idx / d.Z) % d.Y), i = (int)(idx / ((uint64_t)d.Y * d.Z));
         float n[3];
         const bool emptied = normal_of(d, vox, i, j, k, n);
         nrm[3 * idx] = n[0];
@@ -209,20 +204,50 @@ extern "C" int dsmc_geometry_finish_gpu(int device_id, uint32_t nx, uint32_t ny,
     std::vector<float> seed(3 * V);
     Ran1 rnd(-1);
     for (uint64_t q = 0; q < 3 * V; ++q) seed[q] = (float)rnd.next();
-    if ((e = cudaMalloc(&dseed, 12 * V)) || (e = cudaMalloc(&dt1, 12 * V)) || (e = cudaMalloc(&dt2, 12 * V)))
+    if ((e = cudaMemcpy(b.normals, nrm, 12 * V, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(b.seed, seed.data(), 12 * V, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(b.mask, vox, V, cudaMemcpyHostToDevice)))
         return cuda_err(e);
-    if ((e = cudaMemcpy(dn, nrm, 12 * V, cudaMemcpyHostToDevice)) ||
-        (e = cudaMemcpy(dseed, seed.data(), 12 * V, cudaMemcpyHostToDevice)) ||
-        (e = cudaMemcpy(dmask, vox, V, cudaMemcpyHostToDevice)))
-        return cuda_err(e);
-    k_frames<<<grid, block>>>(V, dn, dseed, dt1, dt2, dmask);
+    k_frames<<<grid, block>>>(V, b.normals, b.seed, b.t1, b.t2, b.mask);
     if ((e = cudaGetLastError())) return cuda_err(e);
-    if ((e = cudaMemcpy(t1, dt1, 12 * V, cudaMemcpyDeviceToHost)) ||
-        (e = cudaMemcpy(t2, dt2, 12 * V, cudaMemcpyDeviceToHost)) ||
-        (e = cudaMemcpy(vox, dmask, V, cudaMemcpyDeviceToHost)))
+    if ((e = cudaMemcpy(t1, b.t1, 12 * V, cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(t2, b.t2, 12 * V, cudaMemcpyDeviceToHost)) ||
+        (e = cudaMemcpy(vox, b.mask, V, cudaMemcpyDeviceToHost)))
         return cuda_err(e);
-    cleanup();
     return DSMC_OK;
+}
+
+}  // namespace
+}  // namespace dsmc
+
+extern "C" int dsmc_geometry_finish_gpu(int device_id, uint32_t nx, uint32_t ny, uint32_t nz, int avg, uint8_t *vox,
+                                        float *nrm, float *t1, float *t2) {
+    if (!vox || !nrm || !t1 || !t2 || nx == 0 || ny == 0 || nz == 0 || avg < 0) return DSMC_ERR_ARG;
+    if (cudaSetDevice(device_id) != cudaSuccess) {
+        set_thread_error("no CUDA device for geometry preprocessing");
+        return DSMC_ERR_NO_DEVICE;
+    }
+    const Dims d = {(int)nx, (int)ny, (int)nz, avg};
+    const uint64_t V = (uint64_t)nx * ny * nz;
+    StencilBuffers b = {};
+    auto cleanup = [&]() {
+        cudaFree(b.mask);
+        cudaFree(b.cand);
+        cudaFree(b.normals);
+        cudaFree(b.seed);
+        cudaFree(b.t1);
+        cudaFree(b.t2);
+    };
+    cudaError_t e;
+    if ((e = cudaMalloc(&b.mask, V)) || (e = cudaMalloc(&b.cand, V)) || (e = cudaMalloc(&b.normals, 12 * V)) ||
+        (e = cudaMalloc(&b.seed, 12 * V)) || (e = cudaMalloc(&b.t1, 12 * V)) || (e = cudaMalloc(&b.t2, 12 * V))) {
+        cleanup();
+        set_thread_error(std::string("geometry on the GPU: ") + cudaGetErrorString(e));
+        return DSMC_ERR_CUDA;
+    }
+    const int rc = finish_on_device(d, vox, nrm, t1, t2, b, "geometry on the GPU");
+    cleanup();
+    return rc;
 }
 
 // ---------------------------------------------------------------------------
@@ -238,7 +263,9 @@ extern "C" int dsmc_geometry_finish_gpu(int device_id, uint32_t nx, uint32_t ny,
 // The array's host-side name is only a stand-in for the device symbol: the
 // device address is looked up with cudaGetSymbolAddress once per device, on
 // that device's first call, and cached.  That first call should therefore
-// come before any stream capture.  Every call reuses the same array and
+// come before any stream capture.  A cudaDeviceReset by the caller unloads
+// the module and invalidates the cached address: a process that resets a
+// device must not call this entry point on that device afterwards.  Every call reuses the same array and
 // leaves its contents behind; each kernel here rewrites every element it
 // later reads, so nothing needs clearing between calls.  Calls that overlap
 // on the GPU (two host threads, same device) race on the array.
@@ -285,69 +312,13 @@ extern "C" int dsmc_geometry_finish_gpu_noalloc(int device_id, uint32_t nx, uint
     }
     // layout: mask[V], cand[V], then normals, seeds, tangents1, tangents2
     // (3 floats per voxel each), every part 16-byte aligned
-    uint8_t *dmask = base;
-    uint8_t *dcand = base + kNoAllocMaxVoxels;
-    float *dn = reinterpret_cast<float *>(base + 2 * kNoAllocMaxVoxels);
-    float *dseed = dn + 3 * kNoAllocMaxVoxels;
-    float *dt1 = dseed + 3 * kNoAllocMaxVoxels;
-    float *dt2 = dt1 + 3 * kNoAllocMaxVoxels;
-    auto cuda_err = [&](cudaError_t e) {
-        set_thread_error(std::string("geometry on the GPU (fixed scratch): ") + cudaGetErrorString(e));
-        return DSMC_ERR_CUDA;
-    };
+    StencilBuffers b;
+    b.mask = base;
+    b.cand = base + kNoAllocMaxVoxels;
+    b.normals = reinterpret_cast<float *>(base + 2 * kNoAllocMaxVoxels);
+    b.seed = b.normals + 3 * kNoAllocMaxVoxels;
+    b.t1 = b.seed + 3 * kNoAllocMaxVoxels;
+    b.t2 = b.t1 + 3 * kNoAllocMaxVoxels;
     const Dims d = {(int)nx, (int)ny, (int)nz, avg};
-    cudaError_t e;
-    if ((e = cudaMemcpy(dmask, vox, V, cudaMemcpyHostToDevice))) return cuda_err(e);
-    const int block = 256;
-    const int grid = (int)std::min<uint64_t>((V + block - 1) / block, 148 * 64);
-    k_normals<<<grid, block>>>(d, dmask, dn, dcand);
-    if ((e = cudaGetLastError())) return cuda_err(e);
-    std::vector<uint8_t> cand(V);
-    if ((e = cudaMemcpy(nrm, dn, 12 * V, cudaMemcpyDeviceToHost)) ||
-        (e = cudaMemcpy(cand.data(), dcand, V, cudaMemcpyDeviceToHost)))
-        return cuda_err(e);
-    std::priority_queue<uint64_t, std::vector<uint64_t>, std::greater<uint64_t>> dirty;
-    std::vector<uint8_t> queued(V, 0);
-    for (uint64_t idx = 0; idx < V; ++idx)
-        if (cand[idx]) {
-            dirty.push(idx);
-            queued[idx] = 1;
-        }
-    const int reach = std::max(1, avg);
-    while (!dirty.empty()) {
-        const uint64_t idx = dirty.top();
-        dirty.pop();
-        const int k = (int)(idx % nz), j = (int)((idx / nz) % ny), i = (int)(idx / ((uint64_t)ny * nz));
-        float n[3];
-        const bool emptied = normal_of(d, vox, i, j, k, n);
-        nrm[3 * idx] = n[0];
-        nrm[3 * idx + 1] = n[1];
-        nrm[3 * idx + 2] = n[2];
-        if (emptied && vox[idx] != 0) {
-            vox[idx] = 0;
-            for (int di = -reach; di <= reach; ++di)
-                for (int dj = -reach; dj <= reach; ++dj)
-                    for (int dk = -reach; dk <= reach; ++dk) {
-                        const uint64_t q = lin(d, i + di, j + dj, k + dk);
-                        if (q > idx && !queued[q]) {
-                            queued[q] = 1;
-                            dirty.push(q);
-                        }
-                    }
-        }
-    }
-    std::vector<float> seed(3 * V);
-    Ran1 rnd(-1);
-    for (uint64_t q = 0; q < 3 * V; ++q) seed[q] = (float)rnd.next();
-    if ((e = cudaMemcpy(dn, nrm, 12 * V, cudaMemcpyHostToDevice)) ||
-        (e = cudaMemcpy(dseed, seed.data(), 12 * V, cudaMemcpyHostToDevice)) ||
-        (e = cudaMemcpy(dmask, vox, V, cudaMemcpyHostToDevice)))
-        return cuda_err(e);
-    k_frames<<<grid, block>>>(V, dn, dseed, dt1, dt2, dmask);
-    if ((e = cudaGetLastError())) return cuda_err(e);
-    if ((e = cudaMemcpy(t1, dt1, 12 * V, cudaMemcpyDeviceToHost)) ||
-        (e = cudaMemcpy(t2, dt2, 12 * V, cudaMemcpyDeviceToHost)) ||
-        (e = cudaMemcpy(vox, dmask, V, cudaMemcpyDeviceToHost)))
-        return cuda_err(e);
-    return DSMC_OK;
+    return finish_on_device(d, vox, nrm, t1, t2, b, "geometry on the GPU (fixed scratch)");
 }

@@ -52,7 +52,7 @@ def summarize(rows):
 
 def main():
     if not run_reference.available():
-        raise SystemExit("build oracle/_ref first: make -C oracle ref")
+        raise SystemExit("build oracle/_ref first: make -C oracle ref REF=<reference project>/code/base_code/program/dsmc")
     s = WORKLOAD.settings(statistics_interval=INTERVAL)
     g = WORKLOAD.geometry()
     stats = {k: [] for k in ("collisions", "wall_collisions", "flux", "temperature_K", "molecules")}

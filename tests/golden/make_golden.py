@@ -138,7 +138,7 @@ def geometry_digests():
 
 if __name__ == "__main__":
     if not rh.available():
-        raise SystemExit("build oracle/_ref first: make -C oracle ref")
+        raise SystemExit("build oracle/_ref first: make -C oracle ref REF=<reference project>/code/base_code/program/dsmc")
     only = sys.argv[1:]  # case names to (re)generate; all when none
     for name, c in CASES.items():
         if not only or name in only:
