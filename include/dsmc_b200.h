@@ -360,7 +360,21 @@ int dsmc_pass_info(dsmc_ctx *ctx, int *pipelined, int *grid, int *block, int *st
 int dsmc_ctx_set_timing(dsmc_ctx *ctx, int on);
 int dsmc_pass_times_get(dsmc_ctx *ctx, double ms[4], int64_t *passes);
 
-/* Reads the status of the last pass: bit flags of device-side errors. */
+/* Reads the status of the last pass: bit flags of device-side errors
+ * (DSMC_EBIT_*) and the number of particles spilled to the overflow list. */
+#define DSMC_EBIT_CELL 1u        /* a particle ended in a cell with no free volume */
+#define DSMC_EBIT_FACET 2u       /* facet search found no face of the hit voxel (re-seeded, counted) */
+#define DSMC_EBIT_RESEED 4u      /* re-seeding found no empty voxel within its limit */
+#define DSMC_EBIT_SPILL_FULL 8u  /* the overflow list itself overflowed */
+#define DSMC_EBIT_SMEM 16u       /* a cell held more particles than the staging buffer */
+#define DSMC_EBIT_NAN 32u        /* non-finite position or velocity */
+#define DSMC_EBIT_STRANDED 64u   /* a move ended inside solid whose cell has no free volume; the
+                                    particle stays in its previous cell and is re-seeded next step */
+#define DSMC_EBIT_WALL 512u      /* the Cercignani-Lampis sampler accepted nothing within its limit */
+/* bits that stop the pipeline (a failed facet search or a stranded particle
+ * is re-seeded, counted, and the pipeline goes on) */
+#define DSMC_EBIT_FATAL \
+    (DSMC_EBIT_CELL | DSMC_EBIT_RESEED | DSMC_EBIT_SPILL_FULL | DSMC_EBIT_SMEM | DSMC_EBIT_NAN | DSMC_EBIT_WALL)
 int dsmc_device_status(dsmc_ctx *ctx, uint32_t *error_bits, uint32_t *spill);
 
 /* The CUDA stream (cudaStream_t) the context enqueues its work on, for

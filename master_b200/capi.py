@@ -24,6 +24,11 @@ DSMC_ERR_STATE = 6
 DSMC_ERR_NOT_FOUND = 7
 DSMC_ERR_NO_DEVICE = 8
 
+# error bits of dsmc_device_status (include/dsmc_b200.h)
+EBIT_CELL, EBIT_FACET, EBIT_RESEED, EBIT_SPILL_FULL, EBIT_SMEM, EBIT_NAN, EBIT_STRANDED, EBIT_WALL = (
+    1, 2, 4, 8, 16, 32, 64, 512)
+EBIT_FATAL = EBIT_CELL | EBIT_RESEED | EBIT_SPILL_FULL | EBIT_SMEM | EBIT_NAN | EBIT_WALL
+
 PREC_SPLIT32 = 0
 PREC_FP64 = 1
 

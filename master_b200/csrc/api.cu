@@ -966,7 +966,9 @@ static int place_particles(dsmc_ctx *ctx, int sys_id, long long n, const double 
     CK(e);
     if (st.error & DSMC_EBIT_FATAL) {
         cudaMemsetAsync(ctx->status.p, 0, sizeof(unsigned), ctx->stream);
-        return fail(ctx, DSMC_ERR_STATE, "a particle lies in a solid voxel or a cell with no free volume");
+        return fail(ctx, DSMC_ERR_STATE, (st.error & DSMC_EBIT_NAN)
+                                             ? "a particle has a non-finite position or velocity"
+                                             : "a particle lies in a solid voxel or a cell with no free volume");
     }
     h.num_particles = n;
     h.id_count = (uint32_t)n;

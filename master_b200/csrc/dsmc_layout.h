@@ -34,20 +34,8 @@
 #define DSMC_TAG_COLLIDE 2u
 #define DSMC_TAG_INIT 3u
 
-// error bits reported in Status::error
-#define DSMC_EBIT_CELL 1u        // a particle ended in a cell with no free volume
-#define DSMC_EBIT_FACET 2u       // facet search found no face of the hit voxel
-#define DSMC_EBIT_RESEED 4u      // re-seeding found no empty voxel within its limit
-#define DSMC_EBIT_SPILL_FULL 8u  // the overflow list itself overflowed
-#define DSMC_EBIT_SMEM 16u       // a cell held more particles than the staging buffer
-#define DSMC_EBIT_NAN 32u        // non-finite position or velocity
-#define DSMC_EBIT_WALL 512u      // the Cercignani-Lampis sampler accepted nothing within its limit
-#define DSMC_EBIT_STRANDED 64u   // a move ended inside solid whose cell has no free volume; the
-                                 // particle stays in its previous cell and is re-seeded next step
-// bits that stop the pipeline (a failed facet search or a stranded particle is
-// re-seeded, counted, and the pipeline goes on)
-#define DSMC_EBIT_FATAL \
-    (DSMC_EBIT_CELL | DSMC_EBIT_RESEED | DSMC_EBIT_SPILL_FULL | DSMC_EBIT_SMEM | DSMC_EBIT_NAN | DSMC_EBIT_WALL)
+// error bits reported in Status::error: DSMC_EBIT_* of the public header
+#include "dsmc_b200.h"
 
 // cell_map values of cells that are not this system's active cells
 #define DSMC_CELL_SOLID (-1)    // no free volume

@@ -64,6 +64,14 @@ __global__ void k_from_fp64(const SysDev *sys, int s, const double *r, const dou
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         double rr[3] = {r[3 * i], r[3 * i + 1], r[3 * i + 2]};
         double vv[3] = {v[3 * i], v[3 * i + 1], v[3 * i + 2]};
+        bool finite = true;
+        for (int d = 0; d < 3; ++d) finite = finite && isfinite(rr[d]) && isfinite(vv[d]);
+        if (!finite) {
+            // refused by the caller (DSMC_ERR_STATE); the record is left out
+            atomicOr(err, DSMC_EBIT_NAN);
+            key[i] = DSMC_CELL_SOLID;
+            continue;
+        }
         Particle p;
         Maker<Prec>::make(g, rr, vv, id_base + (uint32_t)i, p);
         const int ac = particle_cell(g, p, err);

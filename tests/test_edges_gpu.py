@@ -149,3 +149,33 @@ def test_device_layout_follows_the_capacity_rule(capacity):
     expect = (z["r0"].shape[0] * pix) / pix.sum()
     cap = np.maximum(np.ceil(factor * np.maximum(expect, present) + pad), 1.0)
     assert S.info().slots == int(cap.sum())
+
+
+@pytest.mark.parametrize("precision", [capi.PREC_SPLIT32, capi.PREC_FP64])
+@pytest.mark.parametrize("where", ["r_nan", "v_nan", "v_inf"])
+def test_non_finite_state_is_refused_and_the_system_keeps_its_particles(precision, where):
+    """A non-finite position or velocity handed to dsmc_particles_set is
+    refused (DSMC_ERR_STATE, the message says why) before it reaches a
+    kernel; the system keeps the particles it had and steps on."""
+    z, meta, s, g = load_case("small_dt1")
+    S = System(s, g, precision=precision, init_particles=False)
+    S.set_particles(z["r0"], z["v0"])
+    r_before, v_before = S.get_particles()
+    r, v = z["r0"].copy(), z["v0"].copy()
+    if where == "r_nan":
+        r[len(r) // 2, 1] = np.nan
+    elif where == "v_nan":
+        v[3, 0] = np.nan
+    else:
+        v[-1, 2] = np.inf
+    with pytest.raises(capi.DsmcError) as e:
+        S.set_particles(r, v)
+    assert e.value.code == capi.DSMC_ERR_STATE and "non-finite" in str(e.value)
+    assert S.num_molecules == len(z["r0"])
+    r_after, v_after = S.get_particles()
+    assert np.array_equal(r_after, r_before) and np.array_equal(v_after, v_before)
+    S.step(3)
+    err, _ = S.ctx.device_status()
+    assert err & capi.EBIT_FATAL == 0
+    r3, v3 = S.get_particles()
+    assert np.isfinite(r3).all() and np.isfinite(v3).all() and S.tallies().step == 3
