@@ -231,6 +231,22 @@ int dsmc_exchange_put(dsmc_ctx *ctx, int sys_id, int64_t n, const void *records,
  * System::setup_molecules (dsmc/system.cpp:398-430); draws come from one
  * counter-based stream per particle.  n < 0: the reference's count. */
 int dsmc_particles_init(dsmc_ctx *ctx, int sys_id, int64_t n);
+/* Warm start: replaces a system's particles by n particles (n < 0: the
+ * reference's count) drawn from a per-voxel field instead of the uniform
+ * Maxwellian at rest of System::setup_molecules (dsmc/system.cpp:398-430):
+ * voxel w is chosen with probability weight[w] / sum(weight) over the empty
+ * voxels, the position uniformly inside it, the velocity drift[3w..3w+2] plus
+ * a Maxwellian of the gas temperature.  weight holds nx*ny*nz floats and
+ * drift 3*nx*ny*nz (reduced velocity units), in the geometry's voxel order;
+ * device != 0: both are device memory of the context's GPU.  Draws come from
+ * one counter-based stream per particle, as dsmc_particles_init's. */
+int dsmc_particles_init_field(dsmc_ctx *ctx, int sys_id, int64_t n, const float *weight, const float *drift,
+                              int device);
+/* Adds one system's per-voxel particle sums {count, sum vx, sum vy, sum vz}
+ * (4 floats per voxel, geometry voxel order, 16-byte aligned) to field: the
+ * steady fields that the warm-start surrogate learns are these sums over
+ * many steps.  device != 0: field is device memory of the context's GPU. */
+int dsmc_field_accumulate(dsmc_ctx *ctx, int sys_id, float *field, int device);
 /* Replaces a system's particles by n particles in the reference's state-file
  * layout: r[3n], v[3n] fp64 (dsmc/dsmc_io.cpp:82-159).  Particle i gets id i. */
 int dsmc_particles_set(dsmc_ctx *ctx, int sys_id, int64_t n, const double *r, const double *v);

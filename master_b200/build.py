@@ -35,6 +35,8 @@ CUDA_SOURCES = {
     "cell_layout.cu": [],
     # must round exactly as the CPU geometry path
     "geometry_gpu.cu": ["-fmad=false"],
+    # the warm-start surrogate's tcgen05 convolutions and training kernels
+    "surrogate.cu": [],
 }
 CXX_SOURCES = ["host_setup.cpp"]
 

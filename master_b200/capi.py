@@ -45,7 +45,14 @@ EXPORTED = [
     "dsmc_pass_times_get", "dsmc_state_file_read", "dsmc_state_file_write", "dsmc_tocontinue_read",
     "dsmc_tocontinue_write", "dsmc_continue_from", "dsmc_checkpoint_save", "dsmc_checkpoint_load",
     "dsmc_profile_sums_get", "dsmc_profiles_finish", "dsmc_profiles_get", "dsmc_measures_get",
-    "dsmc_system_add_slab", "dsmc_exchange_take", "dsmc_exchange_put",
+    "dsmc_system_add_slab", "dsmc_exchange_take", "dsmc_exchange_put", "dsmc_particles_init_field",
+    "dsmc_field_accumulate",
+]
+# every entry point declared in include/dsmc_surrogate.h
+EXPORTED_SURROGATE = [
+    "dsmc_sg_conv3", "dsmc_sg_conv3_wgrad", "dsmc_sg_bias_grad", "dsmc_sg_pool2", "dsmc_sg_pool2_bwd",
+    "dsmc_sg_up2", "dsmc_sg_up2_bwd", "dsmc_sg_pack_input", "dsmc_sg_head", "dsmc_sg_loss_head_bwd",
+    "dsmc_sg_adam", "dsmc_sg_pack_weights", "dsmc_sg_status",
 ]
 
 
@@ -177,11 +184,29 @@ def load() -> C.CDLL:
                                  C.c_float, C.c_int, C.c_int, C.POINTER(C.c_int)],
         "dsmc_exchange_take": [_P, C.c_int64, C.c_void_p, C.c_int, C.POINTER(C.c_int64)],
         "dsmc_exchange_put": [_P, C.c_int, C.c_int64, C.c_void_p, C.c_int],
+        "dsmc_particles_init_field": [_P, C.c_int, C.c_int64, C.c_void_p, C.c_void_p, C.c_int],
+        "dsmc_field_accumulate": [_P, C.c_int, C.c_void_p, C.c_int],
         "dsmc_profiles_finish": [C.POINTER(Settings), C.c_double, C.c_int, _D, _D, _D, _D, _D, _D, _D],
         "dsmc_profiles_get": [_P, C.c_int, C.c_int, _D, _D, _D, _D, _D, _D, C.POINTER(C.c_int)],
         "dsmc_cells_layout": [C.POINTER(Settings), C.c_uint32, C.c_uint32, C.c_uint32, _U8, C.c_int, _I32, _I32,
                               _I32, _D, _D, C.POINTER(C.c_int)],
     }
+    V, I = C.c_void_p, C.c_int
+    sig.update({
+        "dsmc_sg_conv3": [V, I, I, V, I, I, I, V, V, I, V, I, I, I, V, I, I],
+        "dsmc_sg_conv3_wgrad": [V, I, I, V, I, I, I, V, I, I, I, V],
+        "dsmc_sg_bias_grad": [V, I, I, V, I, I, I, V],
+        "dsmc_sg_pool2": [V, I, I, V, I, I, I, V, I, I],
+        "dsmc_sg_pool2_bwd": [V, I, I, V, I, I, V, I, I, V, I, I, I, V, I, I],
+        "dsmc_sg_up2": [V, I, I, V, I, I, I, V, I, I],
+        "dsmc_sg_up2_bwd": [V, I, I, V, I, I, V, I, I, I, V, I, I],
+        "dsmc_sg_pack_input": [V, I, I, V, V, V],
+        "dsmc_sg_head": [V, I, I, V, I, I, V, V, V],
+        "dsmc_sg_loss_head_bwd": [V, I, I, V, V, V, V, C.c_float, V, I, I, V, V, V, V, I, I, V],
+        "dsmc_sg_adam": [V, V, V, V, V, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int64],
+        "dsmc_sg_pack_weights": [V, V, I, I, V, V],
+        "dsmc_sg_status": [C.POINTER(C.c_uint), I],
+    })
     for name, args in sig.items():
         fn = getattr(lib, name)
         fn.argtypes = args

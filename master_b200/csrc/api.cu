@@ -1008,6 +1008,109 @@ int dsmc_particles_init(dsmc_ctx *ctx, int sys_id, int64_t n) {
     return place_particles(ctx, sys_id, n, nullptr, nullptr);
 }
 
+// Warm start: n particles drawn from a per-voxel weight and drift field
+// instead of System::setup_molecules' uniform Maxwellian at rest
+// (dsmc/system.cpp:398-430).  The weights of non-empty voxels are ignored.
+int dsmc_particles_init_field(dsmc_ctx *ctx, int sys_id, int64_t n, const float *weight, const float *drift,
+                              int device) {
+    if (!ctx || sys_id < 0 || sys_id >= (int)ctx->systems.size() || !weight || !drift) return DSMC_ERR_ARG;
+    SysHost &h = *ctx->systems[sys_id];
+    if (h.slab) return fail(ctx, DSMC_ERR_CONFIG, "a slab is initialised by dsmc_particles_init or _set");
+    if (n < 0) n = h.expected;
+    if (n > 0xffffffffLL) return fail(ctx, DSMC_ERR_CAPACITY, "at most 2^32 particles per system");
+    cudaSetDevice(ctx->device);
+    const long long V = (long long)h.n[0] * h.n[1] * h.n[2];
+    std::vector<float> w(V);
+    std::vector<uint8_t> vox(V);
+    if (device) {
+        CK(cudaMemcpy(w.data(), weight, V * sizeof(float), cudaMemcpyDeviceToHost));
+    } else {
+        std::memcpy(w.data(), weight, V * sizeof(float));
+    }
+    CK(cudaMemcpy(vox.data(), h.vox.p, V, cudaMemcpyDeviceToHost));
+    std::vector<double> cdf(V + 1);
+    cdf[0] = 0.0;
+    for (long long i = 0; i < V; ++i) {
+        const float x = w[i];
+        const double wi = (vox[i] == DSMC_VOX_EMPTY && std::isfinite(x) && x > 0.0f) ? (double)x : 0.0;
+        cdf[i + 1] = cdf[i] + wi;
+    }
+    if (!(cdf[V] > 0.0)) return fail(ctx, DSMC_ERR_STATE, "the weight field is zero in every empty voxel");
+    DevBuf<double> dcdf;
+    DevBuf<float> ddrift;
+    CK(dcdf.ensure(V + 1));
+    CK(cudaMemcpyAsync(dcdf.p, cdf.data(), (V + 1) * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    const float *drift_dev = drift;
+    if (!device) {
+        CK(ddrift.ensure(3 * V));
+        CK(cudaMemcpyAsync(ddrift.p, drift, 3 * V * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        drift_dev = ddrift.p;
+    }
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    long long staged = 0;
+    rc = stage_present(ctx, n, sys_id, &staged);
+    if (rc) return rc;
+    const size_t half = ctx->rec_half();
+    if (n) {
+        const cudaError_t e =
+            is_fp64(ctx) ? fp64::launch_init_field(ctx->sys_dev.p, sys_id, h.sqrt_t_over_m, n, dcdf.p, drift_dev, V,
+                                                   ctx->fA.p + staged * half, ctx->fB.p + staged * half,
+                                                   ctx->fkey.p + staged, ctx->hist.p, &ctx->status.p->error,
+                                                   ctx->stream)
+                         : split32::launch_init_field(ctx->sys_dev.p, sys_id, h.sqrt_t_over_m, n, dcdf.p, drift_dev, V,
+                                                      ctx->fA.p + staged * half, ctx->fB.p + staged * half,
+                                                      ctx->fkey.p + staged, ctx->hist.p, &ctx->status.p->error,
+                                                      ctx->stream);
+        CK(e);
+    }
+    cudaError_t e;
+    Status st = read_status(ctx, &e);
+    CK(e);
+    if (st.error & DSMC_EBIT_FATAL) {
+        cudaMemsetAsync(ctx->status.p, 0, sizeof(unsigned), ctx->stream);
+        return fail(ctx, DSMC_ERR_STATE, (st.error & DSMC_EBIT_NAN) ? "a drift is not finite"
+                                                                    : "a particle landed in a cell with no free volume");
+    }
+    h.num_particles = n;
+    h.id_count = (uint32_t)n;
+    return relayout(ctx, staged + n);
+}
+
+// Per-voxel sums {count, sum vx, sum vy, sum vz} of a system's particles added
+// to field (4 floats per voxel in the voxel order of the geometry).
+int dsmc_field_accumulate(dsmc_ctx *ctx, int sys_id, float *field, int device) {
+    if (!ctx || sys_id < 0 || sys_id >= (int)ctx->systems.size() || !field) return DSMC_ERR_ARG;
+    if (((uintptr_t)field & 15u) != 0) return fail(ctx, DSMC_ERR_ARG, "the field must be 16-byte aligned");
+    SysHost &h = *ctx->systems[sys_id];
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    const long long V = (long long)h.n[0] * h.n[1] * h.n[2];
+    DevBuf<float> tmp;
+    float *f = field;
+    if (!device) {
+        CK(tmp.ensure(4 * V));
+        CK(cudaMemcpyAsync(tmp.p, field, 4 * V * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        f = tmp.p;
+    }
+    if (h.active_end > h.active_begin) {
+        const cudaError_t e =
+            is_fp64(ctx) ? fp64::launch_field_accumulate(ctx->sys_dev.p, sys_id, cell_arrays(ctx), particle_arrays(ctx),
+                                                         ctx->cur, ctx->cphase, reinterpret_cast<float4 *>(f),
+                                                         ctx->stream)
+                         : split32::launch_field_accumulate(ctx->sys_dev.p, sys_id, cell_arrays(ctx),
+                                                            particle_arrays(ctx), ctx->cur, ctx->cphase,
+                                                            reinterpret_cast<float4 *>(f), ctx->stream);
+        CK(e);
+    }
+    if (!device) {
+        CK(cudaMemcpyAsync(field, tmp.p, 4 * V * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return DSMC_OK;
+}
+
 // main.cpp:37-55: t, steps, collisions and wall collisions carried over from
 // an earlier run; the flux window restarts at t (system.t0 = t).
 int dsmc_continue_from(dsmc_ctx *ctx, int sys_id, double t, uint64_t steps, uint64_t collisions,

@@ -18,6 +18,12 @@ namespace dsmc {
                                  cudaStream_t st);                                                              \
     cudaError_t launch_init(const SysDev *sys, int s, double sqrt_t_over_m, long long n, void *A, void *B,     \
                             int *key, unsigned *hist, unsigned *err, cudaStream_t st);                          \
+    cudaError_t launch_init_field(const SysDev *sys, int s, double sqrt_t_over_m, long long n, const double *cdf, \
+                                  const float *drift, long long V, void *A, void *B, int *key, unsigned *hist,  \
+                                  unsigned *err, cudaStream_t st);                                              \
+    cudaError_t launch_field_accumulate(const SysDev *sys, int s, const CellArrays &cells,                      \
+                                        const ParticleArrays &parts, int cur, int cin, float4 *field,           \
+                                        cudaStream_t st);                                                       \
     cudaError_t launch_gather(const CellArrays &cells, const ParticleArrays &parts, int cur, int cin, int c0,   \
                               int c1,                                                                           \
                               unsigned nspill, void *A, void *B, int *key, unsigned *hist,                      \

@@ -114,6 +114,86 @@ __global__ void k_init(const SysDev *sys, int s, double sqrt_t_over_m, long long
     }
 }
 
+// Warm start from a field: particle i is placed in voxel w with probability
+// weight[w] / sum(weight) (inverse of the cumulative weights `cdf`, V + 1
+// entries with cdf[0] = 0), uniformly inside it, with velocity drift[w] plus
+// a Maxwellian of sqrt(T/m) per component; stream (id, 0, init) per particle.
+// The field-free counterpart is k_init (System::setup_molecules).
+__global__ void k_init_field(const SysDev *sys, int s, double sqrt_t_over_m, long long n, const double *cdf,
+                             const float *drift, long long V, RecA *A, RecB *B, int *key, unsigned *hist,
+                             unsigned *err) {
+    const SysDev &g = sys[s];
+    const double total = cdf[V];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        DrawStream rs;
+        rs.init(g.seed, (uint32_t)i, 0u, DSMC_TAG_INIT);
+        double v[3], r[3];
+        for (int d = 0; d < 3; ++d) {
+            const double u1 = rs.uniform64();
+            const double u2 = rs.uniform64();
+            v[d] = sqrt(-2.0 * log(1.0 - u1)) * cos(6.283185307 * u2) * sqrt_t_over_m;
+        }
+        // the voxel w with cdf[w] <= u < cdf[w + 1]
+        const double u = rs.uniform64() * total;
+        long long lo = 0, hi = V;
+        while (hi - lo > 1) {
+            const long long mid = (lo + hi) >> 1;
+            if (cdf[mid] <= u) lo = mid; else hi = mid;
+        }
+        const long long w = lo;
+        const int k = (int)(w % g.n[2]), j = (int)((w / g.n[2]) % g.n[1]), ii = (int)(w / ((long long)g.n[1] * g.n[2]));
+        const int c[3] = {ii, j, k};
+        for (int d = 0; d < 3; ++d) {
+            // inside the voxel, away from its faces by a margin of 1e-6 voxel
+            const double f = 1e-6 + (1.0 - 2e-6) * rs.uniform64();
+            r[d] = ((double)c[d] + f) * g.vox_len[d];
+            v[d] += (double)drift[3 * w + d];
+        }
+        if (voxel_type(g, c[0], c[1], c[2]) != DSMC_VOX_EMPTY) atomicOr(err, DSMC_EBIT_RESEED);
+        Particle p;
+        Maker<Prec>::make(g, r, v, (uint32_t)i, p);
+        const int ac = particle_cell(g, p, err);
+        Prec::pack(p, A[i], B[i]);
+        key[i] = ac;
+        if (ac >= 0) atomicAdd(&hist[ac], 1u);
+    }
+}
+
+// Per-voxel sums of one system's particles, added to field[voxel] =
+// {count, sum vx, sum vy, sum vz} (fp32): the steady fields the warm-start
+// surrogate learns, accumulated over many steps.
+__global__ void k_field_accumulate(const SysDev *sys, int s, const CellArrays cells, const ParticleArrays parts, int cur,
+                                   int cin, float4 *field) {
+    const SysDev &g = sys[s];
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const RecA *Ain = reinterpret_cast<const RecA *>(parts.A[cur]);
+    const RecB *Bin = reinterpret_cast<const RecB *>(parts.B[cur]);
+    for (int a = g.active_begin + warp; a < g.active_end; a += nwarps) {
+        const int4 m = cells.meta[a];
+        const unsigned nb = min(cells.bot[cin][a], (unsigned)m.y);
+        const unsigned nt = min(cells.top[cin][a], (unsigned)m.y - nb);
+        for (unsigned q = lane; q < nb + nt; q += 32) {
+            Particle p;
+            const unsigned addr = cell_slot(m.x, m.y, nb, nt, q);
+            Prec::unpack(Ain[addr], Bin[addr], p);
+            double rr[3];
+            Maker<Prec>::position(g, p, rr);
+            int c[3];
+            for (int d = 0; d < 3; ++d) {
+                c[d] = (int)(rr[d] / g.vox_len[d]);
+                c[d] = c[d] < 0 ? 0 : (c[d] >= g.n[d] ? g.n[d] - 1 : c[d]);
+            }
+            float4 *f = field + ((long long)c[0] * g.n[1] + c[1]) * g.n[2] + c[2];
+            atomicAdd(&f->x, 1.0f);
+            atomicAdd(&f->y, (float)p.v[0]);
+            atomicAdd(&f->z, (float)p.v[1]);
+            atomicAdd(&f->w, (float)p.v[2]);
+        }
+    }
+}
+
 // Slots of buffer `cur` (cells [c0, c1)) and the overflow list -> flat records.
 __global__ void k_gather(const CellArrays cells, const ParticleArrays parts, int cur, int cin, int c0, int c1,
                          unsigned nspill, RecA *A, RecB *B, int *key, unsigned *hist, unsigned long long *cursor,
@@ -303,6 +383,20 @@ cudaError_t launch_from_fp64(const SysDev *sys, int s, const double *r, const do
 cudaError_t launch_init(const SysDev *sys, int s, double sqrt_t_over_m, long long n, void *A, void *B, int *key,
                         unsigned *hist, unsigned *err, cudaStream_t st) {
     k_init<<<grid_for(n, 128), 128, 0, st>>>(sys, s, sqrt_t_over_m, n, (RecA *)A, (RecB *)B, key, hist, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_init_field(const SysDev *sys, int s, double sqrt_t_over_m, long long n, const double *cdf,
+                              const float *drift, long long V, void *A, void *B, int *key, unsigned *hist,
+                              unsigned *err, cudaStream_t st) {
+    k_init_field<<<grid_for(n, 128), 128, 0, st>>>(sys, s, sqrt_t_over_m, n, cdf, drift, V, (RecA *)A, (RecB *)B, key,
+                                                    hist, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_field_accumulate(const SysDev *sys, int s, const CellArrays &cells, const ParticleArrays &parts,
+                                    int cur, int cin, float4 *field, cudaStream_t st) {
+    k_field_accumulate<<<148 * 8, 256, 0, st>>>(sys, s, cells, parts, cur, cin, field);
     return cudaGetLastError();
 }
 

@@ -19,8 +19,8 @@ ROOT = Path(__file__).resolve().parents[1]
 GOLDEN = ROOT / "tests" / "golden"
 
 
-def header_functions():
-    text = (ROOT / "include" / "dsmc_b200.h").read_text()
+def header_functions(header="dsmc_b200.h"):
+    text = (ROOT / "include" / header).read_text()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(dsmc_[a-z0-9_]+)\s*\(", text)))
 
@@ -32,6 +32,12 @@ def test_library_exports_every_declared_entry_point():
     for name in names:
         assert hasattr(lib, name), name
     assert set(capi.EXPORTED) == set(names)
+    sg = header_functions("dsmc_surrogate.h")
+    for name in sg:
+        assert hasattr(lib, name), name
+    assert set(capi.EXPORTED_SURROGATE) == set(sg)
+    headers = sorted(p.name for p in (ROOT / "include").glob("*.h"))
+    assert headers == ["dsmc_b200.h", "dsmc_surrogate.h"]
 
 
 def test_settings_defaults_match_python_driver():

@@ -1,0 +1,281 @@
+"""GPU kernels of the warm-start surrogate against CPU references.
+
+Each tcgen05 convolution (forward, input gradient through the packed
+flipped weights, weight gradient), the pooling / upsampling kernels and their
+backward, the head and loss, and Adam are checked against torch's CPU
+operators on the same bf16-rounded inputs; then the whole U-Net's output,
+loss and every parameter gradient against oracle/unet_ref.py, which rounds to
+bf16 at the same points as the GPU path.
+
+Tolerances: a bf16 output differs from the fp32 reference by its rounding
+(relative 2^-8) plus fp32 summation order, so bf16 outputs are held to
+1e-2 of the tensor's largest magnitude elementwise; fp32 outputs (weight and
+bias gradients, head) to 1e-4 relative L2.  Whole-network gradients go
+through ten bf16 roundings of activations and gradients, where an fp32
+accumulation that lands on the other side of a rounding boundary or of a
+ReLU changes one element by one bf16 ulp: they are held to 2e-2 relative L2
+per parameter tensor.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+import torch.nn.functional as F
+
+from master_b200 import capi
+from master_b200 import surrogate as sgm
+
+pytestmark = pytest.mark.gpu
+
+DEV = torch.device("cuda", 0)
+
+
+def lib():
+    return capi.load()
+
+
+def P(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+
+
+def stream():
+    return C.c_void_p(torch.cuda.current_stream(DEV).cuda_stream)
+
+
+def rnd_bf16(shape, gen, scale=1.0):
+    return (torch.randn(shape, generator=gen, dtype=torch.float32) * scale).to(torch.bfloat16)
+
+
+def to_ncdhw(x):
+    """(B, S, S, S, C) -> (B, C, S, S, S) fp64 on the CPU."""
+    return x.detach().cpu().to(torch.float64).permute(0, 4, 1, 2, 3)
+
+
+def torch_weights(w):
+    """(cout, 27, cin) -> conv3d weight (cout, cin, 3, 3, 3)."""
+    cout, _, cin = w.shape
+    return w.reshape(cout, 3, 3, 3, cin).permute(0, 4, 1, 2, 3)
+
+
+def ref_conv(x, w, bias=None):
+    y = F.conv3d(F.pad(x, (1, 1, 1, 1, 1, 1), mode="circular"), torch_weights(w))
+    if bias is not None:
+        y = y + bias.view(1, -1, 1, 1, 1)
+    return y
+
+
+def close_bf16(gpu, ref, tol=1e-2):
+    g = gpu.detach().cpu().to(torch.float64)
+    scale = max(ref.abs().max().item(), 1e-30)
+    err = (g - ref).abs().max().item() / scale
+    assert err <= tol, f"max error {err:.3e} of scale {scale:.3e}"
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+
+
+def sync_ok():
+    torch.cuda.synchronize(DEV)
+    f = C.c_uint()
+    capi.check(lib().dsmc_sg_status(C.byref(f), 1))
+    assert f.value == 0, f"surrogate kernel error flags {f.value:#x}"
+
+
+@pytest.mark.parametrize("cin,cout", [(16, 16), (16, 32), (32, 32), (32, 64), (64, 64), (96, 32), (48, 16),
+                                      (32, 96), (16, 48)])
+def test_conv_forward_matches_torch(cin, cout):
+    g = torch.Generator().manual_seed(cin * 100 + cout)
+    B, S = 2, 16
+    # input as a view into a wider buffer (channel offset 8 of cin + 16)
+    buf = rnd_bf16((B, S, S, S, cin + 16), g)
+    w = rnd_bf16((cout, 27, cin), g, scale=(2.0 / (27 * cin)) ** 0.5)
+    bias = torch.randn(cout, generator=g) * 0.1
+    out = torch.zeros((B, S, S, S, cout + 8), dtype=torch.bfloat16)
+    d_buf, d_w, d_b, d_out = buf.to(DEV), w.to(DEV), bias.to(DEV), out.to(DEV)
+    capi.check(lib().dsmc_sg_conv3(stream(), B, S, P(d_buf), cin + 16, 8, cin, P(d_w), P(d_b), cout, P(d_out),
+                                   cout + 8, 8, 1, None, 0, 0))
+    sync_ok()
+    x = to_ncdhw(buf[..., 8:8 + cin])
+    ref = torch.relu(ref_conv(x, w.to(torch.float64), bias.to(torch.float64)))
+    close_bf16(to_ncdhw(d_out[..., 8:8 + cout]), ref)
+    assert (d_out[..., :8].float() == 0).all()  # channels outside the view untouched
+
+
+def test_conv_mask_and_no_bias():
+    g = torch.Generator().manual_seed(7)
+    B, S, cin, cout = 1, 32, 32, 16
+    x = rnd_bf16((B, S, S, S, cin), g)
+    w = rnd_bf16((cout, 27, cin), g, scale=0.05)
+    mask = rnd_bf16((B, S, S, S, cout), g)
+    out = torch.zeros((B, S, S, S, cout), dtype=torch.bfloat16, device=DEV)
+    dx, dw, dm = x.to(DEV), w.to(DEV), mask.to(DEV)
+    capi.check(lib().dsmc_sg_conv3(stream(), B, S, P(dx), cin, 0, cin, P(dw), None, cout, P(out), cout, 0, 0, P(dm),
+                                   cout, 0))
+    sync_ok()
+    ref = ref_conv(to_ncdhw(x), w.to(torch.float64)) * (to_ncdhw(mask) > 0)
+    close_bf16(to_ncdhw(out), ref)
+
+
+@pytest.mark.parametrize("cin,cout", [(16, 16), (32, 64), (96, 32), (48, 16)])
+def test_conv_input_gradient_through_packed_weights(cin, cout):
+    """dX = conv(dY, w_dgrad): the forward kernel on the weights that
+    dsmc_sg_pack_weights flips and transposes, against torch's autograd."""
+    g = torch.Generator().manual_seed(cin + cout)
+    B, S = 2, 16
+    w32 = torch.randn((cout, 27, cin), generator=g) * 0.05
+    dy = rnd_bf16((B, S, S, S, cout), g)
+    wf = torch.empty(cout * 27 * cin, dtype=torch.int16, device=DEV)
+    wd = torch.empty_like(wf)
+    capi.check(lib().dsmc_sg_pack_weights(stream(), P(w32.to(DEV)), cout, cin, P(wf), P(wd)))
+    dx = torch.zeros((B, S, S, S, cin), dtype=torch.bfloat16, device=DEV)
+    capi.check(lib().dsmc_sg_conv3(stream(), B, S, P(dy.to(DEV)), cout, 0, cout, P(wd), None, cin, P(dx), cin, 0, 0,
+                                   None, 0, 0))
+    sync_ok()
+    wb = w32.to(torch.bfloat16).to(torch.float64)
+    assert torch.equal(wf.view(torch.bfloat16).cpu().to(torch.float64).reshape(cout, 27, cin), wb)
+    x = torch.zeros((B, cin, S, S, S), dtype=torch.float64, requires_grad=True)
+    y = ref_conv(x, wb)
+    y.backward(to_ncdhw(dy))
+    close_bf16(to_ncdhw(dx), x.grad)
+
+
+@pytest.mark.parametrize("cin,cout", [(16, 16), (16, 32), (32, 64), (64, 64), (96, 32), (48, 16)])
+def test_conv_weight_gradient_matches_torch(cin, cout):
+    g = torch.Generator().manual_seed(3 * cin + cout)
+    B, S = 2, 16
+    x = rnd_bf16((B, S, S, S, cin), g)
+    dy = rnd_bf16((B, S, S, S, cout), g)
+    dw = torch.zeros(cout * 27 * cin, dtype=torch.float32, device=DEV)
+    db = torch.zeros(cout, dtype=torch.float32, device=DEV)
+    dxd, dyd = x.to(DEV), dy.to(DEV)
+    capi.check(lib().dsmc_sg_conv3_wgrad(stream(), B, S, P(dyd), cout, 0, cout, P(dxd), cin, 0, cin, P(dw)))
+    capi.check(lib().dsmc_sg_bias_grad(stream(), B, S, P(dyd), cout, 0, cout, P(db)))
+    sync_ok()
+    W = torch.zeros((cout, cin, 3, 3, 3), dtype=torch.float64, requires_grad=True)
+    b = torch.zeros(cout, dtype=torch.float64, requires_grad=True)
+    y = F.conv3d(F.pad(to_ncdhw(x), (1, 1, 1, 1, 1, 1), mode="circular"), W) + b.view(1, -1, 1, 1, 1)
+    y.backward(to_ncdhw(dy))
+    ref = W.grad.permute(0, 2, 3, 4, 1).reshape(cout, 27, cin).numpy()
+    assert rel_l2(dw.cpu().numpy().reshape(cout, 27, cin), ref) <= 1e-4
+    assert rel_l2(db.cpu().numpy(), b.grad.numpy()) <= 1e-4
+
+
+def test_pool_and_upsample_forward_and_backward():
+    g = torch.Generator().manual_seed(11)
+    B, S, Cc = 2, 16, 32
+    x = rnd_bf16((B, S, S, S, Cc), g)
+    act = rnd_bf16((B, S, S, S, Cc), g)
+    skip = rnd_bf16((B, S, S, S, Cc), g)
+    dyp = rnd_bf16((B, S // 2, S // 2, S // 2, Cc), g)
+    L, s = lib(), stream()
+    dx, dact, dskip, ddyp = x.to(DEV), act.to(DEV), skip.to(DEV), dyp.to(DEV)
+    pooled = torch.zeros((B, S // 2, S // 2, S // 2, Cc), dtype=torch.bfloat16, device=DEV)
+    capi.check(L.dsmc_sg_pool2(s, B, S, P(dx), Cc, 0, Cc, P(pooled), Cc, 0))
+    pb = torch.zeros((B, S, S, S, Cc), dtype=torch.bfloat16, device=DEV)
+    capi.check(L.dsmc_sg_pool2_bwd(s, B, S, P(ddyp), Cc, 0, P(dskip), Cc, 0, P(dact), Cc, 0, Cc, P(pb), Cc, 0))
+    up = torch.zeros((B, S, S, S, Cc), dtype=torch.bfloat16, device=DEV)
+    capi.check(L.dsmc_sg_up2(s, B, S, P(ddyp), Cc, 0, Cc, P(up), Cc, 0))
+    ub = torch.zeros((B, S // 2, S // 2, S // 2, Cc), dtype=torch.bfloat16, device=DEV)
+    capi.check(L.dsmc_sg_up2_bwd(s, B, S, P(dx), Cc, 0, None, 0, 0, Cc, P(ub), Cc, 0))
+    sync_ok()
+    X = to_ncdhw(x)
+    close_bf16(to_ncdhw(pooled), F.avg_pool3d(X, 2))
+    upref = to_ncdhw(dyp).repeat_interleave(2, 2).repeat_interleave(2, 3).repeat_interleave(2, 4)
+    assert torch.equal(to_ncdhw(up), upref)
+    close_bf16(to_ncdhw(pb), (to_ncdhw(skip) + upref / 8) * (to_ncdhw(act) > 0))
+    close_bf16(to_ncdhw(ub), F.avg_pool3d(X, 2) * 8)
+
+
+def test_adam_matches_the_published_update():
+    n = 1000
+    g = torch.Generator().manual_seed(5)
+    p0 = torch.randn(n, generator=g)
+    grads = [torch.randn(n, generator=g) for _ in range(3)]
+    p, m, v = p0.to(DEV), torch.zeros(n, device=DEV), torch.zeros(n, device=DEV)
+    for k, gr in enumerate(grads, 1):
+        gd = gr.to(DEV)
+        capi.check(lib().dsmc_sg_adam(stream(), P(p), P(gd), P(m), P(v), n, C.c_float(1e-2), C.c_float(0.9),
+                                      C.c_float(0.999), C.c_float(1e-8), k))
+    torch.cuda.synchronize(DEV)
+    q = p0.clone().to(torch.float64)
+    mm = torch.zeros(n, dtype=torch.float64)
+    vv = torch.zeros(n, dtype=torch.float64)
+    for k, gr in enumerate(grads, 1):
+        gr = gr.to(torch.float64)
+        mm = 0.9 * mm + 0.1 * gr
+        vv = 0.999 * vv + 0.001 * gr * gr
+        q -= 1e-2 * (mm / (1 - 0.9 ** k)) / ((vv / (1 - 0.999 ** k)).sqrt() + 1e-8)
+    assert torch.allclose(p.cpu().to(torch.float64), q, rtol=1e-5, atol=1e-6)
+
+
+def sample_batch(B, S, seed):
+    rng = np.random.default_rng(seed)
+    solid = (rng.random((B, S, S, S)) < 0.35).astype(np.uint8)
+    feature = rng.normal(0, 1, B).astype(np.float32)
+    target = rng.normal(0, 1, (B, S, S, S, 4)).astype(np.float32)
+    valid = (solid == 0).astype(np.uint8)
+    return solid, feature, target, valid
+
+
+def test_unet_forward_backward_matches_cpu_reference():
+    from oracle.unet_ref import UNetRef
+    B, S = 2, 16
+    params = sgm.init_parameters(seed=3)
+    # non-zero biases so every bias path is exercised
+    lay, _ = sgm.parameter_layout()
+    rng = np.random.default_rng(4)
+    for k, (o, sh) in lay.items():
+        if k.endswith(".b"):
+            params[o:o + int(np.prod(sh))] = rng.normal(0, 0.05, int(np.prod(sh)))
+    solid, feature, target, valid = sample_batch(B, S, 9)
+    cw = np.array([1.0, 0.5, 0.25, 0.25], np.float32)
+    net = sgm.UNet(0, params)
+    out = net.forward(torch.tensor(solid, device=DEV), torch.tensor(feature, device=DEV))
+    net.loss_acc.zero_()
+    net.backward(torch.tensor(target, device=DEV), torch.tensor(valid, device=DEV), cw)
+    sync_ok()
+    ref = UNetRef(params, emulate_bf16=True)
+    rout = ref.forward(solid, feature)
+    loss = ref.loss(rout, target, valid, cw)
+    loss.backward()
+    o = out.detach().cpu().numpy()
+    assert rel_l2(o, rout.detach().numpy()) <= 1e-2
+    assert net.loss_acc.item() == pytest.approx(loss.item(), rel=1e-2)
+    gg, rg = net.grads_host(), ref.grads()
+    worst = {k: rel_l2(gg[k], rg[k]) for k in rg}
+    assert max(worst.values()) <= 2e-2, worst
+    # the gradient is the derivative: one step along it lowers the fp64 loss
+    ref2 = UNetRef(params - 1e-3 * net.g.cpu().numpy() / np.linalg.norm(net.g.cpu().numpy()), emulate_bf16=False)
+    l2 = ref2.loss(ref2.forward(solid, feature), target, valid, cw).item()
+    ref3 = UNetRef(params, emulate_bf16=False)
+    l3 = ref3.loss(ref3.forward(solid, feature), target, valid, cw).item()
+    assert l2 < l3
+
+
+def test_training_on_one_batch_lowers_the_loss():
+    B, S = 4, 16
+    solid, feature, _, valid = sample_batch(B, S, 21)
+    # a learnable target: a smooth function of the local openness
+    open_ = 1.0 - solid.astype(np.float32)
+    k = np.ones((3, 3, 3), np.float32) / 27
+    from scipy.ndimage import convolve
+    sm = np.stack([convolve(open_[b], k, mode="wrap") for b in range(B)])
+    target = np.stack([sm, 0.5 * sm, -sm, sm * sm], -1).astype(np.float32)
+    net = sgm.UNet(0, seed=1)
+    d = [torch.tensor(a, device=DEV) for a in (solid, feature, target, valid)]
+    losses = []
+    for it in range(60):
+        net.loss_acc.zero_()
+        net.forward(d[0], d[1])
+        net.backward(d[2], d[3], [1, 1, 1, 1])
+        losses.append(net.loss_acc.item())
+        net.adam(lr=3e-3)
+    sync_ok()
+    assert np.isfinite(losses).all()
+    assert losses[-1] < 0.2 * losses[0], losses[::10]
