@@ -366,6 +366,28 @@ int dsmc_ctx_set_capacity(dsmc_ctx *ctx, double factor, int pad);
  * block of move_cells, and its per-warp staging ring in particles. */
 int dsmc_pass_info(dsmc_ctx *ctx, int *pipelined, int *grid, int *block, int *stage_capacity);
 
+/* Launch tuning of the production pass, for the autotuner
+ * (master_b200/autotune.py): the reference has no counterpart (its stages are
+ * loops over particles on one core).  blocks_per_sm: resident blocks per SM of
+ * collide_cells, move_cells, place_movers, place_walls and sample_cells, each
+ * a persistent grid (0: the most that are resident, the default; larger
+ * values are clamped to it); ring: move_cells' shared-memory staging ring in
+ * particles per warp (0: the smallest that holds the largest cell; larger
+ * rings trade resident blocks for staging depth); collide_claim: how
+ * collide_cells' warps take chunks of 32 cells after their first (0: a
+ * pass-wide counter when each warp has four chunks or more, else a fixed
+ * stride; 1: always the stride; 2: always the counter).  Any setting gives
+ * the same trajectories: only the work distribution changes.
+ * dsmc_tuning_get: the current settings, and in limits the most blocks per SM
+ * of each kernel at the current ring and the ring in use. */
+typedef struct dsmc_tuning {
+    int blocks_per_sm[5];
+    int ring;
+    int collide_claim;
+} dsmc_tuning;
+int dsmc_tuning_set(dsmc_ctx *ctx, const dsmc_tuning *t);
+int dsmc_tuning_get(dsmc_ctx *ctx, dsmc_tuning *current, dsmc_tuning *limits);
+
 /* Per-kernel timers of the production pass, the device-side counterpart of
  * the reference's stage timers (the Moving / Colliding / Accelerating /
  * Sampling lines of its report, dsmc/system.cpp and dsmc/dsmc_io.cpp).  With

@@ -13,7 +13,7 @@
  * `stream` is a cudaStream_t (NULL: the legacy default stream); calls are
  * enqueued and return without synchronising.  Volumes are channels-last
  * bf16 (uint16_t bit patterns) [batch][S][S][S][channels] with S a power of
- * two >= 8, addressed by a channel stride `*_cs` and offset `*_coff` (both
+ * two >= 4 (convolutions: batch*S^3 a multiple of 128), addressed by a channel stride `*_cs` and offset `*_coff` (both
  * multiples of 8, tensors 16-byte aligned), so a channel concatenation is two
  * views of one buffer.  3x3x3 convolutions pad periodically.  Weights of a
  * 3x3x3 layer are [cout][27][cin], tap t = 9*(d0+1) + 3*(d1+1) + (d2+1) for

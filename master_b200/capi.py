@@ -46,7 +46,7 @@ EXPORTED = [
     "dsmc_tocontinue_write", "dsmc_continue_from", "dsmc_checkpoint_save", "dsmc_checkpoint_load",
     "dsmc_profile_sums_get", "dsmc_profiles_finish", "dsmc_profiles_get", "dsmc_measures_get",
     "dsmc_system_add_slab", "dsmc_exchange_take", "dsmc_exchange_put", "dsmc_particles_init_field",
-    "dsmc_field_accumulate",
+    "dsmc_field_accumulate", "dsmc_tuning_set", "dsmc_tuning_get",
 ]
 # every entry point declared in include/dsmc_surrogate.h
 EXPORTED_SURROGATE = [
@@ -54,6 +54,11 @@ EXPORTED_SURROGATE = [
     "dsmc_sg_up2", "dsmc_sg_up2_bwd", "dsmc_sg_pack_input", "dsmc_sg_head", "dsmc_sg_loss_head_bwd",
     "dsmc_sg_adam", "dsmc_sg_pack_weights", "dsmc_sg_status",
 ]
+
+
+class Tuning(C.Structure):
+    """Mirror of dsmc_tuning: launch shape of the production pass."""
+    _fields_ = [("blocks_per_sm", C.c_int * 5), ("ring", C.c_int), ("collide_claim", C.c_int)]
 
 
 class DsmcError(RuntimeError):
@@ -186,6 +191,8 @@ def load() -> C.CDLL:
         "dsmc_exchange_put": [_P, C.c_int, C.c_int64, C.c_void_p, C.c_int],
         "dsmc_particles_init_field": [_P, C.c_int, C.c_int64, C.c_void_p, C.c_void_p, C.c_int],
         "dsmc_field_accumulate": [_P, C.c_int, C.c_void_p, C.c_int],
+        "dsmc_tuning_set": [_P, C.POINTER(Tuning)],
+        "dsmc_tuning_get": [_P, C.POINTER(Tuning), C.POINTER(Tuning)],
         "dsmc_profiles_finish": [C.POINTER(Settings), C.c_double, C.c_int, _D, _D, _D, _D, _D, _D, _D],
         "dsmc_profiles_get": [_P, C.c_int, C.c_int, _D, _D, _D, _D, _D, _D, C.POINTER(C.c_int)],
         "dsmc_cells_layout": [C.POINTER(Settings), C.c_uint32, C.c_uint32, C.c_uint32, _U8, C.c_int, _I32, _I32,

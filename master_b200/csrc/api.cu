@@ -142,6 +142,12 @@ struct dsmc_ctx {
     int block = 256;
     int grid = 0;
     int fused_grids[5] = {0, 0, 0, 0, 0};  // production pass (collide, move, place, walls, sample); 0 = not usable
+    int fused_max_bps[5] = {0, 0, 0, 0, 0};  // the most resident blocks per SM of each at the current ring
+    // launch tuning (dsmc_tuning_set): blocks per SM of each production
+    // kernel (0: the most resident), move_cells ring, collide chunk claims
+    int tune_bps[5] = {0, 0, 0, 0, 0};
+    int tune_ring = 0;
+    int tune_claim = 0;
     bool use_pipelined = true;
     // per-kernel timers of the production pass (dsmc_ctx_set_timing)
     bool timing = false;
@@ -237,6 +243,21 @@ Status read_status(dsmc_ctx *ctx, cudaError_t *err) {
 
 // Rebuilds every cell table and slot buffer from flat staged particles.
 // fA/fB/fkey hold `total` records; hist holds per-cell counts.
+// Grids of the production pass: the most resident blocks per SM of each
+// kernel, or the tuned count when one is set (never above the most).
+void apply_launch_shape(dsmc_ctx *ctx) {
+    for (int &gsz : ctx->fused_grids) gsz = 0;
+    for (int &b : ctx->fused_max_bps) b = 0;
+    if (is_fp64(ctx) || split32::fused_capacity(ctx->smem_cap) <= 0) return;
+    if (!split32::fused_grids(ctx->smem_cap, ctx->num_sms, ctx->fused_grids, ctx->tune_ring, ctx->fused_max_bps)) {
+        for (int &gsz : ctx->fused_grids) gsz = 0;
+        return;
+    }
+    for (int k = 0; k < 5; ++k)
+        if (ctx->tune_bps[k] > 0)
+            ctx->fused_grids[k] = std::min(ctx->tune_bps[k], ctx->fused_max_bps[k]) * ctx->num_sms;
+}
+
 int relayout(dsmc_ctx *ctx, long long total) {
     ctx->drop_graphs();  // slot buffers and grids may change
     const int C = ctx->num_cells;
@@ -300,9 +321,7 @@ int relayout(dsmc_ctx *ctx, long long total) {
                                     : split32::pass_blocks_per_sm(PASS_SORT, ctx->block, ctx->smem_cap);
     if (bps_in <= 0 || bps_so <= 0) return fail(ctx, DSMC_ERR_CUDA, "stage passes cannot be resident (shared memory)");
     ctx->grid = bps * ctx->num_sms;
-    for (int &gsz : ctx->fused_grids) gsz = 0;
-    if (!is_fp64(ctx) && split32::fused_capacity(ctx->smem_cap) > 0)
-        split32::fused_grids(ctx->smem_cap, ctx->num_sms, ctx->fused_grids);
+    apply_launch_shape(ctx);
     Status st;
     cudaError_t e;
     st = read_status(ctx, &e);
@@ -398,6 +417,8 @@ PassParams pass_params(dsmc_ctx *ctx, int do_collide, int do_move, int do_sample
     P.do_sample = do_sample;
     P.smem_cap = ctx->smem_cap;
     P.advance_step = advance;
+    P.ring = ctx->tune_ring;
+    P.claim = ctx->tune_claim;
     return P;
 }
 
@@ -1775,6 +1796,38 @@ int dsmc_pass_times_get(dsmc_ctx *ctx, double ms[4], int64_t *passes) {
     if (!ctx || !ms) return DSMC_ERR_ARG;
     for (int k = 0; k < 4; ++k) ms[k] = ctx->tms[k];
     if (passes) *passes = ctx->tpasses;
+    return DSMC_OK;
+}
+
+int dsmc_tuning_set(dsmc_ctx *ctx, const dsmc_tuning *t) {
+    if (!ctx || !t) return DSMC_ERR_ARG;
+    for (int k = 0; k < 5; ++k)
+        if (t->blocks_per_sm[k] < 0 || t->blocks_per_sm[k] > 64) return fail(ctx, DSMC_ERR_ARG, "blocks per SM out of range");
+    if (t->ring < 0 || t->ring > split32::max_ring()) return fail(ctx, DSMC_ERR_ARG, "ring out of range");
+    if (t->collide_claim < 0 || t->collide_claim > 2) return fail(ctx, DSMC_ERR_ARG, "collide_claim is 0, 1 or 2");
+    cudaSetDevice(ctx->device);
+    int rc = flush_pending(ctx);
+    if (rc) return rc;
+    for (int k = 0; k < 5; ++k) ctx->tune_bps[k] = t->blocks_per_sm[k];
+    ctx->tune_ring = t->ring;
+    ctx->tune_claim = t->collide_claim;
+    ctx->drop_graphs();  // the grids are baked into the captured passes
+    apply_launch_shape(ctx);
+    return DSMC_OK;
+}
+
+int dsmc_tuning_get(dsmc_ctx *ctx, dsmc_tuning *current, dsmc_tuning *limits) {
+    if (!ctx) return DSMC_ERR_ARG;
+    if (current) {
+        for (int k = 0; k < 5; ++k) current->blocks_per_sm[k] = ctx->tune_bps[k];
+        current->ring = ctx->tune_ring;
+        current->collide_claim = ctx->tune_claim;
+    }
+    if (limits) {
+        for (int k = 0; k < 5; ++k) limits->blocks_per_sm[k] = ctx->fused_max_bps[k];
+        limits->ring = is_fp64(ctx) ? 0 : split32::ring_for(ctx->smem_cap, ctx->tune_ring);
+        limits->collide_claim = 2;
+    }
     return DSMC_OK;
 }
 

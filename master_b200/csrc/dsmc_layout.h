@@ -178,6 +178,8 @@ struct PassParams {
     int do_sample;             // sample after the collide, on the reference's cadence
     int smem_cap;              // staging capacity per warp (particles)
     int advance_step;          // increment Status::step at the end of the pass
+    int ring;                  // production pass: move_cells ring slots per warp (0: the smallest that fits)
+    int claim;                 // production pass: collide_cells chunk claims (0 auto, 1 stride, 2 counter)
 };
 
 }  // namespace dsmc

@@ -45,10 +45,16 @@ DSMC_DECLARE_LAUNCHERS(fp64)
 namespace split32 {
 // the production pass (split_pass.cuh)
 int fused_capacity(int smem_cap);   // move_cells ring slots per warp; 0: the production pass cannot run
+// The ring move_cells runs with: the smallest ring of at least max(ring,
+// fused_capacity(smem_cap)) slots (0: none).
+int ring_for(int smem_cap, int ring);
+// The largest ring this build has.
+int max_ring();
 int fused_block();                  // threads per block of the production kernels
 // Persistent grids of collide_cells, move_cells, place_movers, place_walls
 // and sample_cells; 0 when one of them cannot be resident.
-int fused_grids(int smem_cap, int num_sms, int grids[5]);
+// ring: as ring_for.  max_bps (may be null): the most blocks per SM of each.
+int fused_grids(int smem_cap, int num_sms, int grids[5], int ring = 0, int max_bps[5] = nullptr);
 // ev: null, or five events recorded before each kernel and after the last
 // (the sampler, on sampled steps, falls in the collide interval)
 cudaError_t launch_fused(const PassParams &P, const int grids[5], cudaStream_t st, cudaEvent_t *ev = nullptr);

@@ -51,13 +51,25 @@ int fused_capacity(int smem_cap) {
     return 0;
 }
 
+int ring_for(int smem_cap, int ring) {
+    static const int rings[] = {64, 96, 128, 160, 192, 224, 256, 320, 384, 448, 512};
+    const int need = fused_capacity(smem_cap);
+    if (need <= 0) return 0;
+    const int want = std::max(need, ring);
+    for (int r : rings)
+        if (want <= r) return r;
+    return 0;
+}
+
+int max_ring() { return 512; }
+
 int fused_block() { return 32 * pass3::M_WARPS; }
 
 #define DSMC_MOVE_RINGS(X) X(64) X(96) X(128) X(160) X(192) X(224) X(256) X(320) X(384) X(448) X(512)
 
-int fused_grids(int smem_cap, int num_sms, int grids[5]) {
+int fused_grids(int smem_cap, int num_sms, int grids[5], int ring, int max_bps[5]) {
     int bm = 0;
-    switch (fused_capacity(smem_cap)) {
+    switch (ring_for(smem_cap, ring)) {
 #define X(r) \
     case r: bm = move_ring_blocks<r>(); break;
         DSMC_MOVE_RINGS(X)
@@ -74,13 +86,22 @@ int fused_grids(int smem_cap, int num_sms, int grids[5]) {
     grids[2] = bp * num_sms;
     grids[3] = bw * num_sms;
     grids[4] = bs * num_sms;
+    if (max_bps) {
+        max_bps[0] = bc;
+        max_bps[1] = bm;
+        max_bps[2] = bp;
+        max_bps[3] = bw;
+        max_bps[4] = bs;
+    }
     return 1;
 }
 
 // collide_cells with the chunk counter when each warp has many chunks
 static void launch_collide_cells(const PassParams &P, int grid, cudaStream_t st) {
     const long long nchunks = (P.cells.num_cells + 31) / 32;
-    if (nchunks >= (long long)pass3::CLAIM_MIN_CHUNKS_PER_WARP * grid * pass3::C_WARPS)
+    const bool counter = P.claim == 2 ||
+                         (P.claim == 0 && nchunks >= (long long)pass3::CLAIM_MIN_CHUNKS_PER_WARP * grid * pass3::C_WARPS);
+    if (counter)
         pass3::collide_cells_kernel<true><<<grid, 32 * pass3::C_WARPS, 0, st>>>(P);
     else
         pass3::collide_cells_kernel<false><<<grid, 32 * pass3::C_WARPS, 0, st>>>(P);
@@ -100,7 +121,7 @@ cudaError_t launch_fused(const PassParams &P, const int grids[5], cudaStream_t s
     }
     if (ev) cudaEventRecord(ev[1], st);
     cudaError_t e = cudaErrorInvalidValue;
-    switch (fused_capacity(P.smem_cap)) {
+    switch (ring_for(P.smem_cap, P.ring)) {
 #define X(r) \
     case r: e = launch_move_ring<r>(P, grids[1], st); break;
         DSMC_MOVE_RINGS(X)

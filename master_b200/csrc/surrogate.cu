@@ -720,7 +720,8 @@ int dsmc_sg_conv3(void *stream, int batch, int S, const uint16_t *in, int in_cs,
                   const uint16_t *w, const float *bias, int cout, uint16_t *out, int out_cs, int out_coff, int relu,
                   const uint16_t *mask, int mask_cs, int mask_coff) {
     const int lg = lg2_of(S);
-    if (lg < 3 || batch < 1 || !in || !w || !out) return sg_fail(DSMC_ERR_ARG, "conv3: bad shape or pointer");
+    if (lg < 2 || batch < 1 || !in || !w || !out || (((long long)batch << (3 * lg)) & 127))
+        return sg_fail(DSMC_ERR_ARG, "conv3: bad shape (S a power of two >= 4, batch*S^3 a multiple of 128) or pointer");
     if (cin % 16 || cin < 16 || cin > 256 || in_cs % 8 || in_coff % 8 || out_cs % 8 || out_coff % 8 ||
         (mask && (mask_cs % 8 || mask_coff % 8 || mask_coff + cout > mask_cs)) || in_coff + cin > in_cs ||
         out_coff + cout > out_cs)
@@ -752,7 +753,8 @@ int dsmc_sg_conv3(void *stream, int batch, int S, const uint16_t *in, int in_cs,
 int dsmc_sg_conv3_wgrad(void *stream, int batch, int S, const uint16_t *dy, int dy_cs, int dy_coff, int cout,
                         const uint16_t *x, int x_cs, int x_coff, int cin, float *dw) {
     const int lg = lg2_of(S);
-    if (lg < 3 || batch < 1 || !dy || !x || !dw) return sg_fail(DSMC_ERR_ARG, "wgrad: bad shape or pointer");
+    if (lg < 2 || batch < 1 || !dy || !x || !dw || (((long long)batch << (3 * lg)) & 63))
+        return sg_fail(DSMC_ERR_ARG, "wgrad: bad shape (S a power of two >= 4, batch*S^3 a multiple of 64) or pointer");
     if (cout % 16 || cout < 16 || cout > 256 || dy_cs % 8 || dy_coff % 8 || x_cs % 8 || x_coff % 8 ||
         dy_coff + cout > dy_cs || x_coff + cin > x_cs)
         return sg_fail(DSMC_ERR_ARG, "wgrad: channels, strides and offsets must be multiples of 8 (cout of 16)");

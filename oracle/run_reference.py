@@ -244,7 +244,7 @@ def parse_report(text: str) -> dict:
 
 
 def run_replicas(settings, geometry, timesteps: int, replicas: int, seeds=None, workdir: Path | None = None,
-                 timeout: float = 600.0, world_dir: Path | None = None) -> dict:
+                 timeout: float = 600.0, world_dir: Path | None = None, workers: int | None = None) -> dict:
     """Runs `replicas` single-rank reference solvers in parallel on one world.
     Returns per-replica reports plus the summed particle-steps per second of
     the timestep stages (moving + colliding + accelerating + sampling).
@@ -279,7 +279,7 @@ def run_replicas(settings, geometry, timesteps: int, replicas: int, seeds=None, 
             rep["stdout_tail"] = res.stdout[-4000:]
             return rep
 
-        with ThreadPoolExecutor(max_workers=replicas) as ex:
+        with ThreadPoolExecutor(max_workers=min(replicas, workers or replicas)) as ex:
             reports = list(ex.map(one, range(replicas)))
     finally:
         if own:

@@ -16,11 +16,19 @@ reproduce within ensemble 95 % confidence intervals
 Both codes start from a Maxwellian at rest in the empty voxels, so the whole
 run, transient included, is compared.
 
+A second, longer ensemble ("flux_window") pins the number flow rate itself:
+FLUX_REPLICAS runs of FLUX_STEPS steps sampled every FLUX_INTERVAL steps.
+The reference prints the cumulative rate F(t) = F_N count_periodic / t
+(MeasureNumberFlowRate::update, dsmc/statisticalproperty.cpp:87-101), so the
+rate over the window [FLUX_FROM, FLUX_STEPS], past the transient, is the
+difference (F(t2) t2 - F(t1) t1) / (t2 - t1) of two printed values.
+
     python tests/golden/make_ensemble.py
 """
 from __future__ import annotations
 
 import json
+import os
 import sys
 import tempfile
 from pathlib import Path
@@ -43,11 +51,36 @@ WORKLOAD = workloads.Workload("ensemble_32", n=32, radius_voxels=3, porosity=0.6
 STEPS = 400
 INTERVAL = 10
 REPLICAS = 16
+FLUX_REPLICAS = 128
+FLUX_STEPS = 3000
+FLUX_INTERVAL = 500
+FLUX_FROM = 1000
 
 
 def summarize(rows):
     a = np.asarray(rows, np.float64)
     return {"mean": a.mean(axis=0).tolist(), "std": a.std(axis=0, ddof=1).tolist(), "n": int(a.shape[0])}
+
+
+def flux_window(g):
+    """Windowed number flow rate of FLUX_REPLICAS long reference runs."""
+    s = WORKLOAD.settings(statistics_interval=FLUX_INTERVAL)
+    seeds = list(range(1001, 1001 + FLUX_REPLICAS))
+    rates = []
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        run_reference.run_replicas(s, g, timesteps=FLUX_STEPS, replicas=FLUX_REPLICAS, seeds=seeds, workdir=d,
+                                   timeout=3600, workers=os.cpu_count())
+        for i in range(FLUX_REPLICAS):
+            rows = [ln.split() for ln in (d / f"r{i:03d}" / "statistics" / "number_flow_rate.txt").read_text()
+                    .splitlines() if ln.strip()]
+            # one line per sample, at steps FLUX_INTERVAL, 2 FLUX_INTERVAL, ...
+            F = {FLUX_INTERVAL * (k + 1): float(r[1]) for k, r in enumerate(rows)}
+            t1, t2 = FLUX_FROM, FLUX_STEPS
+            rates.append((F[t2] * t2 - F[t1] * t1) / (t2 - t1))
+    r = np.asarray(rates)
+    return {"replicas": FLUX_REPLICAS, "steps": FLUX_STEPS, "from": FLUX_FROM, "interval": FLUX_INTERVAL,
+            "seeds": seeds, "mean": float(r.mean()), "std": float(r.std(ddof=1)), "n": int(r.size)}
 
 
 def main():
@@ -81,6 +114,7 @@ def main():
         "profile_temperature_K": summarize(prof_T),
         "profile_velocity_z": summarize(prof_vz),
     }
+    out["flux_window"] = flux_window(g)
     OUT.write_text(json.dumps(out, indent=1) + "\n")
     for k, v in out["scalars"].items():
         print(k, v["mean"], "+-", v["std"])
