@@ -251,6 +251,65 @@ def run_reference_arm(args, world, rank, pg):
     return 0
 
 
+def _timed_steps(ctx, steps: int) -> float:
+    """Milliseconds of `steps` timesteps of a context, CUDA events on its stream."""
+    import torch
+    from master_b200 import capi
+    lib = capi.load()
+    st = torch.cuda.ExternalStream(lib.dsmc_stream(ctx.handle))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    ctx.sync()
+    e0.record(st)
+    ctx.step(steps)
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def other_configs(args, device):
+    """The plain-DSMC configuration (packed_64: 64^3, r = 4, porosity 0.6,
+    ~3.9e5 particles) in the fp64 reference arithmetic and in split
+    precision, and the batched ensemble (64 packed-sphere geometries of edges
+    32-128, porosity 0.4-0.8, radius 3-8, Knudsen 0.1-10, one context, one
+    launch per stage), each timed over `steps` steps after a warm-up."""
+    from master_b200 import capi, fields, workloads
+    from master_b200.system import System
+    out = {}
+    w = workloads.PACKED_64
+    g = w.geometry()
+    for name, prec in (("packed_64_fp64", capi.PREC_FP64), ("packed_64_split", capi.PREC_SPLIT32)):
+        S = System(w.settings(rng_seed=5, statistics_interval=100), g, device=device, precision=prec)
+        S.step(max(args.warmup, 3))
+        k = 100
+        ms = _timed_steps(S.ctx, k)
+        out[name] = {"value": S.num_molecules * k / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / k, "steps": k,
+                     "particles": S.num_molecules, "dtype": "f64" if prec == capi.PREC_FP64 else
+                     "fp32 state + fp64 tallies"}
+        S.ctx.close()
+    # batched ensemble of uneven geometries
+    rng = np.random.default_rng(3)
+    specs = fields.random_specs(64, 32, seed=3, per_cell=30.0)
+    for sp in specs:
+        sp.n = int(rng.choice([32, 48, 64, 96, 128]))
+    ens = fields.Ensemble(specs, device=device, rng_seed=77)
+    ens.ctx.step(max(args.warmup, 3))
+    k = 20
+    ms = _timed_steps(ens.ctx, k)
+    counts = [S.num_molecules for S in ens.systems]
+    by_edge = {}
+    for sp, c in zip(specs, counts):
+        by_edge.setdefault(str(sp.n), []).append(c)
+    out["batched_64_uneven"] = {
+        "value": sum(counts) * k / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / k, "steps": k,
+        "systems": len(counts), "particles": sum(counts), "particles_min": min(counts), "particles_max": max(counts),
+        "particles_by_edge": {e: sum(v) for e, v in sorted(by_edge.items(), key=lambda kv: int(kv[0]))},
+        "systems_by_edge": {e: len(v) for e, v in sorted(by_edge.items(), key=lambda kv: int(kv[0]))},
+        "launches_per_step": 4, "error_bits": ens.ctx.device_status()[0]}
+    ens.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -262,6 +321,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--ref-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--no-configs", action="store_true", help="skip the packed_64 and batched-ensemble lines")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -291,6 +352,21 @@ def main():
     # warm-up (untimed)
     system.step(args.warmup)
     system.ctx.sync()
+    # launch shapes from the project's autotuner (trial passes are ordinary
+    # untimed timesteps of this workload; the cache is applied when present)
+    tuning = None
+    if not args.no_tune and system.ctx.pass_info()["pipelined"] == 1:
+        from master_b200 import autotune
+        cached = autotune.apply_cached(system.ctx)
+        if cached is not None:
+            tuning = {"source": "cache", "choice": cached["choice"]}
+        else:
+            rep = autotune.tune(system.ctx, steps=10, repeats=3)
+            tuning = {"source": "tuned here", "choice": rep["choice"], "default_ms_per_step": rep["default_ms"]["step"],
+                      "chosen_ms_per_step": rep["chosen_ms"]["step"], "trials": len(rep["trials"])}
+        system.step(3)
+        system.ctx.sync()
+    step_before = int(system.tallies().step)
 
     # ---- device-resident throughput ---------------------------------------
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -306,6 +382,7 @@ def main():
         torch.cuda.synchronize()
         barrier(pg)
     clocks = clk.summary()
+    step_after = int(system.tallies().step)
     ms_rank = ev0.elapsed_time(ev1)
     ms_max = allreduce_max(pg, ms_rank)
     n_total = allreduce_sum(pg, float(N))
@@ -324,6 +401,19 @@ def main():
         system.ctx.set_timing(False)
         kernels = {k: pt[k] / pt["passes"] for k in ("collide_cells", "move_cells", "place_movers", "place_walls")}
         kernels["passes"] = pt["passes"]
+    # ---- one whole sampler cadence (statistics_interval steps, one of them
+    # sampled: sample_cells runs after its collide) -------------------------
+    cad = settings.statistics_interval
+    c0 = torch.cuda.Event(enable_timing=True)
+    c1 = torch.cuda.Event(enable_timing=True)
+    system.ctx.sync()
+    c0.record(stream)
+    system.step(cad)
+    c1.record(stream)
+    c1.synchronize()
+    cad_ms = c0.elapsed_time(c1)
+    cadence = {"steps": cad, "sampled_steps": 1, "ms_per_step": cad_ms / cad, "value": N * cad / (cad_ms / 1e3),
+               "sampled_step_extra_ms": cad_ms - cad * (ms_rank / args.steps)}
     tal = system.tallies()
 
     # ---- end to end through the C ABI with host buffers --------------------
@@ -356,6 +446,21 @@ def main():
     e2e_s = time.perf_counter() - t0
     e2e_s = allreduce_max(pg, e2e_s)
     e2e_value = n_total * k_e2e / e2e_s
+
+    # the same with K steps per upload/download for a longer K: the state
+    # crosses PCIe once each way per K steps, so e2e rises with K
+    k_long = max(200, k_e2e)
+    barrier(pg)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    system.ctx.check(lib.dsmc_particles_set(system.ctx.handle, system.id, N, C.cast(r_pin.data_ptr(), D),
+                                            C.cast(v_pin.data_ptr(), D)))
+    for _ in range(k_long):
+        system.ctx.check(lib.dsmc_step(system.ctx.handle, 1))
+        system.ctx.check(lib.dsmc_counters_get(system.ctx.handle, system.id, counters))
+    system.ctx.check(lib.dsmc_particles_get(system.ctx.handle, system.id, N, C.cast(r_out.data_ptr(), D),
+                                            C.cast(v_out.data_ptr(), D), None, C.byref(got)))
+    e2e_long_s = allreduce_max(pg, time.perf_counter() - t0)
 
     # ---- roofline of the dominant kernel: move_cells streams every particle
     # record in and out once (32 B read + 32 B written per particle-step) ----
@@ -394,24 +499,31 @@ def main():
                      "algorithmic_bytes_per_launch": BYTES_PER_PARTICLE_STEP * N},
         "kernels_ms": kernels,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48 * N / k_e2e,
-                "d2h_bytes_per_step": (48 * N + 64 * k_e2e) / k_e2e, "steps": k_e2e},
+                "d2h_bytes_per_step": (48 * N + 64 * k_e2e) / k_e2e, "steps": k_e2e,
+                "note": "K dsmc_step(1) calls between one upload and one download of the fp64 state; rises with K"},
+        "e2e_long": {"value": n_total * k_long / e2e_long_s, "unit": UNIT, "steps": k_long,
+                     "h2d_bytes_per_step": 48 * N / k_long, "d2h_bytes_per_step": (48 * N + 64 * k_long) / k_long},
+        "cadence": cadence,
+        "tuning": tuning,
         # collide_cells + move_cells + place_movers + place_walls per step
         # (production pass) and sample_cells on the sampled steps the timed
         # passes collide; one pass kernel per step otherwise
         "gpu_launches": args.steps * (4 if pipelined else 1) + (sum(
-            1 for st in range(args.warmup, args.warmup + args.steps)
+            1 for st in range(step_before, step_after)
             if st > 0 and st % settings.statistics_interval == 0) if pipelined else 0),
         "clocks": clocks,
         "device_status": {"error_bits": err, "spill": spill},
         "pass": system.ctx.pass_info(),
         "physics": physics,
     }
+    system.ctx.close()
+    if rank == 0 and world == 1 and not args.no_configs:
+        line["configs"] = other_configs(args, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_reference_sample(steps=args.cpu_steps)
         except Exception as e:  # noqa: BLE001
             line["cpu_baseline"] = {"value": None, "unavailable": str(e)}
-    system.ctx.close()
     if rank == 0:
         print(json.dumps(line))
     if pg is not None:

@@ -78,3 +78,31 @@ def test_profiles_within_confidence_intervals(ours, key, idx):
     ok = overlap(prof.mean(0), prof.std(0, ddof=1), prof.shape[0], r["mean"], r["std"], r["n"])
     # independent bins: allow one of sixteen outside its interval by chance
     assert (~ok).sum() <= 1, (key, np.flatnonzero(~ok))
+
+
+def test_windowed_flux_matches_the_reference_ensemble():
+    """The number flow rate past the transient (steps 1000-3000) of 128
+    independent runs against the reference solver's own 128 runs
+    (tests/golden/ensemble_ref.json "flux_window", differenced from its
+    cumulative rate): the two means must agree within a two-sample 95 %
+    interval (about 13 % of the flux here), which an x flux off by a sign,
+    a factor or a lost crossing tally fails."""
+    from master_b200 import steady
+    fw = REF["flux_window"]
+    wl = REF["workload"]
+    w = workloads.Workload(wl["name"], n=wl["n"], radius_voxels=wl["radius_voxels"], porosity=wl["porosity"],
+                           geometry_seed=wl["geometry_seed"], cells=wl["cells"],
+                           atoms_per_molecule=wl["atoms_per_molecule"])
+    g = w.geometry()
+    ctx = Context(0)
+    systems = [System(w.settings(rng_seed=9000 + k, statistics_interval=10 ** 9), g, context=ctx)
+               for k in range(fw["replicas"])]
+    counts = steady.run_counts(ctx, systems, fw["steps"], fw["interval"])
+    s = systems[0].settings
+    i1 = fw["from"] // fw["interval"]
+    rate = s.atoms_per_molecule * (counts[-1] - counts[i1]) / ((fw["steps"] - fw["from"]) * s.dt)
+    se = np.hypot(rate.std(ddof=1) / np.sqrt(rate.size), fw["std"] / np.sqrt(fw["n"]))
+    assert abs(rate.mean() - fw["mean"]) <= Z95 * se, (rate.mean(), fw["mean"], se)
+    # and the interval is tight enough to mean something
+    assert Z95 * se < 0.2 * abs(fw["mean"])
+    ctx.close()
