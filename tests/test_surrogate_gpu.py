@@ -11,10 +11,11 @@ Tolerances: a bf16 output differs from the fp32 reference by its rounding
 (relative 2^-8) plus fp32 summation order, so bf16 outputs are held to
 1e-2 of the tensor's largest magnitude elementwise; fp32 outputs (weight and
 bias gradients, head) to 1e-4 relative L2.  Whole-network gradients go
-through ten bf16 roundings of activations and gradients, where an fp32
-accumulation that lands on the other side of a rounding boundary or of a
-ReLU changes one element by one bf16 ulp: they are held to 2e-2 relative L2
-per parameter tensor.
+through ten bf16 roundings of activations and gradients: bf16 alone moves
+them 1-9 % (relative L2 per tensor) from the exact fp64 gradient; the
+emulating reference reproduces most of that, and the GPU's distance to it
+must stay below 0.6 of that bf16 effect per tensor, with a cosine
+similarity of the whole gradient of at least 0.999.
 """
 from __future__ import annotations
 
@@ -248,8 +249,19 @@ def test_unet_forward_backward_matches_cpu_reference():
     assert rel_l2(o, rout.detach().numpy()) <= 1e-2
     assert net.loss_acc.item() == pytest.approx(loss.item(), rel=1e-2)
     gg, rg = net.grads_host(), ref.grads()
-    worst = {k: rel_l2(gg[k], rg[k]) for k in rg}
-    assert max(worst.values()) <= 2e-2, worst
+    # bf16 itself moves the gradient by 1-9 % from the exact fp64 one; the
+    # emulating reference reproduces most of that, and what is left (an fp32
+    # sum on the other side of a rounding boundary, compounded through the
+    # backward chain) must stay well inside it
+    exact = UNetRef(params, emulate_bf16=False)
+    exact.loss(exact.forward(solid, feature), target, valid, cw).backward()
+    eg = exact.grads()
+    for k in rg:
+        e_gpu, e_bf16 = rel_l2(gg[k], rg[k]), rel_l2(rg[k], eg[k])
+        assert e_gpu <= max(0.6 * e_bf16, 2e-3), (k, e_gpu, e_bf16)
+    flat_g = np.concatenate([gg[k].ravel() for k in rg])
+    flat_r = np.concatenate([rg[k].ravel() for k in rg])
+    assert flat_g @ flat_r / (np.linalg.norm(flat_g) * np.linalg.norm(flat_r)) >= 0.999
     # the gradient is the derivative: one step along it lowers the fp64 loss
     ref2 = UNetRef(params - 1e-3 * net.g.cpu().numpy() / np.linalg.norm(net.g.cpu().numpy()), emulate_bf16=False)
     l2 = ref2.loss(ref2.forward(solid, feature), target, valid, cw).item()
