@@ -310,6 +310,29 @@ def other_configs(args, device):
     return out
 
 
+def surrogate_line(device):
+    """The warm-start surrogate's training step (batch 8 of 64^3 boxes) and
+    its convolutions on the tensor cores, against the measured dense bf16
+    peak: the dominant convolution by time is the roofline kernel."""
+    from master_b200 import surrogate
+    b = surrogate.benchmark(batch=8, S=64, repeats=5, device=device)
+    peak = None
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            peak = float(json.loads(p.read_text())["bf16_tflops"])
+        except Exception:
+            peak = None
+    kind = "measured" if peak else "fallback"
+    peak = peak or 1590.0
+    top = max(((n, k, v) for n, L in b["layers"].items() for k, v in L.items() if isinstance(v, dict)),
+              key=lambda x: x[2]["ms"])
+    b["roofline"] = {"bound": "tensor", "kernel": f"conv3 {top[0]} {top[1]}", "achieved": top[2]["tflops"],
+                     "peak": peak, "unit": "TFLOP/s", "frac": top[2]["tflops"] / peak, "peak_kind": kind}
+    b["train_step_frac_of_peak"] = b["train_step_tflops"] / peak
+    return b
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -519,6 +542,10 @@ def main():
     system.ctx.close()
     if rank == 0 and world == 1 and not args.no_configs:
         line["configs"] = other_configs(args, local)
+        try:
+            line["surrogate"] = surrogate_line(local)
+        except Exception as e:  # noqa: BLE001
+            line["surrogate"] = {"unavailable": str(e)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_reference_sample(steps=args.cpu_steps)

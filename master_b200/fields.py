@@ -95,12 +95,12 @@ class Ensemble:
     """Geometries of a field set as systems of one context (one launch per stage)."""
 
     def __init__(self, specs: list[PackSpec], device: int = 0, rng_seed: int = 1, precision=capi.PREC_SPLIT32,
-                 cold: bool = True):
+                 cold: bool = True, geoms: list | None = None):
         self.specs = specs
         self.ctx = Context(device, precision)
         self.geoms, self.systems, self.settings = [], [], []
         for i, sp in enumerate(specs):
-            g = sp.geometry()
+            g = geoms[i] if geoms is not None else sp.geometry()
             w = sp.workload(g)
             s = w.settings(rng_seed=rng_seed + i, statistics_interval=10 ** 9)
             self.geoms.append(g)
