@@ -11,7 +11,8 @@ are keyed by particle id and cell index, not by rank, so a run over slabs
 takes the same trajectory as the same geometry on one GPU.
 
 Transports: `exchange_dist` over a torch.distributed group (nccl with the
-records on the GPU, gloo through the host); `step_local` drives several
+records on the GPU from the take to the put, their owners computed there;
+gloo through the host); `step_local` drives several
 slabs held by one process (one GPU or several) in lock step.
 """
 from __future__ import annotations
@@ -102,6 +103,17 @@ class Slab:
         cx = (rec[:, 0] & VOXEL_I_MASK).astype(np.int64) // self.voxels_per_cell_x
         return self.owner[cx]
 
+    def destinations_device(self, records):
+        """destinations() on the device: records is an (n, 8) int32 tensor on
+        the context's GPU; returns an int64 tensor there (no host copy)."""
+        import torch
+        own = getattr(self, "_owner_dev", None)
+        if own is None or own.device != records.device:
+            own = torch.as_tensor(self.owner, dtype=torch.int64, device=records.device)
+            self._owner_dev = own
+        cx = torch.bitwise_and(records[:, 0], VOXEL_I_MASK).to(torch.int64) // self.voxels_per_cell_x
+        return own[cx]
+
     def step_dist(self, pg, n: int = 1) -> None:
         """n steps of this rank's slab, exchanging over `pg` after each."""
         for _ in range(n):
@@ -120,10 +132,10 @@ def exchange_dist(pg, slab: Slab) -> int:
         raise ValueError("the group's size differs from the slab count")
     on_gpu = pg.get_backend() == "nccl"
     if on_gpu:
+        # the records stay on the GPU: owners from their voxel column there
         dev = torch.device("cuda", torch.cuda.current_device())
         out = slab.ctx.exchange_take_device(dev)
-        rec_np = out.cpu().numpy() if out.shape[0] else np.empty((0, 8), np.int32)
-        dest = torch.from_numpy(slab.destinations(rec_np)).to(dev)
+        dest = slab.destinations_device(out)
     else:
         dev = torch.device("cpu")
         rec_np = slab.ctx.exchange_take()

@@ -175,8 +175,8 @@ def test_two_processes_exchange_over_gloo():
 
 def test_device_records_path_equals_host_path():
     """The exchange through device buffers (the nccl transport's path:
-    exchange_take_device / exchange_put of CUDA tensors) moves the same
-    records as the host path."""
+    exchange_take_device, owners on the device, exchange_put of CUDA
+    tensors) moves the same records as the host path."""
     import torch
     case, K, world = "small_dt5", 6, 2
     z, meta, s, g = load_case(case)
@@ -194,7 +194,8 @@ def test_device_records_path_equals_host_path():
             parts = []
             for o, src in zip(outs, dev):
                 if o.shape[0]:
-                    d = torch.from_numpy(src.destinations(o.cpu().numpy())).to(cuda)
+                    d = src.destinations_device(o)  # owners computed on the GPU
+                    assert np.array_equal(d.cpu().numpy(), src.destinations(o.cpu().numpy()))
                     parts.append(o[d == sl.rank])
             if parts:
                 sl.ctx.exchange_put(sl.id, torch.cat(parts).contiguous())
