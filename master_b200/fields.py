@@ -95,9 +95,11 @@ class Ensemble:
     """Geometries of a field set as systems of one context (one launch per stage)."""
 
     def __init__(self, specs: list[PackSpec], device: int = 0, rng_seed: int = 1, precision=capi.PREC_SPLIT32,
-                 cold: bool = True, geoms: list | None = None):
+                 cold: bool = True, geoms: list | None = None, capacity: tuple | None = None):
         self.specs = specs
         self.ctx = Context(device, precision)
+        if capacity is not None:  # slots per cell: ceil(factor * max(expected, present) + pad)
+            self.ctx.check(self.ctx.lib.dsmc_ctx_set_capacity(self.ctx.handle, float(capacity[0]), int(capacity[1])))
         self.geoms, self.systems, self.settings = [], [], []
         for i, sp in enumerate(specs):
             g = geoms[i] if geoms is not None else sp.geometry()

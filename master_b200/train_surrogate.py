@@ -9,7 +9,8 @@ generates, with the library's own forward and backward kernels.
    by the production pass: `--warmup` steps of transient from a cold start,
    then per-voxel sums every `--every` steps over `--steps` steps, in two
    halves whose difference estimates the sampling noise of the targets.
-2. Training: Adam (lr `--lr`, batch `--batch`) on the weighted squared error
+2. Training: Adam (lr `--lr` decayed on a cosine to 5 % of it, batch
+   `--batch`) on the weighted squared error
    over empty voxels of density (relative to the mean) and drift (in units of
    fields.VELOCITY_SCALE); each batch is shifted by a random periodic offset
    (an exact symmetry of the periodic boxes).
@@ -123,7 +124,7 @@ def evaluate(net, solid, feat, target, halves, edge, batch, device):
     return summary, pred, res
 
 
-def train(net, solid, feat, target, edge, epochs, batch, lr, device, seed=0, log=print):
+def train(net, solid, feat, target, edge, epochs, batch, lr, device, seed=0, lr_min=None, log=print):
     import torch
     dev = torch.device("cuda", device)
     n = len(solid)
@@ -135,6 +136,8 @@ def train(net, solid, feat, target, edge, epochs, batch, lr, device, seed=0, log
     hist = []
     t0 = time.perf_counter()
     steps = 0
+    total = epochs * (n // batch)
+    lr_min = lr * 0.05 if lr_min is None else lr_min
     for ep in range(epochs):
         order = rng.permutation(n)
         net.loss_acc.zero_()
@@ -147,7 +150,8 @@ def train(net, solid, feat, target, edge, epochs, batch, lr, device, seed=0, log
             valid = (s == 0).to(torch.uint8)
             net.forward(s, F_all[idx])
             net.backward(t, valid, cw)
-            net.adam(lr=lr)
+            # cosine decay from lr to lr_min over the run
+            net.adam(lr=lr_min + 0.5 * (lr - lr_min) * (1.0 + np.cos(np.pi * steps / max(total, 1))))
             nb += 1
             steps += 1
         torch.cuda.synchronize(dev)
@@ -169,7 +173,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--every", type=int, default=10)
     ap.add_argument("--per-cell", type=float, default=60.0)
-    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--epochs", type=int, default=200)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--chunk", type=int, default=128, help="geometries per context while generating")

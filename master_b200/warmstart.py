@@ -48,7 +48,7 @@ def predict_fields(net, specs, geoms, batch: int = 1):
 
 def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: int = 1000, tol: float = 0.02,
             field_error: float = 0.0, max_field_error: float = 0.10, device: int = 0, rng_seed: int = 500,
-            log=print) -> dict:
+            capacity: tuple | None = None, force: bool = False, log=print) -> dict:
     """Runs the cold ensemble, then the warm one (one context at a time, so
     the two never share the device memory), `steps` steps each, and returns
     the steps and wall time to steady of both."""
@@ -62,7 +62,7 @@ def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: i
     rep["geometry_s"] = time.perf_counter() - t0
     out = {}
     # cold: the reference's start
-    cold = fields.Ensemble(specs, device=device, rng_seed=rng_seed, cold=True, geoms=geoms)
+    cold = fields.Ensemble(specs, device=device, rng_seed=rng_seed, cold=True, geoms=geoms, capacity=capacity)
     counts_n = [S.num_molecules for S in cold.systems]
     weights = np.array([s.atoms_per_molecule for s in cold.settings], np.float64)
     dt = cold.settings[0].dt
@@ -73,8 +73,9 @@ def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: i
     cold.close()
     log("cold", out["cold"]["seconds"], "s")
     # warm: same geometries, seeds and particle counts, seeded from the surrogate
-    warm = fields.Ensemble(specs, device=device, rng_seed=rng_seed, cold=False, geoms=geoms)
-    use_net = field_error <= max_field_error
+    warm = fields.Ensemble(specs, device=device, rng_seed=rng_seed, cold=False, geoms=geoms, capacity=capacity)
+    use_net = force or field_error <= max_field_error
+    rep["forced"] = bool(force and field_error > max_field_error)
     t0 = time.perf_counter()
     preds = predict_fields(net, specs, geoms) if use_net else [None] * len(specs)
     torch.cuda.synchronize()
@@ -149,20 +150,24 @@ def main(argv=None):
     ap.add_argument("--every", type=int, default=10)
     ap.add_argument("--per-cell", type=float, default=30.0)
     ap.add_argument("--knudsen", type=float, nargs=2, default=(0.3, 3.0))
+    ap.add_argument("--capacity", type=float, nargs=2, default=None, metavar=("FACTOR", "PAD"))
+    ap.add_argument("--force", action="store_true",
+                    help="seed from the surrogate even when its field error is above the fallback threshold")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     import torch
     net, held = load_net(a.weights)
     specs = fields.random_specs(a.geometries, a.edge, seed=5, porosity=(0.45, 0.75), knudsen=tuple(a.knudsen),
                                 per_cell=a.per_cell)
-    rep = compare(net, specs, a.steps, every=a.every, field_error=float(held.get("field_error", 0.0)))
+    rep = compare(net, specs, a.steps, every=a.every, field_error=float(held.get("field_error", 0.0)),
+                  capacity=tuple(a.capacity) if a.capacity else None, force=a.force)
     rep["surrogate_held_out"] = held
     text = json.dumps(rep, default=float)
     if a.out:
         from pathlib import Path
         Path(a.out).mkdir(parents=True, exist_ok=True)
         (Path(a.out) / "warmstart.json").write_text(json.dumps(rep, indent=1, default=float))
-    print(json.dumps({k: v for k, v in rep.items() if k in ("ratio_steps", "fallback", "particles")} |
+    print(json.dumps({k: v for k, v in rep.items() if k in ("ratio_steps", "fallback", "particles", "forced")} |
                      {n: {k: rep[n][k] for k in ("steps_to_steady", "wall_s_to_steady", "ms_per_step",
                                                   "window_noise")} for n in ("cold", "warm")}))
     del torch, text
