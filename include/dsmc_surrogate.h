@@ -79,11 +79,22 @@ int dsmc_sg_head(void *stream, int batch, int S, const uint16_t *e, int e_cs, in
 
 /* Weighted squared error over the rows with valid[v] != 0 and its backward
  * through the head: *loss += sum_v sum_c cw[c] (out - target)^2 * inv_count;
- * dwh, dbh accumulate; de[v][k] = (sum_c wh[c][k] dout[v][c]) * (e[v][k] > 0). */
+ * dwh, dbh accumulate; de[v][k] = (sum_c wh[c][k] dout[v][c]) * (e[v][k] > 0).
+ * sample_coef (NULL: none): per-sample values added to dout[v][coef_channel]
+ * of every valid row of the sample (dsmc_sg_sample_flux_loss's coef). */
 int dsmc_sg_loss_head_bwd(void *stream, int batch, int S, const float *out, const float *target,
                           const uint8_t *valid, const float *channel_weight, float inv_count, const uint16_t *e,
                           int e_cs, int e_coff, const float *wh, float *dwh, float *dbh, uint16_t *de, int de_cs,
-                          int de_coff, double *loss);
+                          int de_coff, double *loss, const double *sample_coef, int coef_channel);
+
+/* Per-sample mean term of the loss: with m_b the mean over sample b's valid
+ * rows of out[v][channel] - target[v][channel] (the error of the sample's
+ * mean drift, i.e. of its flux), *loss += weight * sum_b m_b^2 / batch and
+ * coef[b] = its derivative with respect to each of those outputs, for
+ * dsmc_sg_loss_head_bwd.  work: 2*batch doubles of scratch (device). */
+int dsmc_sg_sample_flux_loss(void *stream, int batch, int S, const float *out, const float *target,
+                             const uint8_t *valid, int channel, float weight, double *work, double *coef,
+                             double *loss);
 
 /* Adam (Kingma & Ba 2015) with bias correction, step >= 1, on n fp32 values. */
 int dsmc_sg_adam(void *stream, float *param, const float *grad, float *m, float *v, int64_t n, float lr, float beta1,

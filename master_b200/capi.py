@@ -52,7 +52,7 @@ EXPORTED = [
 EXPORTED_SURROGATE = [
     "dsmc_sg_conv3", "dsmc_sg_conv3_wgrad", "dsmc_sg_bias_grad", "dsmc_sg_pool2", "dsmc_sg_pool2_bwd",
     "dsmc_sg_up2", "dsmc_sg_up2_bwd", "dsmc_sg_pack_input", "dsmc_sg_head", "dsmc_sg_loss_head_bwd",
-    "dsmc_sg_adam", "dsmc_sg_pack_weights", "dsmc_sg_status",
+    "dsmc_sg_adam", "dsmc_sg_pack_weights", "dsmc_sg_status", "dsmc_sg_sample_flux_loss",
 ]
 
 
@@ -209,7 +209,8 @@ def load() -> C.CDLL:
         "dsmc_sg_up2_bwd": [V, I, I, V, I, I, V, I, I, I, V, I, I],
         "dsmc_sg_pack_input": [V, I, I, V, V, V],
         "dsmc_sg_head": [V, I, I, V, I, I, V, V, V],
-        "dsmc_sg_loss_head_bwd": [V, I, I, V, V, V, V, C.c_float, V, I, I, V, V, V, V, I, I, V],
+        "dsmc_sg_loss_head_bwd": [V, I, I, V, V, V, V, C.c_float, V, I, I, V, V, V, V, I, I, V, V, I],
+        "dsmc_sg_sample_flux_loss": [V, I, I, V, V, V, I, C.c_float, V, V, V],
         "dsmc_sg_adam": [V, V, V, V, V, C.c_int64, C.c_float, C.c_float, C.c_float, C.c_float, C.c_int64],
         "dsmc_sg_pack_weights": [V, V, I, I, V, V],
         "dsmc_sg_status": [C.POINTER(C.c_uint), I],

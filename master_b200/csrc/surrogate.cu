@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <string>
 
 #include "dsmc_b200.h"
@@ -552,7 +553,8 @@ __global__ void head_kernel(Vol e, const float *wh, const float *bh, float *out,
 //   de[r][k] = (sum_c wh[c][k] dout[c]) * (e[r][k] > 0)   (bf16).
 __global__ void loss_head_bwd_kernel(const float *out, const float *tgt, const uint8_t *valid, const float *cw,
                                      float inv_count, Vol e, const float *wh, float *dwh, float *dbh,
-                                     VolOut de, double *loss, long long rows) {
+                                     VolOut de, double *loss, long long rows, const double *coef, int coef_ch,
+                                     int lg) {
     __shared__ float w[64];
     __shared__ float gw[64 + 4];
     __shared__ double ls;
@@ -574,6 +576,7 @@ __global__ void loss_head_bwd_kernel(const float *out, const float *tgt, const u
                 lloss += (double)(cw[c] * diff * diff * inv_count);
                 d[c] = 2.0f * cw[c] * diff * inv_count;
             }
+            if (coef) d[coef_ch] += (float)coef[r >> (3 * lg)];
         }
         float x[16];
         const uint4 u0 = *reinterpret_cast<const uint4 *>(e.p + r * e.cs + e.coff);
@@ -623,6 +626,54 @@ __global__ void loss_head_bwd_kernel(const float *out, const float *tgt, const u
     if (threadIdx.x < 64) atomicAdd(&dwh[threadIdx.x], gw[threadIdx.x]);
     if (threadIdx.x < 4) atomicAdd(&dbh[threadIdx.x], gw[64 + threadIdx.x]);
     if (threadIdx.x == 0) atomicAdd(loss, ls);
+}
+
+// Per-sample sums over the valid rows of out[r][ch] - tgt[r][ch] and of the
+// valid rows themselves: acc[2b], acc[2b + 1] (fp64 atomics of block sums).
+// blockIdx.y = sample.
+__global__ void sample_diff_kernel(const float *out, const float *tgt, const uint8_t *valid, int ch,
+                                   long long rows_per_sample, double *acc) {
+    __shared__ double part[2];
+    if (threadIdx.x < 2) part[threadIdx.x] = 0.0;
+    __syncthreads();
+    const long long b = blockIdx.y;
+    double sd = 0.0, sn = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < rows_per_sample;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long r = b * rows_per_sample + i;
+        if (valid[r]) {
+            sd += (double)(out[r * 4 + ch] - tgt[r * 4 + ch]);
+            sn += 1.0;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        sd += __shfl_xor_sync(0xffffffffu, sd, o);
+        sn += __shfl_xor_sync(0xffffffffu, sn, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&part[0], sd);
+        atomicAdd(&part[1], sn);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        atomicAdd(&acc[2 * b], part[0]);
+        atomicAdd(&acc[2 * b + 1], part[1]);
+    }
+}
+
+// The per-sample mean term: loss += w * sum_b m_b^2 / B with m_b the mean of
+// out - tgt over sample b's valid rows; coef[b] = 2 w m_b / (n_b B) is its
+// derivative with respect to each of those rows' outputs.
+__global__ void sample_flux_finish_kernel(const double *acc, int batch, float w, double *coef, double *loss) {
+    double l = 0.0;
+    for (int b = threadIdx.x; b < batch; b += blockDim.x) {
+        const double n = acc[2 * b + 1] > 0.0 ? acc[2 * b + 1] : 1.0;
+        const double m = acc[2 * b] / n;
+        coef[b] = 2.0 * (double)w * m / (n * (double)batch);
+        l += (double)w * m * m / (double)batch;
+    }
+    for (int o = 16; o > 0; o >>= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, l);
 }
 
 // Adam with bias correction on n fp32 parameters.
@@ -858,14 +909,32 @@ int dsmc_sg_head(void *stream, int batch, int S, const uint16_t *e, int e_cs, in
 int dsmc_sg_loss_head_bwd(void *stream, int batch, int S, const float *out, const float *target,
                           const uint8_t *valid, const float *channel_weight, float inv_count, const uint16_t *e,
                           int e_cs, int e_coff, const float *wh, float *dwh, float *dbh, uint16_t *de, int de_cs,
-                          int de_coff, double *loss) {
+                          int de_coff, double *loss, const double *sample_coef, int coef_channel) {
     const int lg = lg2_of(S);
-    if (lg < 1 || !out || !target || !valid || !channel_weight || !e || !wh || !dwh || !dbh || !de || !loss)
+    if (lg < 1 || !out || !target || !valid || !channel_weight || !e || !wh || !dwh || !dbh || !de || !loss ||
+        coef_channel < 0 || coef_channel > 3)
         return sg_fail(DSMC_ERR_ARG, "loss_head_bwd: bad argument");
     const long long rows = (long long)batch << (3 * lg);
     loss_head_bwd_kernel<<<grid_for(rows, 128), 128, 0, static_cast<cudaStream_t>(stream)>>>(
         out, target, valid, channel_weight, inv_count, {reinterpret_cast<const bf16 *>(e), e_cs, e_coff}, wh, dwh, dbh,
-        {reinterpret_cast<bf16 *>(de), de_cs, de_coff}, loss, rows);
+        {reinterpret_cast<bf16 *>(de), de_cs, de_coff}, loss, rows, sample_coef, coef_channel, lg);
+    return cuda_rc(cudaGetLastError());
+}
+
+int dsmc_sg_sample_flux_loss(void *stream, int batch, int S, const float *out, const float *target,
+                             const uint8_t *valid, int channel, float weight, double *work, double *coef,
+                             double *loss) {
+    const int lg = lg2_of(S);
+    if (lg < 1 || batch < 1 || batch > 1024 || channel < 0 || channel > 3 || !out || !target || !valid || !work ||
+        !coef || !loss)
+        return sg_fail(DSMC_ERR_ARG, "sample_flux_loss: bad argument");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemsetAsync(work, 0, 2 * (size_t)batch * sizeof(double), st);
+    if (e != cudaSuccess) return cuda_rc(e);
+    const long long per = 1ll << (3 * lg);
+    dim3 grid((unsigned)std::max<long long>(1, std::min<long long>((per + 255) / 256, 256)), (unsigned)batch);
+    sample_diff_kernel<<<grid, 256, 0, st>>>(out, target, valid, channel, per, work);
+    sample_flux_finish_kernel<<<1, 256, 0, st>>>(work, batch, weight, coef, loss);
     return cuda_rc(cudaGetLastError());
 }
 

@@ -101,6 +101,7 @@ class UNet:
             self.wd[name] = torch.empty(cout * 27 * cin, dtype=torch.int16, device=self.dev)
         self.buf: Buffers | None = None
         self.loss_acc = torch.zeros(1, dtype=torch.float64, device=self.dev)
+        self.flux_work = None
         self.stream = None  # the current torch stream at each call
         self.pack_weights()
 
@@ -197,11 +198,13 @@ class UNet:
                                    self._ptr(t["out"])))
         return t["out"]
 
-    def backward(self, target, valid, channel_weight) -> None:
+    def backward(self, target, valid, channel_weight, flux_weight: float = 0.0) -> None:
         """Gradients of the weighted squared error of the last forward's
         output against target (B, S, S, S, 4) over the voxels with valid != 0
-        (uint8 (B, S, S, S)), into self.g (zeroed first).  The loss is added
-        to self.loss_acc."""
+        (uint8 (B, S, S, S)), into self.g (zeroed first); with flux_weight,
+        plus flux_weight times the squared error of each sample's mean x
+        drift over its valid voxels (its flux), averaged over the batch.  The
+        loss is added to self.loss_acc."""
         t = self.buf.t
         B, S = self.buf.batch, self.buf.S
         H, Q = S // 2, S // 4
@@ -211,11 +214,21 @@ class UNet:
         count = max(1, int(valid.sum().item()))
         cw = channel_weight if hasattr(channel_weight, "data_ptr") else self.torch.tensor(
             channel_weight, dtype=self.torch.float32, device=self.dev)
-        self._check(L.dsmc_sg_loss_head_bwd(s, B, S, self._ptr(t["out"]), self._ptr(target.contiguous()),
-                                            self._ptr(valid.contiguous()), self._ptr(cw), C.c_float(1.0 / count),
+        target = target.contiguous()
+        valid = valid.contiguous()
+        coef = None
+        if flux_weight > 0:
+            if self.flux_work is None or self.flux_work.numel() < 3 * B:
+                self.flux_work = self.torch.zeros(3 * B, dtype=self.torch.float64, device=self.dev)
+            coef = self.flux_work[2 * B:3 * B]
+            self._check(L.dsmc_sg_sample_flux_loss(s, B, S, self._ptr(t["out"]), self._ptr(target), self._ptr(valid),
+                                                   1, C.c_float(flux_weight), self._ptr(self.flux_work),
+                                                   self._ptr(coef), self._ptr(self.loss_acc)))
+        self._check(L.dsmc_sg_loss_head_bwd(s, B, S, self._ptr(t["out"]), self._ptr(target),
+                                            self._ptr(valid), self._ptr(cw), C.c_float(1.0 / count),
                                             self._ptr(t["e1"]), 16, 0, self._pp("head.w"), self._gp("head.w"),
                                             self._gp("head.b"), self._ptr(t["de1"]), 16, 0,
-                                            self._ptr(self.loss_acc)))
+                                            self._ptr(self.loss_acc), self._ptr(coef), 1))
         # level 0 decoder
         self._wgrad(B, S, t["de1"], 16, 0, 16, t["d1"], 16, 0, 16, "c1d")
         self._conv(B, S, t["de1"], 16, 0, 16, "c1d", 16, t["dd1"], 16, 0, relu=False, mask=t["d1"], mcs=16,

@@ -10,7 +10,9 @@ generates, with the library's own forward and backward kernels.
    then per-voxel sums every `--every` steps over `--steps` steps, in two
    halves whose difference estimates the sampling noise of the targets.
 2. Training: Adam (lr `--lr` decayed on a cosine to 5 % of it, batch
-   `--batch`) on the weighted squared error
+   `--batch`) on the weighted squared error, plus FLUX_WEIGHT times the
+   squared error of each box's mean x drift (the per-voxel drift targets are
+   mostly sampling noise; their mean over a box, the flux, is not),
    over empty voxels of density (relative to the mean) and drift (in units of
    fields.VELOCITY_SCALE); each batch is shifted by a random periodic offset
    (an exact symmetry of the periodic boxes).
@@ -34,6 +36,9 @@ import numpy as np
 from . import fields, surrogate
 
 CHANNEL_WEIGHT = [1.0, 4.0, 1.0, 1.0]  # density, drift x, y, z
+# weight of each sample's mean x drift error (its flux): the per-voxel drift
+# targets are mostly sampling noise, their mean over a box is not
+FLUX_WEIGHT = 100.0
 
 
 def generate(specs, warmup: int, steps: int, every: int, device: int = 0, log=print):
@@ -124,7 +129,8 @@ def evaluate(net, solid, feat, target, halves, edge, batch, device):
     return summary, pred, res
 
 
-def train(net, solid, feat, target, edge, epochs, batch, lr, device, seed=0, lr_min=None, log=print):
+def train(net, solid, feat, target, edge, epochs, batch, lr, device, seed=0, lr_min=None, flux_weight=FLUX_WEIGHT,
+          log=print):
     import torch
     dev = torch.device("cuda", device)
     n = len(solid)
@@ -149,7 +155,7 @@ def train(net, solid, feat, target, edge, epochs, batch, lr, device, seed=0, lr_
             t = torch.roll(T_all[idx], sh, dims=(1, 2, 3))
             valid = (s == 0).to(torch.uint8)
             net.forward(s, F_all[idx])
-            net.backward(t, valid, cw)
+            net.backward(t, valid, cw, flux_weight=flux_weight)
             # cosine decay from lr to lr_min over the run
             net.adam(lr=lr_min + 0.5 * (lr - lr_min) * (1.0 + np.cos(np.pi * steps / max(total, 1))))
             nb += 1

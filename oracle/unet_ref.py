@@ -114,13 +114,23 @@ class UNetRef:
         out = torch.einsum("bkzyx,ck->bzyxc", e1, self.t["head.w"]) + self.t["head.b"]
         return out
 
-    def loss(self, out, target: np.ndarray, valid: np.ndarray, channel_weight) -> torch.Tensor:
+    def loss(self, out, target: np.ndarray, valid: np.ndarray, channel_weight, flux_weight: float = 0.0):
+        """sum over valid voxels and channels of cw (out - target)^2 / count,
+        plus flux_weight * the batch mean of (each sample's mean over its
+        valid voxels of out - target in channel 1)^2."""
         tg = torch.tensor(np.asarray(target, np.float64))
         m = torch.tensor(np.asarray(valid, bool))
         cw = torch.tensor(np.asarray(channel_weight, np.float64))
         count = max(1, int(m.sum()))
         d = (out - tg) ** 2 * cw
-        return d[m].sum() / count
+        loss = d[m].sum() / count
+        if flux_weight:
+            B = out.shape[0]
+            mf = m.reshape(B, -1).to(out.dtype)
+            diff = (out[..., 1] - tg[..., 1]).reshape(B, -1)
+            mean = (diff * mf).sum(1) / mf.sum(1).clamp(min=1)
+            loss = loss + flux_weight * (mean ** 2).mean()
+        return loss
 
     def grads(self) -> dict:
         return {k: v.grad.detach().numpy().copy() for k, v in self.t.items()}

@@ -239,11 +239,11 @@ def test_unet_forward_backward_matches_cpu_reference():
     net = sgm.UNet(0, params)
     out = net.forward(torch.tensor(solid, device=DEV), torch.tensor(feature, device=DEV))
     net.loss_acc.zero_()
-    net.backward(torch.tensor(target, device=DEV), torch.tensor(valid, device=DEV), cw)
+    net.backward(torch.tensor(target, device=DEV), torch.tensor(valid, device=DEV), cw, flux_weight=3.0)
     sync_ok()
     ref = UNetRef(params, emulate_bf16=True)
     rout = ref.forward(solid, feature)
-    loss = ref.loss(rout, target, valid, cw)
+    loss = ref.loss(rout, target, valid, cw, flux_weight=3.0)
     loss.backward()
     o = out.detach().cpu().numpy()
     assert rel_l2(o, rout.detach().numpy()) <= 1e-2
@@ -254,7 +254,7 @@ def test_unet_forward_backward_matches_cpu_reference():
     # sum on the other side of a rounding boundary, compounded through the
     # backward chain) must stay well inside it
     exact = UNetRef(params, emulate_bf16=False)
-    exact.loss(exact.forward(solid, feature), target, valid, cw).backward()
+    exact.loss(exact.forward(solid, feature), target, valid, cw, flux_weight=3.0).backward()
     eg = exact.grads()
     for k in rg:
         e_gpu, e_bf16 = rel_l2(gg[k], rg[k]), rel_l2(rg[k], eg[k])
@@ -264,9 +264,9 @@ def test_unet_forward_backward_matches_cpu_reference():
     assert flat_g @ flat_r / (np.linalg.norm(flat_g) * np.linalg.norm(flat_r)) >= 0.999
     # the gradient is the derivative: one step along it lowers the fp64 loss
     ref2 = UNetRef(params - 1e-3 * net.g.cpu().numpy() / np.linalg.norm(net.g.cpu().numpy()), emulate_bf16=False)
-    l2 = ref2.loss(ref2.forward(solid, feature), target, valid, cw).item()
+    l2 = ref2.loss(ref2.forward(solid, feature), target, valid, cw, flux_weight=3.0).item()
     ref3 = UNetRef(params, emulate_bf16=False)
-    l3 = ref3.loss(ref3.forward(solid, feature), target, valid, cw).item()
+    l3 = ref3.loss(ref3.forward(solid, feature), target, valid, cw, flux_weight=3.0).item()
     assert l2 < l3
 
 

@@ -23,9 +23,10 @@ def test_parameter_layouts_agree():
 
 
 def test_reference_gradient_matches_finite_differences():
-    """fp64 without bf16 emulation: the analytic gradient of the loss equals
-    central differences along random directions (periodic padding, pooling,
-    upsampling, skips and the head included)."""
+    """fp64 without bf16 emulation: the analytic gradient of the loss (the
+    per-sample flux term included) equals central differences along random
+    directions (periodic padding, pooling, upsampling, skips and the head
+    included)."""
     rng = np.random.default_rng(0)
     B, S = 1, 16
     solid = (rng.random((B, S, S, S)) < 0.3).astype(np.uint8)
@@ -38,7 +39,7 @@ def test_reference_gradient_matches_finite_differences():
         if k.endswith(".b"):
             p[o:o + int(np.prod(sh))] = rng.normal(0, 0.05, int(np.prod(sh)))
     ref = unet_ref.UNetRef(p, emulate_bf16=False)
-    loss = ref.loss(ref.forward(solid, feature), target, valid, cw)
+    loss = ref.loss(ref.forward(solid, feature), target, valid, cw, flux_weight=2.0)
     loss.backward()
     g = ref.grads()
     flat = np.concatenate([g[k].ravel() for k in unet_ref.unpack(p)])  # layout order
@@ -51,7 +52,7 @@ def test_reference_gradient_matches_finite_differences():
     def f(q):
         r = unet_ref.UNetRef(q, emulate_bf16=False)
         with torch.no_grad():
-            return r.loss(r.forward(solid, feature), target, valid, cw).item()
+            return r.loss(r.forward(solid, feature), target, valid, cw, flux_weight=2.0).item()
 
     for trial in range(3):
         d = rng.normal(0, 1, n)
