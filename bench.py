@@ -270,7 +270,7 @@ def _timed_steps(ctx, steps: int) -> float:
 def other_configs(args, device):
     """The plain-DSMC configuration (packed_64: 64^3, r = 4, porosity 0.6,
     ~3.9e5 particles) in the fp64 reference arithmetic and in split
-    precision, and the batched ensemble (64 packed-sphere geometries of edges
+    precision, the large geometry (packed_256) in fp64, and the batched ensemble (64 packed-sphere geometries of edges
     32-128, porosity 0.4-0.8, radius 3-8, Knudsen 0.1-10, one context, one
     launch per stage), each timed over `steps` steps after a warm-up."""
     from master_b200 import capi, fields, workloads
@@ -287,6 +287,17 @@ def other_configs(args, device):
                      "particles": S.num_molecules, "dtype": "f64" if prec == capi.PREC_FP64 else
                      "fp32 state + fp64 tallies"}
         S.ctx.close()
+    # the large geometry in the fp64 reference arithmetic (the judge of the
+    # split-precision numbers above)
+    w256 = workloads.PACKED_256
+    S = System(w256.settings(rng_seed=5, statistics_interval=100), w256.geometry(), device=device,
+               precision=capi.PREC_FP64)
+    S.step(3)
+    k = 10
+    ms = _timed_steps(S.ctx, k)
+    out["packed_256_fp64"] = {"value": S.num_molecules * k / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / k,
+                              "steps": k, "particles": S.num_molecules, "dtype": "f64"}
+    S.ctx.close()
     # batched ensemble of uneven geometries
     rng = np.random.default_rng(3)
     specs = fields.random_specs(64, 32, seed=3, per_cell=30.0)
