@@ -103,9 +103,11 @@ __global__ void __launch_bounds__(kThreads) conv3_kernel(ConvArgs a) {
     const int cpt = a.cin >> 3;                  // 16-byte chunks per tap
     const int Q = 27 * cpt;                      // chunks of K
     const int nst = (Q + kChunks - 1) / kChunks; // stages per tile
-    const long long tiles = a.rows >> 7;
-    const long long my_tiles = tiles > blockIdx.x ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
-    const long long G = my_tiles * nst;
+    const int tiles = (int)(a.rows >> 7);
+    const int my_tiles = tiles > (int)blockIdx.x ? (tiles - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    const int G = my_tiles * nst;                // stages of this CTA (32-bit: at most 2^31)
+    const int lg = a.lg, msk = a.S - 1;
+    const int lg2 = 2 * lg, lg3 = 3 * lg;
 
     if (warp == 0) {
         tc05::tmem_alloc(tslot, Sh::kCols);
@@ -120,55 +122,67 @@ __global__ void __launch_bounds__(kThreads) conv3_kernel(ConvArgs a) {
     tc05::fence_after_sync();
     const uint32_t tmem = *tslot;
 
-    auto load_stage = [&](long long g) {
-        const int s = (int)(g % kStages);
-        unsigned char *As = smem + s * Sh::kStageBytes;
+    // Position of the next stage to load (tile ordinal, stage in tile, ring
+    // buffer), advanced one stage per call; no divisions in the loop.
+    int ld_t = 0, ld_j = 0, ld_s = 0;
+    auto load_next = [&]() {
+        unsigned char *As = smem + ld_s * Sh::kStageBytes;
         unsigned char *Bs = As + kATileBytes;
-        const long long tile = blockIdx.x + (g / nst) * gridDim.x;
-        const int j = (int)(g % nst);
-        const int q0 = j * kChunks, nq = min(kChunks, Q - q0);
-        // A: row tid, chunks q0..q0+nq-1
-        const long long row = tile * 128 + tid;
-        int last_tap = -1;
-        long long nrow = 0;
+        const long long row = ((long long)blockIdx.x + (long long)ld_t * gridDim.x) * 128 + tid;
+        const int q0 = ld_j * kChunks, nq = min(kChunks, Q - q0);
+        // this thread's row: sample base and coordinates
+        const long long base = (row >> lg3) << lg3;
+        const int v = (int)(row - base);
+        const int x0 = v >> lg2, x1 = (v >> lg) & msk, x2 = v & msk;
+        int t = q0 / cpt, c8 = q0 - t * cpt;
+        const bf16 *src = nullptr;
+        auto at_tap = [&](int tt) {
+            const int y0 = (x0 + tt / 9 - 1) & msk, y1 = (x1 + (tt / 3) % 3 - 1) & msk, y2 = (x2 + tt % 3 - 1) & msk;
+            const long long nrow = base + ((long long)y0 << lg2) + ((long long)y1 << lg) + y2;
+            src = a.in.p + nrow * a.in.cs + a.in.coff;
+        };
+        at_tap(t);
         for (int c = 0; c < nq; ++c) {
-            const int q = q0 + c;
-            const int t = q / cpt, c8 = q - t * cpt;
-            if (t != last_tap) {
-                nrow = neighbour(row, t, 1, a.S, a.lg);
-                last_tap = t;
+            tc05::cp_async16(As + c * 2048 + (tid >> 3) * 128 + (tid & 7) * 16, src + c8 * 8);
+            if (++c8 == cpt) {
+                c8 = 0;
+                if (++t < 27) at_tap(t);
             }
-            const bf16 *src = a.in.p + nrow * a.in.cs + a.in.coff + c8 * 8;
-            tc05::cp_async16(As + c * 2048 + (tid >> 3) * 128 + (tid & 7) * 16, src);
         }
         // B: n rows x nq chunks of the weights
+        const bf16 *wsrc = a.w + q0 * 8;
         for (int idx = tid; idx < N * nq; idx += kThreads) {
             const int n = idx % N, c = idx / N;
-            const bf16 *src = a.w + (long long)n * (27 * a.cin) + (q0 + c) * 8;
-            tc05::cp_async16(Bs + c * (N * 16) + (n >> 3) * 128 + (n & 7) * 16, src);
+            tc05::cp_async16(Bs + c * (N * 16) + (n >> 3) * 128 + (n & 7) * 16, wsrc + (long long)n * (27 * a.cin) + c * 8);
         }
+        if (++ld_j == nst) {
+            ld_j = 0;
+            ++ld_t;
+        }
+        if (++ld_s == kStages) ld_s = 0;
     };
 
-    for (long long g = 0; g < kStages - 1; ++g) {
-        if (g < G) load_stage(g);
+    for (int g = 0; g < kStages - 1; ++g) {
+        if (g < G) load_next();
         tc05::cp_async_commit();
     }
-    for (long long g = 0; g < G; ++g) {
-        const long long gn = g + kStages - 1;
-        if (gn < G) {
+    int j = 0, s = 0, ti = 0;  // the stage in work: stage in tile, ring buffer, tile ordinal
+    int ph_prev = 0;           // parity of the commit of stage g - 1 on its buffer
+    int s_prev = kStages - 1;
+    uint32_t parity_bits = 0;  // bit b: parity of the next commit on buffer b
+    for (int g = 0; g < G; ++g) {
+        if (g + kStages - 1 < G) {
             if (g >= 1) {
-                // the MMAs of stage g-1 read the buffer stage gn reuses
-                if (!tc05::mbar_wait(&mbar[(g - 1) % kStages], (uint32_t)(((g - 1) / kStages) & 1)))
-                    atomicOr(&g_error, 1u);
+                // the MMAs of stage g-1 read the buffer the next load reuses
+                if (!tc05::mbar_wait(&mbar[s_prev], (uint32_t)ph_prev)) atomicOr(&g_error, 1u);
             }
-            load_stage(gn);
+            load_next();
         }
         tc05::cp_async_commit();
         tc05::cp_async_wait<kStages - 1>();
         tc05::fence_proxy_async_smem();
         __syncthreads();
-        const int j = (int)(g % nst);
-        const int s = (int)(g % kStages);
+        const uint32_t my_parity = (parity_bits >> s) & 1u;
         if (tid == 0) {
             tc05::fence_after_sync();
             const uint32_t As = tc05::smem_u32(smem + s * Sh::kStageBytes);
@@ -183,9 +197,9 @@ __global__ void __launch_bounds__(kThreads) conv3_kernel(ConvArgs a) {
         }
         if (j == nst - 1) {
             // tile complete: wait for its MMAs, then the epilogue
-            if (!tc05::mbar_wait(&mbar[s], (uint32_t)((g / kStages) & 1))) atomicOr(&g_error, 1u);
+            if (!tc05::mbar_wait(&mbar[s], my_parity)) atomicOr(&g_error, 1u);
             tc05::fence_after_sync();
-            const long long tile = blockIdx.x + (g / nst) * gridDim.x;
+            const long long tile = (long long)blockIdx.x + (long long)ti * gridDim.x;
             const long long row = tile * 128 + warp * 32 + lane;
             bf16 *dst = a.out.p + row * a.out.cs + a.out.coff;
             const bf16 *mk = a.mask.p ? a.mask.p + row * a.mask.cs + a.mask.coff : nullptr;
@@ -224,6 +238,15 @@ __global__ void __launch_bounds__(kThreads) conv3_kernel(ConvArgs a) {
                 *reinterpret_cast<uint4 *>(dst + c0 + 8) = o1;
             }
             tc05::fence_before_sync();
+        }
+        // advance the stage in work
+        ph_prev = (int)my_parity;
+        s_prev = s;
+        parity_bits ^= 1u << s;
+        if (++s == kStages) s = 0;
+        if (++j == nst) {
+            j = 0;
+            ++ti;
         }
     }
     tc05::fence_before_sync();
@@ -265,7 +288,7 @@ __global__ void __launch_bounds__(kThreads) wgrad_kernel(WgradArgs a) {
     const int m_total = 27 * a.cout;
     const long long u_begin = (long long)blockIdx.y * a.kv;
     const long long u_end = min(a.rows, u_begin + a.kv);
-    const long long G = (u_end - u_begin) / 64;
+    const int G = (int)((u_end - u_begin) / 64);
 
     if (warp == 0) {
         tc05::tmem_alloc(tslot, Sh::kCols);
@@ -280,48 +303,73 @@ __global__ void __launch_bounds__(kThreads) wgrad_kernel(WgradArgs a) {
     tc05::fence_after_sync();
     const uint32_t tmem = *tslot;
 
-    auto load_stage = [&](long long g) {
-        const int s = (int)(g % kStages);
-        unsigned char *As = smem + s * Sh::kStageBytes;
+    // This thread's eight row groups of the M tile: tap offset (negated) and
+    // channel offset, fixed for the CTA; -1: a padding group (zeros).
+    const int msk = a.S - 1, lg = a.lg, lg2 = 2 * a.lg, lg3 = 3 * a.lg;
+    int goff[8], gco[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int m = blockIdx.x * 128 + ((tid >> 6) + 2 * i) * 8;
+        if (m < m_total) {
+            const int t = m / a.cout;
+            gco[i] = m - t * a.cout;
+            goff[i] = t;
+        } else {
+            gco[i] = -1;
+            goff[i] = 0;
+        }
+    }
+    int ld_s = 0;
+    long long ld_u = u_begin + (tid & 63);  // this thread's voxel of the next stage to load
+    auto load_next = [&]() {
+        unsigned char *As = smem + ld_s * Sh::kStageBytes;
         unsigned char *Bs = As + kATileBytes;
         const int k = tid & 63;
-        const long long u = u_begin + g * 64 + k;
         const int kg = k >> 3, k8 = k & 7;
-        // A: 16 groups of 8 rows (tap, co..co+7) at voxel u
-        for (int mg = tid >> 6; mg < 16; mg += 2) {
-            const int m = blockIdx.x * 128 + mg * 8;
+        const long long u = ld_u;
+        const long long base = (u >> lg3) << lg3;
+        const int v = (int)(u - base);
+        const int x0 = v >> lg2, x1 = (v >> lg) & msk, x2 = v & msk;
+        // A: 8 of the 16 groups of 8 rows (tap, co..co+7) at voxel u - off(tap)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int mg = (tid >> 6) + 2 * i;
             unsigned char *dst = As + kg * 2048 + mg * 128 + k8 * 16;
-            if (m < m_total) {
-                const int t = m / a.cout, co = m - t * a.cout;
-                const long long nrow = neighbour(u, t, -1, a.S, a.lg);
-                tc05::cp_async16(dst, a.dy.p + nrow * a.dy.cs + a.dy.coff + co);
+            if (gco[i] >= 0) {
+                const int t = goff[i];
+                const int y0 = (x0 - (t / 9 - 1)) & msk, y1 = (x1 - ((t / 3) % 3 - 1)) & msk,
+                          y2 = (x2 - (t % 3 - 1)) & msk;
+                const long long nrow = base + ((long long)y0 << lg2) + ((long long)y1 << lg) + y2;
+                tc05::cp_async16(dst, a.dy.p + nrow * a.dy.cs + a.dy.coff + gco[i]);
             } else {
                 tc05::cp_async16_zfill(dst, a.dy.p, 0);
             }
         }
         // B: N/8 groups of 8 input channels at voxel u
+        const bf16 *xs = a.x.p + u * a.x.cs + a.x.coff;
         for (int ng = tid >> 6; ng < N / 8; ng += 2)
-            tc05::cp_async16(Bs + kg * (N * 16) + ng * 128 + k8 * 16, a.x.p + u * a.x.cs + a.x.coff + ng * 8);
+            tc05::cp_async16(Bs + kg * (N * 16) + ng * 128 + k8 * 16, xs + ng * 8);
+        ld_u += 64;
+        if (++ld_s == kStages) ld_s = 0;
     };
 
-    for (long long g = 0; g < kStages - 1; ++g) {
-        if (g < G) load_stage(g);
+    for (int g = 0; g < kStages - 1; ++g) {
+        if (g < G) load_next();
         tc05::cp_async_commit();
     }
-    for (long long g = 0; g < G; ++g) {
-        const long long gn = g + kStages - 1;
-        if (gn < G) {
+    int s = 0, s_prev = kStages - 1;
+    uint32_t parity_bits = 0, ph_prev = 0;
+    for (int g = 0; g < G; ++g) {
+        if (g + kStages - 1 < G) {
             if (g >= 1) {
-                if (!tc05::mbar_wait(&mbar[(g - 1) % kStages], (uint32_t)(((g - 1) / kStages) & 1)))
-                    atomicOr(&g_error, 2u);
+                if (!tc05::mbar_wait(&mbar[s_prev], ph_prev)) atomicOr(&g_error, 2u);
             }
-            load_stage(gn);
+            load_next();
         }
         tc05::cp_async_commit();
         tc05::cp_async_wait<kStages - 1>();
         tc05::fence_proxy_async_smem();
         __syncthreads();
-        const int s = (int)(g % kStages);
         if (tid == 0) {
             tc05::fence_after_sync();
             const uint32_t As = tc05::smem_u32(smem + s * Sh::kStageBytes);
@@ -333,10 +381,14 @@ __global__ void __launch_bounds__(kThreads) wgrad_kernel(WgradArgs a) {
             }
             tc05::mma_commit(&mbar[s]);
         }
+        ph_prev = (parity_bits >> s) & 1u;
+        s_prev = s;
+        parity_bits ^= 1u << s;
+        if (++s == kStages) s = 0;
     }
     if (G > 0) {
-        if (!tc05::mbar_wait(&mbar[(G - 1) % kStages], (uint32_t)(((G - 1) / kStages) & 1)))
-            atomicOr(&g_error, 2u);
+        // the last stage's commit: buffer s_prev, parity ph_prev
+        if (!tc05::mbar_wait(&mbar[s_prev], ph_prev)) atomicOr(&g_error, 2u);
         tc05::fence_after_sync();
         const int m = blockIdx.x * 128 + warp * 32 + lane;
 #pragma unroll
