@@ -350,3 +350,24 @@ def benchmark(batch: int = 8, S: int = 64, repeats: int = 5, device: int = 0) ->
     return {"batch": batch, "edge": S, "train_step_ms": step_ms,
             "train_step_tflops": flops_total / (step_ms / 1e3) / 1e12, "layers": layers,
             "status": net.status()}
+
+
+def _one_step(batch: int = 8, S: int = 64, device: int = 0) -> None:
+    """One forward and backward pass of a random-init network on random
+    masks (the small case its kernels are profiled on)."""
+    import torch
+    dev = torch.device("cuda", device)
+    net = UNet(device, seed=0)
+    rng = np.random.default_rng(0)
+    solid = torch.tensor((rng.random((batch, S, S, S)) < 0.4).astype(np.uint8), device=dev)
+    feat = torch.zeros(batch, dtype=torch.float32, device=dev)
+    tgt = torch.zeros((batch, S, S, S, 4), dtype=torch.float32, device=dev)
+    out = net.forward(solid, feat)
+    net.backward(tgt, (solid == 0).to(torch.uint8), [1.0, 1.0, 1.0, 1.0])
+    torch.cuda.synchronize(dev)
+    print("one training step", batch, S, float(out.abs().mean()), "status", net.status())
+
+
+if __name__ == "__main__":
+    import sys
+    _one_step(*(int(x) for x in sys.argv[1:3]))
