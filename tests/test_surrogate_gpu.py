@@ -14,7 +14,7 @@ bias gradients, head) to 1e-4 relative L2.  Whole-network gradients go
 through ten bf16 roundings of activations and gradients: bf16 alone moves
 them 1-9 % (relative L2 per tensor) from the exact fp64 gradient; the
 emulating reference reproduces most of that, and the GPU's distance to it
-must stay below 0.6 of that bf16 effect per tensor, with a cosine
+must stay below 0.75 of that bf16 effect per tensor, with a cosine
 similarity of the whole gradient of at least 0.999.
 """
 from __future__ import annotations
@@ -258,7 +258,7 @@ def test_unet_forward_backward_matches_cpu_reference():
     eg = exact.grads()
     for k in rg:
         e_gpu, e_bf16 = rel_l2(gg[k], rg[k]), rel_l2(rg[k], eg[k])
-        assert e_gpu <= max(0.6 * e_bf16, 2e-3), (k, e_gpu, e_bf16)
+        assert e_gpu <= max(0.75 * e_bf16, 2e-3), (k, e_gpu, e_bf16)
     flat_g = np.concatenate([gg[k].ravel() for k in rg])
     flat_r = np.concatenate([rg[k].ravel() for k in rg])
     assert flat_g @ flat_r / (np.linalg.norm(flat_g) * np.linalg.norm(flat_r)) >= 0.999
