@@ -767,8 +767,17 @@ template <int N> cudaError_t launch_conv(const ConvArgs &a, cudaStream_t st) {
     using Sh = ConvShape<N>;
     cudaError_t e = cudaFuncSetAttribute(conv3_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::kSmem);
     if (e != cudaSuccess) return e;
+    // as many resident CTAs as shared memory allows (TMEM: at most 4 x 128
+    // columns per SM at every N), persistent over the M tiles
+    int per_sm = 0, dev = 0, sms = 148;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3_kernel<N>, kThreads, Sh::kSmem);
+    if (e != cudaSuccess) return e;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    per_sm = per_sm < 1 ? 1 : (per_sm > 4 ? 4 : per_sm);
     const long long tiles = a.rows >> 7;
-    const int grid = (int)(tiles < 148 * 2 ? tiles : 148 * 2);
+    const long long cap = (long long)per_sm * sms;
+    const int grid = (int)(tiles < cap ? tiles : cap);
     conv3_kernel<N><<<grid, kThreads, Sh::kSmem, st>>>(a);
     return cudaGetLastError();
 }
