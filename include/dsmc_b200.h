@@ -245,7 +245,10 @@ int dsmc_particles_init_field(dsmc_ctx *ctx, int sys_id, int64_t n, const float 
 /* Adds one system's per-voxel particle sums {count, sum vx, sum vy, sum vz}
  * (4 floats per voxel, geometry voxel order, 16-byte aligned) to field: the
  * steady fields that the warm-start surrogate learns are these sums over
- * many steps.  device != 0: field is device memory of the context's GPU. */
+ * many steps.  device != 0: field is device memory of the context's GPU and
+ * the call is asynchronous: the sums are added on the context's stream
+ * (dsmc_stream), so read them after a dsmc_sync or an event on that stream;
+ * device == 0: a host array, complete when the call returns. */
 int dsmc_field_accumulate(dsmc_ctx *ctx, int sys_id, float *field, int device);
 /* Replaces a system's particles by n particles in the reference's state-file
  * layout: r[3n], v[3n] fp64 (dsmc/dsmc_io.cpp:82-159).  Particle i gets id i. */

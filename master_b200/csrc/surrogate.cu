@@ -767,14 +767,15 @@ template <int N> cudaError_t launch_conv(const ConvArgs &a, cudaStream_t st) {
     using Sh = ConvShape<N>;
     cudaError_t e = cudaFuncSetAttribute(conv3_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, Sh::kSmem);
     if (e != cudaSuccess) return e;
-    // as many resident CTAs as shared memory allows (TMEM: at most 4 x 128
-    // columns per SM at every N), persistent over the M tiles
+    // two resident CTAs per SM, persistent over the M tiles: three or four
+    // (as shared memory would allow at N <= 64) measured slower, the gathers
+    // of more CTAs contending for L2 (c1c forward 2.0 -> 2.5 ms at four)
     int per_sm = 0, dev = 0, sms = 148;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, conv3_kernel<N>, kThreads, Sh::kSmem);
     if (e != cudaSuccess) return e;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    per_sm = per_sm < 1 ? 1 : (per_sm > 4 ? 4 : per_sm);
+    per_sm = per_sm < 1 ? 1 : (per_sm > 2 ? 2 : per_sm);
     const long long tiles = a.rows >> 7;
     const long long cap = (long long)per_sm * sms;
     const int grid = (int)(tiles < cap ? tiles : cap);

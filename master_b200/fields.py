@@ -129,9 +129,12 @@ class Ensemble:
                 self.ctx.check(self.ctx.lib.dsmc_field_accumulate(self.ctx.handle, S.id, C.c_void_p(f.data_ptr()), 1))
             samples += 1
             if samples % 64 == 0:  # fp32 partial sums folded into fp64 on the host
+                self.ctx.sync()    # the sums are written on the context's stream
                 for a, f in zip(acc, fields):
                     a += f.cpu().numpy()
                     f.zero_()
+                torch.cuda.synchronize()  # zeroed before the next sums
+        self.ctx.sync()
         for a, f in zip(acc, fields):
             a += f.cpu().numpy()
         self.samples = samples

@@ -37,6 +37,7 @@ def test_field_sums_equal_the_particles(precision, device):
         f = torch.zeros((V, 4), dtype=torch.float32, device="cuda")
         for _ in range(2):
             S.ctx.check(S.ctx.lib.dsmc_field_accumulate(S.ctx.handle, S.id, C.c_void_p(f.data_ptr()), 1))
+        S.ctx.sync()  # device mode is asynchronous on the context's stream
         got = f.cpu().numpy().astype(np.float64) / 2
     else:
         f = np.zeros((V, 4), np.float32)
