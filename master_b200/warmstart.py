@@ -48,7 +48,7 @@ def predict_fields(net, specs, geoms, batch: int = 1):
 
 def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: int = 1000, tol: float = 0.02,
             field_error: float = 0.0, max_field_error: float = 0.10, device: int = 0, rng_seed: int = 500,
-            capacity: tuple | None = None, force: bool = False, log=print) -> dict:
+            capacity: tuple | None = None, force: bool = False, measured: tuple | None = None, log=print) -> dict:
     """Runs the cold ensemble, then the warm one (one context at a time, so
     the two never share the device memory), `steps` steps each, and returns
     the steps and wall time to steady of both."""
@@ -77,7 +77,22 @@ def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: i
     use_net = force or field_error <= max_field_error
     rep["forced"] = bool(force and field_error > max_field_error)
     t0 = time.perf_counter()
-    preds = predict_fields(net, specs, geoms) if use_net else [None] * len(specs)
+    if measured is not None:
+        # control: seed from the steady fields measured by the DSMC itself (a
+        # separate cold ensemble, other seeds: `measured` = (transient steps,
+        # sampling steps)) instead of the network's prediction
+        warm.close()
+        ref = fields.Ensemble(specs, device=device, rng_seed=rng_seed + 100000, cold=True, geoms=geoms,
+                              capacity=capacity)
+        ref.ctx.step(measured[0])
+        sums = ref.accumulate_fields(measured[1], 10)
+        ref.close()
+        preds = [fields.finish_field(sm, (g.voxels > 0).astype(np.uint8).ravel()) for sm, g in zip(sums, geoms)]
+        rep["seeded_from"] = f"DSMC-measured fields ({measured[0]} + {measured[1]} steps)"
+        warm = fields.Ensemble(specs, device=device, rng_seed=rng_seed, cold=False, geoms=geoms, capacity=capacity)
+    else:
+        preds = predict_fields(net, specs, geoms) if use_net else [None] * len(specs)
+        rep["seeded_from"] = "surrogate" if use_net else "cold (fallback)"
     torch.cuda.synchronize()
     rep["inference_s"] = time.perf_counter() - t0
     fallback = []
@@ -153,6 +168,8 @@ def main(argv=None):
     ap.add_argument("--capacity", type=float, nargs=2, default=None, metavar=("FACTOR", "PAD"))
     ap.add_argument("--force", action="store_true",
                     help="seed from the surrogate even when its field error is above the fallback threshold")
+    ap.add_argument("--measured", type=int, nargs=2, default=None, metavar=("TRANSIENT", "SAMPLING"),
+                    help="control: seed from fields the DSMC measures itself instead of the network's")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     import torch
@@ -160,7 +177,8 @@ def main(argv=None):
     specs = fields.random_specs(a.geometries, a.edge, seed=5, porosity=(0.45, 0.75), knudsen=tuple(a.knudsen),
                                 per_cell=a.per_cell)
     rep = compare(net, specs, a.steps, every=a.every, field_error=float(held.get("field_error", 0.0)),
-                  capacity=tuple(a.capacity) if a.capacity else None, force=a.force)
+                  capacity=tuple(a.capacity) if a.capacity else None, force=a.force,
+                  measured=tuple(a.measured) if a.measured else None)
     rep["surrogate_held_out"] = held
     text = json.dumps(rep, default=float)
     if a.out:
