@@ -344,6 +344,39 @@ def surrogate_line(device):
     return b
 
 
+def run_warmstart(args, rank):
+    """The second half of the metric: steps and wall time until the x mass
+    flux stays within 2 % of its steady value for 1000 steps, from the cold
+    start (the reference's) and from the surrogate's warm start, on unseen
+    packed-sphere boxes of 64^3 (master_b200/warmstart.py)."""
+    if rank != 0:
+        return 0
+    import torch
+    from master_b200 import fields, warmstart
+    torch.cuda.set_device(0)
+    net, held = warmstart.load_net(ROOT / "master_b200" / "weights" / "surrogate_64.npz")
+    specs = fields.random_specs(args.warmstart_geometries, 64, seed=5, porosity=(0.45, 0.75), knudsen=(0.3, 3.0),
+                                per_cell=60)
+    rep = warmstart.compare(net, specs, 6000, every=10, field_error=float(held.get("field_error", 0.0)),
+                            capacity=(1.6, 12), log=lambda *a: None)
+    line = {"metric": "steps to steady x mass flux (2 % for 1000 steps), cold vs warm", "unit": "steps",
+            "higher_is_better": False, "data": "synthetic", "n_gpus": 1,
+            "config": {"workload": f"{len(specs)} unseen packed-sphere boxes of 64^3, porosity 0.45-0.75, "
+                                   f"radius 3-8, Kn 0.3-3, 60 simulators per cell", "particles": rep["particles"],
+                       "window": rep["window"], "hold": rep["hold"], "tol": rep["tol"]},
+            "cold": {k: rep["cold"][k] for k in ("steps_to_steady", "wall_s_to_steady", "ms_per_step",
+                                                 "window_noise")},
+            "warm": {k: rep["warm"][k] for k in ("steps_to_steady", "wall_s_to_steady", "ms_per_step",
+                                                 "window_noise")},
+            "ratio_steps": rep["ratio_steps"], "seeded_from": rep.get("seeded_from"),
+            "surrogate_field_error": rep["surrogate_field_error"], "inference_s": rep["inference_s"],
+            "seed_s": rep["seed_s"],
+            "cold_flux_over_steady": rep["cold"]["flux_over_steady_window"][:40:2],
+            "warm_flux_over_steady": rep["warm"]["flux_over_steady_window"][:40:2]}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -357,10 +390,16 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--no-configs", action="store_true", help="skip the packed_64 and batched-ensemble lines")
+    ap.add_argument("--warmstart", action="store_true",
+                    help="instead of the throughput line: steps and wall time to a steady flux, cold against "
+                         "the surrogate's warm start, on unseen 64^3 packs (about 10 minutes)")
+    ap.add_argument("--warmstart-geometries", type=int, default=384)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
     world, rank, local, pg = dist_setup(args)
+    if args.warmstart:
+        return run_warmstart(args, rank)
     if args.impl == "reference":
         rc = run_reference_arm(args, world, rank, pg)
         if pg is not None:
