@@ -85,7 +85,7 @@ def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: i
         ref = fields.Ensemble(specs, device=device, rng_seed=rng_seed + 100000, cold=True, geoms=geoms,
                               capacity=capacity)
         ref.ctx.step(measured[0])
-        sums = ref.accumulate_fields(measured[1], 10)
+        sums = ref.accumulate_fields(measured[1], 20)
         ref.close()
         preds = [fields.finish_field(sm, (g.voxels > 0).astype(np.uint8).ravel()) for sm, g in zip(sums, geoms)]
         rep["seeded_from"] = f"DSMC-measured fields ({measured[0]} + {measured[1]} steps)"
