@@ -287,7 +287,7 @@ def other_configs(args, device):
                      "particles": S.num_molecules, "dtype": "f64" if prec == capi.PREC_FP64 else
                      "fp32 state + fp64 tallies"}
         S.ctx.close()
-    # the large geometry in the fp64 reference arithmetic (the judge of the
+    # the large geometry in the fp64 reference arithmetic (the yardstick of the
     # split-precision numbers above)
     w256 = workloads.PACKED_256
     S = System(w256.settings(rng_seed=5, statistics_interval=100), w256.geometry(), device=device,

@@ -5,7 +5,7 @@ against the fp64 path's on the same workload.
 
 The fp64 path reproduces the reference's own routines operation by operation
 (positions bit-identical, velocities within 1e-12, every integer index and
-counter identical), so it is the judge at sizes the reference cannot run.
+counter identical), so it is the yardstick at sizes the reference cannot run.
 Both precisions run the same `replicas` draw seeds as systems of one context
 each; the flux of each replica is its crossing count over [from, steps]
 (MoleculeMover::count_periodic, dsmc/moleculemover.h:29-38) times F_N over
@@ -15,7 +15,7 @@ precisions' trajectories are uncorrelated (a rounding that moves one
 particle across a cell face changes its cell's collision partners), so the
 two ensemble means are compared as independent samples:
   rel_diff = (split - fp64) / fp64, with a 95 % interval 1.96 * se_rel.
-The north-star bar is |rel_diff| within 2 % with that interval inside 2 %.
+The split precision is held to |rel_diff| within 2 % with that interval inside 2 %.
 Collision rates and temperatures are compared the same way.
 """
 from __future__ import annotations

@@ -5,7 +5,7 @@ The fp64 path reproduces the reference's own routines bit for bit
 (tests/test_parity_gpu.py: positions identical, velocities within 1e-12,
 integer voxel and cell indices and every counter identical).  The draws of
 both precisions are keyed by particle id, cell and step, never by precision,
-so the fp64 path judges the production kernels at full size:
+so the fp64 path serves as the yardstick of the production kernels at full size:
 
 * packed_64: 64^3 voxels, r = 4 voxel spheres to porosity 0.6, 32^3 cells,
   ~3.9e5 particles (the plain-DSMC configuration);
