@@ -36,7 +36,7 @@ def windowed_flux(counts: np.ndarray, every: int, window: int, weight: float, dt
 @dataclass
 class Steady:
     steps: int | None        # first window start from which the flux stays within tol (None: never)
-    value: float             # the steady value it was judged against
+    value: float             # the steady value it was compared against
     series: np.ndarray       # ensemble-mean windowed flux per sampled window start
     stderr: np.ndarray       # its standard error over the replicas
     every: int
@@ -51,13 +51,39 @@ def steps_to_steady(counts: np.ndarray, every: int, steady_value: float, weight:
     mean = f.mean(axis=1)
     se = f.std(axis=1, ddof=1) / np.sqrt(f.shape[1]) if f.shape[1] > 1 else np.zeros_like(mean)
     ok = np.abs(mean - steady_value) <= tol * abs(steady_value)
+    return Steady(first_steady(ok, every, hold), steady_value, mean, se, every)
+
+
+def first_steady(ok: np.ndarray, every: int, hold: int) -> int | None:
+    """The first sampled step t0 with ok[t] for every sampled t in [t0, t0 + hold]."""
     h = hold // every
-    first = None
     for i in range(0, len(ok) - h):
         if ok[i:i + h + 1].all():
-            first = i * every
-            break
-    return Steady(first, steady_value, mean, se, every)
+            return i * every
+    return None
+
+
+@dataclass
+class TotalSteady:
+    steps: int | None        # steps to steady of the total (None: never within the record)
+    total: np.ndarray        # the systems' summed windowed flux over their summed steady flux
+    noise: float             # median standard error of `total` per window start
+
+
+def total_steps_to_steady(counts: np.ndarray, every: int, weights: np.ndarray, steady_values: np.ndarray,
+                          dt: float, window: int = 1000, hold: int = 1000, tol: float = 0.02) -> TotalSteady:
+    """Steps to steady of an ensemble of different systems (one geometry
+    each): the summed windowed flux sum_j F_W,j(t), normalised by the summed
+    steady flux sum_j s_j, must stay within `tol` of 1.  weights: F_N of
+    each system.  The systems' windowed fluxes are independent, so the
+    variance of the total is the sum of theirs, estimated from the spread of
+    F_W,j / s_j over the systems."""
+    f = windowed_flux(counts, every, window, 1.0, dt) * np.asarray(weights, np.float64)
+    sv = np.asarray(steady_values, np.float64)
+    tot = f.sum(axis=1) / sv.sum()
+    fn = f / sv
+    se = np.sqrt(((fn - fn.mean(axis=1, keepdims=True)) ** 2).sum(axis=1)) / f.shape[1]
+    return TotalSteady(first_steady(np.abs(tot - 1.0) <= tol, every, hold), tot, float(np.median(se)))
 
 
 def steady_flux(counts: np.ndarray, every: int, start: int, weight: float, dt: float):

@@ -124,27 +124,16 @@ def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: i
     for name in ("cold", "warm"):
         c = out[name]["counts"].astype(np.float64)
         # the ensemble's total flux over its total steady flux
-        f = steady.windowed_flux(c, every, window, 1.0, dt) * weights
-        tot = f.sum(axis=1) / steady_val.sum()
-        ok = np.abs(tot - 1.0) <= tol
-        h = hold // every
-        first = None
-        for i in range(0, len(ok) - h):
-            if ok[i:i + h + 1].all():
-                first = i * every
-                break
-        # per-window noise of the total: geometries' windowed fluxes are
-        # independent, so their variance adds
-        fn = f / steady_val
-        se = np.sqrt(((fn - fn.mean(axis=1, keepdims=True)) ** 2).sum(axis=1)) / f.shape[1]
+        r = steady.total_steps_to_steady(c, every, weights, steady_val, dt, window, hold, tol)
+        first = r.steps
         ms_step = 1e3 * out[name]["seconds"] / steps
         # short windows resolve the transient itself
         f100 = steady.windowed_flux(c, every, 100, 1.0, dt) * weights
         res[name] = {"steps_to_steady": first, "ms_per_step": ms_step,
                      "wall_s_to_steady": None if first is None else first * ms_step / 1e3,
-                     "flux_over_steady_window": tot[::max(1, 100 // every)].tolist(),
+                     "flux_over_steady_window": r.total[::max(1, 100 // every)].tolist(),
                      "flux_over_steady_100step": (f100.sum(axis=1) / steady_val.sum())[::max(1, 100 // every)].tolist(),
-                     "window_noise": float(np.median(se)),
+                     "window_noise": r.noise,
                      "error_bits": out[name]["error_bits"]}
     if res["warm"]["wall_s_to_steady"] is not None:
         res["warm"]["wall_s_to_steady"] += rep["inference_s"] + rep["seed_s"]

@@ -41,3 +41,40 @@ def test_steady_flux_and_its_error():
     c = t[:, None] * rates[None, :]
     m, se, per = steady.steady_flux(c, every, 1000, weight=1.0, dt=1.0)
     assert np.allclose(per, rates) and abs(m - rates.mean()) < 1e-12 and se > 0
+
+
+def test_total_steps_to_steady_of_uneven_systems():
+    """The ensemble criterion of the warm start: systems of different
+    weight and steady flux, summed, against the summed steady flux."""
+    every, window, hold, tau = 10, 1000, 1000, 300.0
+    t = np.arange(0, 8001, every, dtype=np.float64)
+    rates = np.array([1.0, 3.0, 0.5, 2.0])
+    weights = np.array([2.0, 1.0, 4.0, 0.5])
+    c = (t - tau * (1 - np.exp(-t / tau)))[:, None] * rates[None, :]
+    sv = weights * rates
+    r = steady.total_steps_to_steady(c, every, weights, sv, 1.0, window, hold, 0.02)
+    # every system approaches its rate on the same exponential, so the
+    # normalised total does too: the single-system answer
+    expect = tau * np.log(tau / window * (1 - np.exp(-window / tau)) / 0.02)
+    assert abs(r.steps - expect) <= every
+    assert abs(r.total[-1] - 1.0) < 1e-9 and r.noise < 1e-9
+    # a system that never settles holds the total off its steady value
+    c2 = c.copy()
+    c2[:, 1] *= 1.2
+    assert steady.total_steps_to_steady(c2, every, weights, sv, 1.0, window, hold, 0.02).steps is None
+
+
+def test_total_noise_estimates_the_spread_of_the_total():
+    every, window = 10, 1000
+    t = np.arange(0, 6001, every)
+    rng = np.random.default_rng(1)
+    n = 256
+    # independent Poisson crossings, 2 per step on average, per system
+    c = np.vstack([np.zeros(n), rng.poisson(2.0 * every, (len(t) - 1, n)).cumsum(0)])
+    sv = np.full(n, 2.0)
+    r = steady.total_steps_to_steady(c, every, np.ones(n), sv, 1.0, window, 1000, 0.02)
+    # a window holds 2000 crossings per system: relative sd sqrt(2000)/2000
+    # per system, over sqrt(n) for the total
+    expect = np.sqrt(2000.0) / 2000.0 / np.sqrt(n)
+    assert 0.85 * expect < r.noise < 1.15 * expect
+    assert r.steps == 0
