@@ -242,6 +242,18 @@ int dsmc_particles_init(dsmc_ctx *ctx, int sys_id, int64_t n);
  * one counter-based stream per particle, as dsmc_particles_init's. */
 int dsmc_particles_init_field(dsmc_ctx *ctx, int sys_id, int64_t n, const float *weight, const float *drift,
                               int device);
+/* Batched dsmc_particles_init / dsmc_particles_init_field for the systems of
+ * a multi-system context: the listed systems (count distinct ids, no slabs)
+ * get the same particles as from one call each (a system's draws depend only
+ * on its seed, count and field), but the context's other particles are
+ * staged and all of them re-laid out once, not once per system.  n: count
+ * values, n[i] < 0 or n null the reference's count.  _field: weights[i] and
+ * drifts[i] as dsmc_particles_init_field's weight and drift for system
+ * sys_ids[i], every field checked before any particle is replaced.  A
+ * system listed twice is DSMC_ERR_ARG. */
+int dsmc_particles_init_many(dsmc_ctx *ctx, int count, const int *sys_ids, const int64_t *n);
+int dsmc_particles_init_field_many(dsmc_ctx *ctx, int count, const int *sys_ids, const int64_t *n,
+                                   const float *const *weights, const float *const *drifts, int device);
 /* Adds one system's per-voxel particle sums {count, sum vx, sum vy, sum vz}
  * (4 floats per voxel, geometry voxel order, 16-byte aligned) to field: the
  * steady fields that the warm-start surrogate learns are these sums over

@@ -46,7 +46,8 @@ EXPORTED = [
     "dsmc_tocontinue_write", "dsmc_continue_from", "dsmc_checkpoint_save", "dsmc_checkpoint_load",
     "dsmc_profile_sums_get", "dsmc_profiles_finish", "dsmc_profiles_get", "dsmc_measures_get",
     "dsmc_system_add_slab", "dsmc_exchange_take", "dsmc_exchange_put", "dsmc_particles_init_field",
-    "dsmc_field_accumulate", "dsmc_tuning_set", "dsmc_tuning_get",
+    "dsmc_field_accumulate", "dsmc_tuning_set", "dsmc_tuning_get", "dsmc_particles_init_many",
+    "dsmc_particles_init_field_many",
 ]
 # every entry point declared in include/dsmc_surrogate.h
 EXPORTED_SURROGATE = [
@@ -190,6 +191,9 @@ def load() -> C.CDLL:
         "dsmc_exchange_take": [_P, C.c_int64, C.c_void_p, C.c_int, C.POINTER(C.c_int64)],
         "dsmc_exchange_put": [_P, C.c_int, C.c_int64, C.c_void_p, C.c_int],
         "dsmc_particles_init_field": [_P, C.c_int, C.c_int64, C.c_void_p, C.c_void_p, C.c_int],
+        "dsmc_particles_init_many": [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int64)],
+        "dsmc_particles_init_field_many": [_P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int64),
+                                           C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_int],
         "dsmc_field_accumulate": [_P, C.c_int, C.c_void_p, C.c_int],
         "dsmc_tuning_set": [_P, C.POINTER(Tuning)],
         "dsmc_tuning_get": [_P, C.POINTER(Tuning), C.POINTER(Tuning)],

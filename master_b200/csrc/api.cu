@@ -331,10 +331,13 @@ int relayout(dsmc_ctx *ctx, long long total) {
 }
 
 // Stages every present particle (all systems, or all but `skip`) into fA/fB.
-int stage_present(dsmc_ctx *ctx, long long extra, int skip, long long *staged) {
+// Every particle of the systems not marked in `skip` (skip.empty(): all)
+// into the staging buffer, sized for `extra` more records.
+static int stage_present_set(dsmc_ctx *ctx, long long extra, const std::vector<char> &skip, long long *staged) {
+    auto skipped = [&](size_t s) { return s < skip.size() && skip[s]; };
     long long present = 0;
     for (size_t s = 0; s < ctx->systems.size(); ++s)
-        if ((int)s != skip) present += ctx->systems[s]->num_particles;
+        if (!skipped(s)) present += ctx->systems[s]->num_particles;
     Status st;
     cudaError_t e;
     st = read_status(ctx, &e);
@@ -351,7 +354,7 @@ int stage_present(dsmc_ctx *ctx, long long extra, int skip, long long *staged) {
     *staged = 0;
     if (ctx->A0.p && ctx->num_cells) {
         for (size_t s = 0; s < ctx->systems.size(); ++s) {
-            if ((int)s == skip) continue;
+            if (skipped(s)) continue;
             SysHost &h = *ctx->systems[s];
             if (h.active_end <= h.active_begin) continue;
             e = is_fp64(ctx) ? fp64::launch_gather(cell_arrays(ctx), particle_arrays(ctx), ctx->cur, ctx->cphase,
@@ -371,6 +374,15 @@ int stage_present(dsmc_ctx *ctx, long long extra, int skip, long long *staged) {
         *staged = (long long)got;
     }
     return DSMC_OK;
+}
+
+int stage_present(dsmc_ctx *ctx, long long extra, int skip, long long *staged) {
+    std::vector<char> set;
+    if (skip >= 0 && skip < (int)ctx->systems.size()) {
+        set.assign(ctx->systems.size(), 0);
+        set[skip] = 1;
+    }
+    return stage_present_set(ctx, extra, set, staged);
 }
 
 // Runs the collide + sample of the last step if it is still pending.
@@ -520,85 +532,93 @@ int flush_pending(dsmc_ctx *ctx) {
     return DSMC_OK;
 }
 
+// Grows b to hold `need` elements (at least doubling, so that n appends cost
+// O(n) copies in all), keeping its first `keep` elements.
+template <class T> static cudaError_t grow_keep(DevBuf<T> &b, size_t need, size_t keep, cudaStream_t st) {
+    if (b.p && need <= b.n) return cudaSuccess;
+    const size_t cap = std::max<size_t>(std::max<size_t>(need, 2 * b.n), 1);
+    T *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, cap * sizeof(T));
+    if (e != cudaSuccess) return e;
+    if (keep && b.p) {
+        e = cudaMemcpyAsync(p, b.p, keep * sizeof(T), cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the copy is done before the old buffer goes
+    }
+    if (e != cudaSuccess) {
+        cudaFree(p);
+        return e;
+    }
+    b.release();
+    b.p = p;
+    b.n = cap;
+    return cudaSuccess;
+}
+
+// Appends the cells of the context's last system (just added) after those of
+// the systems before it, which keep their cell indices, cell state, moment
+// sums, tallies and device cell maps: systems are only ever appended, so
+// only the new system's cells are built on the host and uploaded (adding n
+// systems one by one costs O(total cells), not O(n * total cells)).
+// Occupancy sets are cleared for every cell; the caller re-lays the
+// particles out.
 int rebuild_cells(dsmc_ctx *ctx) {
     ctx->drop_graphs();
-    // Keep the cell state and tallies of the systems already present: a new
-    // system's cells are appended after theirs.
     const int C_old = ctx->num_cells;
-    std::vector<double4> old_state(C_old);
-    std::vector<double> old_mom(8 * (size_t)C_old);
-    std::vector<SysTally> old_tally(ctx->systems.size() > 0 ? ctx->systems.size() - 1 : 0);
-    if (C_old > 0) {
-        CK(cudaMemcpyAsync(old_state.data(), ctx->state.p, C_old * sizeof(double4), cudaMemcpyDeviceToHost, ctx->stream));
-        CK(cudaMemcpyAsync(old_mom.data(), ctx->mom.p, 8 * C_old * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    }
-    if (!old_tally.empty())
-        CK(cudaMemcpyAsync(old_tally.data(), ctx->tally.p, old_tally.size() * sizeof(SysTally), cudaMemcpyDeviceToHost,
-                           ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    // Concatenate the active cells of all systems.
-    int C = 0;
-    for (auto &s : ctx->systems) C += (int)s->cell_global.size();
-    std::vector<int4> h_meta(C, int4{0, 0, 0, 0});  // {base, cap: set by each layout; global, sys}
-    std::vector<int> pix(C);
-    std::vector<double4> state(C);
-    int a = 0;
-    for (size_t si = 0; si < ctx->systems.size(); ++si) {
-        SysHost &s = *ctx->systems[si];
-        s.active_begin = a;
-        s.pixel_sum = 0;
-        for (size_t c = 0; c < s.cell_global.size(); ++c, ++a) {
-            h_meta[a].z = s.cell_global[c];
-            h_meta[a].w = (int)si;
-            pix[a] = s.pixels[c];
-            s.pixel_sum += s.pixels[c];
-            // Cell::vr_max starts at 3*sqrt(T) (dsmc/system.cpp:451,477)
-            state[a] = double4{s.vr_max0, 0.0, s.coeff[c], 0.0};
-        }
-        s.active_end = a;
-        s.dev.active_begin = s.active_begin;
-        s.dev.active_end = s.active_end;
-        std::vector<int> map_abs(s.cell_map.size());
-        for (size_t g = 0; g < s.cell_map.size(); ++g)
-            map_abs[g] = s.cell_map[g] < 0 ? s.cell_map[g] : s.cell_map[g] + s.active_begin;
-        CK(s.cell_map_dev.ensure(map_abs.size()));
-        CK(cudaMemcpyAsync(s.cell_map_dev.p, map_abs.data(), map_abs.size() * sizeof(int), cudaMemcpyHostToDevice,
-                           ctx->stream));
-        s.dev.cell_map = s.cell_map_dev.p;
-        CK(cudaStreamSynchronize(ctx->stream));
-    }
-    ctx->num_cells = C;
+    const int si = (int)ctx->systems.size() - 1;
+    SysHost &s = *ctx->systems[si];
+    const int nc = (int)s.cell_global.size();
+    const int C = C_old + nc;
     const size_t Cn = std::max(C, 1);
-    CK(ctx->meta.alloc(Cn));
-    CK(ctx->pix.alloc(Cn));
-    CK(ctx->state.alloc(Cn));
+    CK(grow_keep(ctx->meta, Cn, C_old, ctx->stream));
+    CK(grow_keep(ctx->pix, Cn, C_old, ctx->stream));
+    CK(grow_keep(ctx->state, Cn, C_old, ctx->stream));
+    CK(grow_keep(ctx->mom, 8 * Cn, 8 * (size_t)C_old, ctx->stream));
     for (int q = 0; q < 3; ++q) {
-        CK(ctx->bot[q].alloc(Cn));
-        CK(ctx->top[q].alloc(Cn));
+        CK(grow_keep(ctx->bot[q], Cn, 0, ctx->stream));
+        CK(grow_keep(ctx->top[q], Cn, 0, ctx->stream));
     }
-    CK(ctx->mom.alloc(8 * Cn));
-    CK(ctx->room.alloc(Cn));
-    CK(ctx->hist.alloc(Cn));
-    if (C) {
-        if (C_old > 0 && C_old <= C)
-            for (int q = 0; q < C_old; ++q) state[q] = old_state[q];
-        CK(cudaMemcpyAsync(ctx->meta.p, h_meta.data(), C * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemcpyAsync(ctx->pix.p, pix.data(), C * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemcpyAsync(ctx->state.p, state.data(), C * sizeof(double4), cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemsetAsync(ctx->mom.p, 0, 8 * C * sizeof(double), ctx->stream));
+    CK(grow_keep(ctx->room, Cn, 0, ctx->stream));
+    CK(grow_keep(ctx->hist, Cn, 0, ctx->stream));
+    CK(grow_keep(ctx->tally, std::max<size_t>(ctx->systems.size(), 1), (size_t)si, ctx->stream));
+    CK(cudaMemsetAsync(ctx->tally.p + si, 0, sizeof(SysTally), ctx->stream));
+    // the new system's cells
+    s.active_begin = C_old;
+    s.active_end = C;
+    s.pixel_sum = 0;
+    std::vector<int4> h_meta(std::max(nc, 1), int4{0, 0, 0, 0});  // {base, cap: set by each layout; global, sys}
+    std::vector<int> pix(std::max(nc, 1));
+    std::vector<double4> state(std::max(nc, 1));
+    for (int c = 0; c < nc; ++c) {
+        h_meta[c].z = s.cell_global[c];
+        h_meta[c].w = si;
+        pix[c] = s.pixels[c];
+        s.pixel_sum += s.pixels[c];
+        // Cell::vr_max starts at 3*sqrt(T) (dsmc/system.cpp:451,477)
+        state[c] = double4{s.vr_max0, 0.0, s.coeff[c], 0.0};
+    }
+    s.dev.active_begin = s.active_begin;
+    s.dev.active_end = s.active_end;
+    std::vector<int> map_abs(s.cell_map.size());
+    for (size_t g = 0; g < s.cell_map.size(); ++g)
+        map_abs[g] = s.cell_map[g] < 0 ? s.cell_map[g] : s.cell_map[g] + s.active_begin;
+    CK(s.cell_map_dev.ensure(map_abs.size()));
+    CK(cudaMemcpyAsync(s.cell_map_dev.p, map_abs.data(), map_abs.size() * sizeof(int), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    s.dev.cell_map = s.cell_map_dev.p;
+    ctx->num_cells = C;
+    if (nc) {
+        CK(cudaMemcpyAsync(ctx->meta.p + C_old, h_meta.data(), nc * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->pix.p + C_old, pix.data(), nc * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->state.p + C_old, state.data(), nc * sizeof(double4), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        CK(cudaMemsetAsync(ctx->mom.p + 8 * (size_t)C_old, 0, 8 * (size_t)nc * sizeof(double), ctx->stream));
+    }
+    if (C)
         for (int q = 0; q < 3; ++q) {
             CK(cudaMemsetAsync(ctx->bot[q].p, 0, C * sizeof(unsigned), ctx->stream));
             CK(cudaMemsetAsync(ctx->top[q].p, 0, C * sizeof(unsigned), ctx->stream));
         }
-        if (C_old > 0 && C_old <= C)
-            CK(cudaMemcpyAsync(ctx->mom.p, old_mom.data(), 8 * C_old * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    }
-    CK(ctx->tally.alloc(std::max<size_t>(ctx->systems.size(), 1)));
-    CK(cudaMemsetAsync(ctx->tally.p, 0, std::max<size_t>(ctx->systems.size(), 1) * sizeof(SysTally), ctx->stream));
-    if (!old_tally.empty())
-        CK(cudaMemcpyAsync(ctx->tally.p, old_tally.data(), old_tally.size() * sizeof(SysTally), cudaMemcpyHostToDevice,
-                           ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));  // the host vectors above are released on return
     return upload_sys_table(ctx);
 }
 
@@ -1029,73 +1049,183 @@ int dsmc_particles_init(dsmc_ctx *ctx, int sys_id, int64_t n) {
     return place_particles(ctx, sys_id, n, nullptr, nullptr);
 }
 
-// Warm start: n particles drawn from a per-voxel weight and drift field
-// instead of System::setup_molecules' uniform Maxwellian at rest
-// (dsmc/system.cpp:398-430).  The weights of non-empty voxels are ignored.
-int dsmc_particles_init_field(dsmc_ctx *ctx, int sys_id, int64_t n, const float *weight, const float *drift,
-                              int device) {
-    if (!ctx || sys_id < 0 || sys_id >= (int)ctx->systems.size() || !weight || !drift) return DSMC_ERR_ARG;
-    SysHost &h = *ctx->systems[sys_id];
-    if (h.slab) return fail(ctx, DSMC_ERR_CONFIG, "a slab is initialised by dsmc_particles_init or _set");
-    if (n < 0) n = h.expected;
-    if (n > 0xffffffffLL) return fail(ctx, DSMC_ERR_CAPACITY, "at most 2^32 particles per system");
-    cudaSetDevice(ctx->device);
+// One system of a batched initialisation: its count and, for a warm start,
+// its per-voxel field (weight null: System::setup_molecules' uniform
+// Maxwellian at rest, dsmc/system.cpp:398-430).
+struct InitItem {
+    int sys;
+    long long n;
+    const float *weight, *drift;
+};
+
+// The weights of system h's empty voxels (host copy of a host or device
+// field) and their sum; the weights of non-empty voxels are ignored.
+static int field_weights(dsmc_ctx *ctx, const SysHost &h, const float *weight, int device, std::vector<float> &w,
+                         std::vector<uint8_t> &vox) {
     const long long V = (long long)h.n[0] * h.n[1] * h.n[2];
-    std::vector<float> w(V);
-    std::vector<uint8_t> vox(V);
+    w.resize(V);
+    vox.resize(V);
     if (device) {
         CK(cudaMemcpy(w.data(), weight, V * sizeof(float), cudaMemcpyDeviceToHost));
     } else {
         std::memcpy(w.data(), weight, V * sizeof(float));
     }
     CK(cudaMemcpy(vox.data(), h.vox.p, V, cudaMemcpyDeviceToHost));
-    std::vector<double> cdf(V + 1);
-    cdf[0] = 0.0;
     for (long long i = 0; i < V; ++i) {
         const float x = w[i];
-        const double wi = (vox[i] == DSMC_VOX_EMPTY && std::isfinite(x) && x > 0.0f) ? (double)x : 0.0;
-        cdf[i + 1] = cdf[i] + wi;
+        if (!(vox[i] == DSMC_VOX_EMPTY && std::isfinite(x) && x > 0.0f)) w[i] = 0.0f;
     }
-    if (!(cdf[V] > 0.0)) return fail(ctx, DSMC_ERR_STATE, "the weight field is zero in every empty voxel");
-    DevBuf<double> dcdf;
-    DevBuf<float> ddrift;
-    CK(dcdf.ensure(V + 1));
-    CK(cudaMemcpyAsync(dcdf.p, cdf.data(), (V + 1) * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    const float *drift_dev = drift;
-    if (!device) {
-        CK(ddrift.ensure(3 * V));
-        CK(cudaMemcpyAsync(ddrift.p, drift, 3 * V * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
-        drift_dev = ddrift.p;
+    return DSMC_OK;
+}
+
+// Replaces the particles of every listed system (distinct, not slabs) by
+// freshly drawn ones: one staging of the other systems' particles, the
+// draws of each listed system appended in list order, one re-layout.  A
+// system's particles depend only on its seed, count and field (one
+// counter-based stream per particle id), so the result is that of one call
+// per system, without re-laying the whole context out once per system.
+static int init_systems(dsmc_ctx *ctx, const std::vector<InitItem> &items, int device) {
+    cudaSetDevice(ctx->device);
+    std::vector<char> set(ctx->systems.size(), 0);
+    long long extra = 0;
+    bool any_field = false;
+    std::vector<float> w;
+    std::vector<uint8_t> vox;
+    for (const InitItem &it : items) {
+        set[it.sys] = 1;
+        extra += it.n;
+        if (!it.weight) continue;
+        any_field = true;
+        // every field is checked before anything is staged
+        int rc = field_weights(ctx, *ctx->systems[it.sys], it.weight, device, w, vox);
+        if (rc) return rc;
+        double total = 0.0;
+        for (float x : w) total += (double)x;
+        if (!(total > 0.0)) return fail(ctx, DSMC_ERR_STATE, "the weight field is zero in every empty voxel");
     }
     int rc = flush_pending(ctx);
     if (rc) return rc;
     long long staged = 0;
-    rc = stage_present(ctx, n, sys_id, &staged);
+    rc = stage_present_set(ctx, extra, set, &staged);
     if (rc) return rc;
     const size_t half = ctx->rec_half();
-    if (n) {
-        const cudaError_t e =
-            is_fp64(ctx) ? fp64::launch_init_field(ctx->sys_dev.p, sys_id, h.sqrt_t_over_m, n, dcdf.p, drift_dev, V,
-                                                   ctx->fA.p + staged * half, ctx->fB.p + staged * half,
-                                                   ctx->fkey.p + staged, ctx->hist.p, &ctx->status.p->error,
-                                                   ctx->stream)
-                         : split32::launch_init_field(ctx->sys_dev.p, sys_id, h.sqrt_t_over_m, n, dcdf.p, drift_dev, V,
-                                                      ctx->fA.p + staged * half, ctx->fB.p + staged * half,
-                                                      ctx->fkey.p + staged, ctx->hist.p, &ctx->status.p->error,
-                                                      ctx->stream);
+    long long at = staged;
+    DevBuf<double> dcdf;
+    DevBuf<float> ddrift;
+    std::vector<double> cdf;
+    for (const InitItem &it : items) {
+        SysHost &h = *ctx->systems[it.sys];
+        unsigned char *A = ctx->fA.p + at * half, *B = ctx->fB.p + at * half;
+        int *key = ctx->fkey.p + at;
+        cudaError_t e = cudaSuccess;
+        if (!it.weight) {
+            if (it.n)
+                e = is_fp64(ctx) ? fp64::launch_init(ctx->sys_dev.p, it.sys, h.sqrt_t_over_m, it.n, A, B, key,
+                                                     ctx->hist.p, &ctx->status.p->error, ctx->stream)
+                                 : split32::launch_init(ctx->sys_dev.p, it.sys, h.sqrt_t_over_m, it.n, A, B, key,
+                                                        ctx->hist.p, &ctx->status.p->error, ctx->stream);
+        } else {
+            rc = field_weights(ctx, h, it.weight, device, w, vox);
+            if (rc) return rc;
+            const long long V = (long long)w.size();
+            cdf.resize(V + 1);
+            cdf[0] = 0.0;
+            for (long long i = 0; i < V; ++i) cdf[i + 1] = cdf[i] + (double)w[i];
+            // the host buffers may be reused once an upload from pageable
+            // memory returns; the device buffers once the stream has reached
+            // the next upload, which follows this system's draws
+            CK(dcdf.ensure(V + 1));
+            CK(cudaMemcpyAsync(dcdf.p, cdf.data(), (V + 1) * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+            const float *drift_dev = it.drift;
+            if (!device) {
+                CK(ddrift.ensure(3 * V));
+                CK(cudaMemcpyAsync(ddrift.p, it.drift, 3 * V * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+                drift_dev = ddrift.p;
+            }
+            if (it.n)
+                e = is_fp64(ctx) ? fp64::launch_init_field(ctx->sys_dev.p, it.sys, h.sqrt_t_over_m, it.n, dcdf.p,
+                                                           drift_dev, V, A, B, key, ctx->hist.p,
+                                                           &ctx->status.p->error, ctx->stream)
+                                 : split32::launch_init_field(ctx->sys_dev.p, it.sys, h.sqrt_t_over_m, it.n, dcdf.p,
+                                                              drift_dev, V, A, B, key, ctx->hist.p,
+                                                              &ctx->status.p->error, ctx->stream);
+        }
         CK(e);
+        at += it.n;
     }
     cudaError_t e;
     Status st = read_status(ctx, &e);
     CK(e);
     if (st.error & DSMC_EBIT_FATAL) {
         cudaMemsetAsync(ctx->status.p, 0, sizeof(unsigned), ctx->stream);
-        return fail(ctx, DSMC_ERR_STATE, (st.error & DSMC_EBIT_NAN) ? "a drift is not finite"
-                                                                    : "a particle landed in a cell with no free volume");
+        return fail(ctx, DSMC_ERR_STATE,
+                    (st.error & DSMC_EBIT_NAN) ? (any_field ? "a drift is not finite" : "a velocity is not finite")
+                                               : "a particle landed in a solid voxel or a cell with no free volume");
     }
-    h.num_particles = n;
-    h.id_count = (uint32_t)n;
-    return relayout(ctx, staged + n);
+    for (const InitItem &it : items) {
+        SysHost &h = *ctx->systems[it.sys];
+        h.num_particles = it.n;
+        h.id_count = (uint32_t)it.n;
+    }
+    return relayout(ctx, at);
+}
+
+// The listed systems as InitItems: distinct, not slabs, n < 0 (or no n) the
+// reference's count, at most 2^32 particles each.
+static int init_items(dsmc_ctx *ctx, int count, const int *sys_ids, const int64_t *n, const float *const *weights,
+                      const float *const *drifts, std::vector<InitItem> &items) {
+    if (count < 0 || (count && !sys_ids)) return DSMC_ERR_ARG;
+    std::vector<char> seen(ctx->systems.size(), 0);
+    items.clear();
+    for (int i = 0; i < count; ++i) {
+        const int s = sys_ids[i];
+        if (s < 0 || s >= (int)ctx->systems.size()) return DSMC_ERR_ARG;
+        if (seen[s]) return fail(ctx, DSMC_ERR_ARG, "a system is listed twice");
+        seen[s] = 1;
+        SysHost &h = *ctx->systems[s];
+        if (h.slab) return fail(ctx, DSMC_ERR_CONFIG, "a slab is initialised by dsmc_particles_init or _set");
+        long long k = n && n[i] >= 0 ? (long long)n[i] : h.expected;
+        if (k > 0xffffffffLL) return fail(ctx, DSMC_ERR_CAPACITY, "at most 2^32 particles per system");
+        InitItem it{s, k, nullptr, nullptr};
+        if (weights) {
+            if (!drifts || !weights[i] || !drifts[i]) return DSMC_ERR_ARG;
+            it.weight = weights[i];
+            it.drift = drifts[i];
+        } else if (h.settings.max_molecules_per_node > 0 && k > h.settings.max_molecules_per_node) {
+            char buf[200];
+            std::snprintf(buf, sizeof(buf), "Node 0 wants to create %lld molecules (MAX_MOLECULE_NUM=%d)", k,
+                          h.settings.max_molecules_per_node);
+            return fail(ctx, DSMC_ERR_CAPACITY, buf);
+        }
+        items.push_back(it);
+    }
+    return DSMC_OK;
+}
+
+int dsmc_particles_init_many(dsmc_ctx *ctx, int count, const int *sys_ids, const int64_t *n) {
+    if (!ctx) return DSMC_ERR_ARG;
+    std::vector<InitItem> items;
+    int rc = init_items(ctx, count, sys_ids, n, nullptr, nullptr, items);
+    if (rc) return rc;
+    return items.empty() ? DSMC_OK : init_systems(ctx, items, 0);
+}
+
+// Warm start: n particles drawn from a per-voxel weight and drift field
+// instead of System::setup_molecules' uniform Maxwellian at rest
+// (dsmc/system.cpp:398-430).  The weights of non-empty voxels are ignored.
+int dsmc_particles_init_field(dsmc_ctx *ctx, int sys_id, int64_t n, const float *weight, const float *drift,
+                              int device) {
+    if (!ctx || sys_id < 0 || sys_id >= (int)ctx->systems.size() || !weight || !drift) return DSMC_ERR_ARG;
+    return dsmc_particles_init_field_many(ctx, 1, &sys_id, &n, &weight, &drift, device);
+}
+
+int dsmc_particles_init_field_many(dsmc_ctx *ctx, int count, const int *sys_ids, const int64_t *n,
+                                   const float *const *weights, const float *const *drifts, int device) {
+    if (!ctx || (count > 0 && (!weights || !drifts))) return DSMC_ERR_ARG;
+    std::vector<InitItem> items;
+    int rc = init_items(ctx, count, sys_ids, n, weights, drifts, items);
+    if (rc) return rc;
+    return items.empty() ? DSMC_OK : init_systems(ctx, items, device);
 }
 
 // Per-voxel sums {count, sum vx, sum vy, sum vz} of a system's particles added

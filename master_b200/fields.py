@@ -107,7 +107,18 @@ class Ensemble:
             s = w.settings(rng_seed=rng_seed + i, statistics_interval=10 ** 9)
             self.geoms.append(g)
             self.settings.append(s)
-            self.systems.append(System(s, g, context=self.ctx, init_particles=cold))
+            self.systems.append(System(s, g, context=self.ctx, init_particles=False))
+        if cold:  # every system's cold start in one call: one re-layout, not one per system
+            self.init_cold(self.systems)
+
+    def init_cold(self, systems, counts=None) -> None:
+        """System::setup_molecules for the given systems of this ensemble
+        (counts: particles per system, None: the reference's count)."""
+        if not systems:
+            return
+        ids = (C.c_int * len(systems))(*[S.id for S in systems])
+        n = None if counts is None else (C.c_int64 * len(systems))(*[int(k) for k in counts])
+        self.ctx.check(self.ctx.lib.dsmc_particles_init_many(self.ctx.handle, len(systems), ids, n))
 
     @property
     def particles(self) -> int:
@@ -162,10 +173,35 @@ def finish_field(sums: np.ndarray, solid: np.ndarray) -> np.ndarray:
     return out
 
 
+def _seed_arrays(field_out: np.ndarray, solid: np.ndarray, uniform_density: bool = False):
+    empty = solid.ravel() == 0
+    dens = np.ones(len(empty)) if uniform_density else np.maximum(field_out[:, 0], 0.0)
+    w = np.ascontiguousarray(np.where(empty, dens, 0.0), np.float32)
+    drift = np.ascontiguousarray(field_out[:, 1:4] * VELOCITY_SCALE, np.float32)
+    return w, drift
+
+
+def warm_start_many(ctx: Context, systems, field_outs, solids, counts, uniform_density: bool = False,
+                    group: int = 64) -> None:
+    """warm_start for many systems of one context, `group` systems per
+    dsmc_particles_init_field_many call (each call re-lays the context out
+    once).  uniform_density: seed uniformly over the empty voxels (the cold
+    start's density) with the fields' drift."""
+    for g0 in range(0, len(systems), group):
+        sl = slice(g0, g0 + group)
+        arrs = [_seed_arrays(f, so, uniform_density) for f, so in zip(field_outs[sl], solids[sl])]
+        k = len(arrs)
+        ids = (C.c_int * k)(*[S.id for S in systems[sl]])
+        n = (C.c_int64 * k)(*[int(c) for c in counts[sl]])
+        w = (C.c_void_p * k)(*[a[0].ctypes.data for a in arrs])
+        d = (C.c_void_p * k)(*[a[1].ctypes.data for a in arrs])
+        ctx.check(ctx.lib.dsmc_particles_init_field_many(ctx.handle, k, ids, n, w, d, 0))
+        del arrs
+
+
 def warm_start(system: System, field_out: np.ndarray, solid: np.ndarray, n: int = -1) -> None:
     """Seeds the system's particles from a predicted field (V, 4) as
     finish_field writes it: density weights and drift * VELOCITY_SCALE."""
-    w = np.ascontiguousarray(np.where(solid.ravel() == 0, np.maximum(field_out[:, 0], 0.0), 0.0), np.float32)
-    drift = np.ascontiguousarray(field_out[:, 1:4] * VELOCITY_SCALE, np.float32)
+    w, drift = _seed_arrays(field_out, solid)
     ctx = system.ctx
     ctx.check(ctx.lib.dsmc_particles_init_field(ctx.handle, system.id, n, w.ctypes.data, drift.ctypes.data, 0))

@@ -3,19 +3,19 @@ until the x mass flux is steady.
 
 For a set of unseen packed-sphere geometries the surrogate (a trained
 surrogate.UNet) predicts each one's steady density and drift from its solid
-mask and Knudsen number; `dsmc_particles_init_field` seeds the particles from
-the local drifting Maxwellian of that field.  The cold start is the
+mask and Knudsen number; `dsmc_particles_init_field_many` seeds the particles
+of every geometry from the local drifting Maxwellian of its field.  The cold start is the
 reference's own (System::setup_molecules, dsmc/system.cpp:398-430: uniform in
 the empty voxels, Maxwellian at rest).  Both ensembles hold the same
 geometries, particle counts and draw seeds as systems of one context each,
 and run the split-precision production pass.
 
 Steady value: each geometry's mean flux over the second half of its cold run
-(the plain method's own steady state).  The per-geometry windowed flux
-(steady.windowed_flux) is normalised by it and averaged over the geometries,
-which divides the sampling noise of one geometry's flux by the square root
-of their number; steps to steady is steady.steps_to_steady of that
-normalised curve against 1.
+(the plain method's own steady state).  The geometries' windowed fluxes
+(steady.windowed_flux) are summed and normalised by the sum of their steady
+values, which divides the sampling noise of one geometry's flux by about
+the square root of their number; steps to steady is
+steady.total_steps_to_steady of that normalised total against 1.
 
 Fallback: when the surrogate's held-out field error (train_surrogate's
 "field_error", the relative error of the predicted mean x flux over the
@@ -48,10 +48,13 @@ def predict_fields(net, specs, geoms, batch: int = 1):
 
 def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: int = 1000, tol: float = 0.02,
             field_error: float = 0.0, max_field_error: float = 0.10, device: int = 0, rng_seed: int = 500,
-            capacity: tuple | None = None, force: bool = False, measured: tuple | None = None, log=print) -> dict:
+            capacity: tuple | None = None, force: bool = False, measured: tuple | None = None,
+            uniform_density: bool = False, log=print) -> dict:
     """Runs the cold ensemble, then the warm one (one context at a time, so
     the two never share the device memory), `steps` steps each, and returns
-    the steps and wall time to steady of both."""
+    the steps and wall time to steady of both.  uniform_density: seed the
+    particles uniformly over the empty voxels, as the cold start does, with
+    the predicted drift (the density channel left out)."""
     import torch
     rep = {"geometries": len(specs), "steps": steps, "every": every, "window": window, "hold": hold, "tol": tol,
            "surrogate_field_error": field_error, "max_field_error": max_field_error,
@@ -62,7 +65,9 @@ def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: i
     rep["geometry_s"] = time.perf_counter() - t0
     out = {}
     # cold: the reference's start
+    t0 = time.perf_counter()
     cold = fields.Ensemble(specs, device=device, rng_seed=rng_seed, cold=True, geoms=geoms, capacity=capacity)
+    rep["cold_setup_s"] = time.perf_counter() - t0
     counts_n = [S.num_molecules for S in cold.systems]
     weights = np.array([s.atoms_per_molecule for s in cold.settings], np.float64)
     dt = cold.settings[0].dt
@@ -95,16 +100,17 @@ def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: i
         rep["seeded_from"] = "surrogate" if use_net else "cold (fallback)"
     torch.cuda.synchronize()
     rep["inference_s"] = time.perf_counter() - t0
-    fallback = []
+    fallback, seeded = [], []
     t0 = time.perf_counter()
-    for i, (S, g, p) in enumerate(zip(warm.systems, geoms, preds)):
-        solid = (g.voxels > 0).astype(np.uint8).ravel()
-        if p is None or not np.isfinite(p).all() or not (np.maximum(p[solid == 0, 0], 0).sum() > 0):
-            fallback.append(i)
-            S.ctx.check(S.ctx.lib.dsmc_particles_init(S.ctx.handle, S.id, counts_n[i]))
-        else:
-            fields.warm_start(S, p, solid, n=counts_n[i])
+    solids = [(g.voxels > 0).astype(np.uint8).ravel() for g in geoms]
+    for i, (p, solid) in enumerate(zip(preds, solids)):
+        ok = p is not None and np.isfinite(p).all() and (uniform_density or np.maximum(p[solid == 0, 0], 0).sum() > 0)
+        (seeded if ok else fallback).append(i)
+    fields.warm_start_many(warm.ctx, [warm.systems[i] for i in seeded], [preds[i] for i in seeded],
+                           [solids[i] for i in seeded], [counts_n[i] for i in seeded], uniform_density=uniform_density)
+    warm.init_cold([warm.systems[i] for i in fallback], [counts_n[i] for i in fallback])
     rep["seed_s"] = time.perf_counter() - t0
+    rep["density"] = "uniform" if uniform_density else "field"
     rep["fallback"] = fallback
     if preds[0] is not None:
         rep["predicted_mean_drift_x"] = [float(p[(g.voxels.ravel() == 0), 1].mean()) for p, g in zip(preds, geoms)]
@@ -159,6 +165,8 @@ def main(argv=None):
                     help="seed from the surrogate even when its field error is above the fallback threshold")
     ap.add_argument("--measured", type=int, nargs=2, default=None, metavar=("TRANSIENT", "SAMPLING"),
                     help="control: seed from fields the DSMC measures itself instead of the network's")
+    ap.add_argument("--density", choices=("field", "uniform"), default="field",
+                    help="seed density: the field's, or uniform over the empty voxels with the field's drift")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     import torch
@@ -167,7 +175,7 @@ def main(argv=None):
                                 per_cell=a.per_cell)
     rep = compare(net, specs, a.steps, every=a.every, field_error=float(held.get("field_error", 0.0)),
                   capacity=tuple(a.capacity) if a.capacity else None, force=a.force,
-                  measured=tuple(a.measured) if a.measured else None)
+                  measured=tuple(a.measured) if a.measured else None, uniform_density=a.density == "uniform")
     rep["surrogate_held_out"] = held
     text = json.dumps(rep, default=float)
     if a.out:

@@ -102,3 +102,72 @@ def test_field_seeding_rejects_a_field_without_weight():
         S.ctx.check(S.ctx.lib.dsmc_particles_init_field(S.ctx.handle, S.id, 100, weight.ctypes.data,
                                                        drift.ctypes.data, 0))
     assert e.value.code == capi.DSMC_ERR_STATE
+
+
+def _synthetic_field(g, phase):
+    """A weight and drift pattern over the voxels of g, as finish_field writes them."""
+    V = int(np.prod(g.shape))
+    i = np.arange(V) // (g.shape[1] * g.shape[2])
+    out = np.zeros((V, 4))
+    out[:, 0] = 1.0 + 0.5 * np.sin(2 * np.pi * i / g.shape[0] + phase)
+    out[:, 1] = 30.0 * np.cos(2 * np.pi * i / g.shape[0] + phase)
+    out[:, 2] = 5.0
+    return out
+
+
+def test_field_seeding_many_systems_at_once_equals_one_call_each():
+    """dsmc_particles_init_field_many on systems of one context (one
+    re-layout) gives each system the particles, and then the trajectory, of
+    dsmc_particles_init_field on that system alone."""
+    specs = fields.random_specs(4, 32, seed=44, per_cell=20)
+    ens = fields.Ensemble(specs, rng_seed=60, cold=False)
+    solids = [(g.voxels > 0).astype(np.uint8).ravel() for g in ens.geoms]
+    outs = [_synthetic_field(g, k) for k, g in enumerate(ens.geoms)]
+    counts = [30_000 + 1000 * k for k in range(len(specs))]
+    fields.warm_start_many(ens.ctx, ens.systems, outs, solids, counts, group=3)  # two calls: 3 + 1
+    ens.ctx.step(5)
+    for k, S in enumerate(ens.systems):
+        alone = System(ens.settings[k], ens.geoms[k], init_particles=False)
+        fields.warm_start(alone, outs[k], solids[k], n=counts[k])
+        alone.step(5)
+        ra, va, ca = S.get_particles(with_cells=True)
+        rb, vb, cb = alone.get_particles(with_cells=True)
+        assert len(ra) == counts[k]
+        assert np.array_equal(ra, rb) and np.array_equal(va, vb) and np.array_equal(ca, cb), k
+        alone.ctx.close()
+    # uniform density: the weight 1 in every empty voxel, the fields' drift
+    ens2 = fields.Ensemble(specs[:2], rng_seed=60, cold=False)
+    fields.warm_start_many(ens2.ctx, ens2.systems, outs[:2], solids[:2], counts[:2], uniform_density=True)
+    for k, S in enumerate(ens2.systems):
+        alone = System(ens2.settings[k], ens2.geoms[k], init_particles=False)
+        flat = outs[k].copy()
+        flat[:, 0] = 1.0
+        fields.warm_start(alone, flat, solids[k], n=counts[k])
+        ra, va = S.get_particles()
+        rb, vb = alone.get_particles()
+        assert np.array_equal(ra, rb) and np.array_equal(va, vb), k
+        alone.ctx.close()
+    ens2.close()
+    assert ens.ctx.device_status()[0] & capi.EBIT_FATAL == 0
+    ens.close()
+
+
+def test_field_seeding_many_checks_every_field_first():
+    specs = fields.random_specs(2, 32, seed=45, per_cell=20)
+    ens = fields.Ensemble(specs, rng_seed=61)
+    before = [S.get_particles() for S in ens.systems]
+    solids = [(g.voxels > 0).astype(np.uint8).ravel() for g in ens.geoms]
+    outs = [_synthetic_field(g, 0.0) for g in ens.geoms]
+    outs[1][:, 0] = 0.0  # no weight anywhere in the second system
+    with pytest.raises(capi.DsmcError) as e:
+        fields.warm_start_many(ens.ctx, ens.systems, outs, solids, [1000, 1000])
+    assert e.value.code == capi.DSMC_ERR_STATE
+    for S, (r, v) in zip(ens.systems, before):  # nothing replaced
+        r2, v2 = S.get_particles()
+        assert np.array_equal(r, r2) and np.array_equal(v, v2)
+    # a system listed twice
+    ids = (C.c_int * 2)(ens.systems[0].id, ens.systems[0].id)
+    with pytest.raises(capi.DsmcError) as e:
+        ens.ctx.check(ens.ctx.lib.dsmc_particles_init_many(ens.ctx.handle, 2, ids, None))
+    assert e.value.code == capi.DSMC_ERR_ARG
+    ens.close()
