@@ -68,7 +68,6 @@ def signature(ctx) -> dict:
     import torch
     props = torch.cuda.get_device_properties(torch.cuda.current_device())
     cells = parts = 0
-    n = C.c_int()
     # every system's active cells and particles
     sid = 0
     info = capi.SystemInfo()
@@ -76,16 +75,16 @@ def signature(ctx) -> dict:
         cells += info.num_active_cells
         parts += info.num_particles
         sid += 1
-    _, lim = get(ctx)
-
-    def p2(x):
-        return 0 if x <= 0 else 2 ** round(math.log2(x))
     pipelined = C.c_int()
     grid, block, cap = C.c_int(), C.c_int(), C.c_int()
     ctx.check(ctx.lib.dsmc_pass_info(ctx.handle, C.byref(pipelined), C.byref(grid), C.byref(block), C.byref(cap)))
-    del n
-    return {"gpu": props.name, "sms": props.multi_processor_count, "cells": p2(cells), "particles": p2(parts),
+    return {"gpu": props.name, "sms": props.multi_processor_count, "cells": _pow2(cells), "particles": _pow2(parts),
             "min_ring": cap.value, "pipelined": pipelined.value}
+
+
+def _pow2(x: int) -> int:
+    """x rounded to the nearest power of two in log scale (0 for x <= 0)."""
+    return 0 if x <= 0 else 2 ** round(math.log2(x))
 
 
 def _key(sig: dict) -> str:

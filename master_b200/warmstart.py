@@ -46,6 +46,16 @@ def predict_fields(net, specs, geoms, batch: int = 1):
     return out
 
 
+def seedable(pred, solid, uniform_density: bool = False) -> bool:
+    """Whether a predicted field (V, 4) can seed its geometry: present, finite
+    everywhere, and (unless the density is taken uniform) with positive
+    density in some empty voxel of `solid` (V,).  Otherwise the geometry
+    starts cold."""
+    if pred is None or not np.isfinite(pred).all():
+        return False
+    return uniform_density or float(np.maximum(pred[solid == 0, 0], 0).sum()) > 0
+
+
 def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: int = 1000, tol: float = 0.02,
             field_error: float = 0.0, max_field_error: float = 0.10, device: int = 0, rng_seed: int = 500,
             capacity: tuple | None = None, force: bool = False, measured: tuple | None = None,
@@ -104,8 +114,7 @@ def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: i
     t0 = time.perf_counter()
     solids = [(g.voxels > 0).astype(np.uint8).ravel() for g in geoms]
     for i, (p, solid) in enumerate(zip(preds, solids)):
-        ok = p is not None and np.isfinite(p).all() and (uniform_density or np.maximum(p[solid == 0, 0], 0).sum() > 0)
-        (seeded if ok else fallback).append(i)
+        (seeded if seedable(p, solid, uniform_density) else fallback).append(i)
     fields.warm_start_many(warm.ctx, [warm.systems[i] for i in seeded], [preds[i] for i in seeded],
                            [solids[i] for i in seeded], [counts_n[i] for i in seeded], uniform_density=uniform_density)
     warm.init_cold([warm.systems[i] for i in fallback], [counts_n[i] for i in fallback])
