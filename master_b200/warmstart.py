@@ -29,10 +29,10 @@ import time
 
 import numpy as np
 
-from . import capi, fields, steady
+from . import fields, steady
 
 
-def predict_fields(net, specs, geoms, batch: int = 1):
+def predict_fields(net, specs, geoms):
     """The surrogate's output (V, 4) for each geometry (edge a power of two)."""
     import torch
     dev = net.dev
@@ -178,7 +178,6 @@ def main(argv=None):
                     help="seed density: the field's, or uniform over the empty voxels with the field's drift")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
-    import torch
     net, held = load_net(a.weights)
     specs = fields.random_specs(a.geometries, a.edge, seed=5, porosity=(0.45, 0.75), knudsen=tuple(a.knudsen),
                                 per_cell=a.per_cell)
@@ -186,7 +185,6 @@ def main(argv=None):
                   capacity=tuple(a.capacity) if a.capacity else None, force=a.force,
                   measured=tuple(a.measured) if a.measured else None, uniform_density=a.density == "uniform")
     rep["surrogate_held_out"] = held
-    text = json.dumps(rep, default=float)
     if a.out:
         from pathlib import Path
         Path(a.out).mkdir(parents=True, exist_ok=True)
@@ -194,7 +192,6 @@ def main(argv=None):
     print(json.dumps({k: v for k, v in rep.items() if k in ("ratio_steps", "fallback", "particles", "forced")} |
                      {n: {k: rep[n][k] for k in ("steps_to_steady", "wall_s_to_steady", "ms_per_step",
                                                   "window_noise")} for n in ("cold", "warm")}))
-    del torch, text
 
 
 def load_net(path, device: int = 0):

@@ -13,7 +13,6 @@ a dsmc.ini for the solver.  Nothing here imports or loads the B200 library.
 """
 from __future__ import annotations
 
-import math
 import os
 import re
 import shutil

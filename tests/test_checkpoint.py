@@ -4,7 +4,6 @@ reference solver built from its sources, and the exact checkpoint of this
 library (continuation gives the same trajectories)."""
 from __future__ import annotations
 
-import shutil
 
 import numpy as np
 import pytest

@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 
 from master_b200 import capi
-from master_b200.system import Context, Geometry, Settings, System
+from master_b200.system import Geometry, Settings, System
 
 pytestmark = pytest.mark.gpu
 

@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 
 from master_b200 import workloads
-from master_b200.system import Geometry, System, time_from_si
+from master_b200.system import Geometry, System
 
 pytestmark = pytest.mark.gpu
 

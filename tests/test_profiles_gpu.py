@@ -18,7 +18,7 @@ import numpy as np
 import pytest
 
 from master_b200 import capi, workloads
-from master_b200.system import Context, Geometry, System, finish_profiles
+from master_b200.system import System, finish_profiles
 from test_parity_gpu import CASES, load_case
 
 pytestmark = pytest.mark.gpu
