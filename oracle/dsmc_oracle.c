@@ -419,3 +419,81 @@ void oracle_collide(const oracle_system *s, int num_cells, const int *global_ind
         vr_max[a] = crm;
     }
 }
+
+/* ---- sampler ------------------------------------------------------------ */
+/* Reduced units of the reference (dsmc/unitconverter.cpp:3-21). */
+static const double U_M0 = 1.66053886e-27, U_L0 = 1e-6, U_E0 = 1.65088e-21, U_E0EV = 1.0318e-2,
+                    U_KB = 1.3806503e-23;
+
+void oracle_sample_profiles(const oracle_system *s, long n, const double *r, const double *v, double mass,
+                            double temperature, int bins, double *sums) {
+    /* one sample's per-bin values, summed in particle order, then added to
+     * the running sums (StatisticalValue::add_value, dsmc/statisticalvalue.h:38-46) */
+    double *cnt = calloc((size_t)bins, sizeof(double));
+    double *vz = calloc((size_t)bins, sizeof(double));
+    double *ez = calloc((size_t)bins, sizeof(double));
+    double *hx = calloc((size_t)bins, sizeof(double));
+    const double one_over_ly = 1.0 / s->L[1];
+    /* MeasureVelocityDistribution's histogram over [-4, 4] sqrt(T/m)
+     * (dsmc/statisticalproperty.cpp:432-438) */
+    const double std_dev = sqrt(temperature / mass);
+    const double v_min = -4 * std_dev, v_max = 4 * std_dev;
+    const double bin_size = (v_max - v_min) / bins;
+    for (long i = 0; i < n; ++i) {
+        /* MeasureCount, MeasureVelocityDistributionPoiseuille and
+         * MeasureTemperatureDistribution bin by y (:229-244, :261-278, :322-338) */
+        const int b = (int)(r[3 * i + 1] * one_over_ly * bins);
+        cnt[b] += 1.0;
+        vz[b] += v[3 * i + 2];
+        ez[b] += 0.5 * mass * v[3 * i + 2] * v[3 * i + 2];
+        /* the histogram keeps the bin of v_x only, truncated toward zero (:440-452) */
+        const int bx = (int)((v[3 * i] - v_min) / bin_size);
+        if (bx < 0 || bx > bins - 1) continue;
+        hx[bx] += 1.0;
+    }
+    for (int b = 0; b < bins; ++b) {
+        sums[3 * b] += cnt[b];
+        sums[3 * b + 1] += vz[b];
+        sums[3 * b + 2] += ez[b];
+        sums[3 * bins + b] += hx[b];
+    }
+    free(cnt);
+    free(vz);
+    free(ez);
+    free(hx);
+}
+
+void oracle_measures(const oracle_system *s, const oracle_gas *g, long n, const double *v, long long crossings,
+                     double elapsed, double out[6]) {
+    const double t0 = U_L0 * sqrt(U_M0 / U_E0);
+    const double T0 = U_E0 / U_KB;
+    const double P0 = U_M0 / (t0 * t0 * U_L0);
+    const double perm0 = U_L0 * U_L0;
+    /* MeasureEnergy (dsmc/statisticalproperty.cpp:21-41) */
+    double ke = 0;
+    for (long i = 0; i < n; ++i)
+        ke += (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+    ke *= 0.5 * g->mass * g->atoms_per_molecule;
+    /* System::get_number_of_atoms_global (dsmc/system.cpp:509-511): a long */
+    const long atoms = (long)((double)n * g->atoms_per_molecule);
+    /* MeasureTemperature (:57-70) */
+    const double T = 2.0 / 3.0 * ke / atoms;
+    /* MeasureNumberFlowRate (:87-101): cumulative net crossings over the elapsed time */
+    const double flux = g->atoms_per_molecule * (double)crossings / elapsed;
+    /* MeasureVolumetricFlowRate (:117-131) */
+    const double q = flux * (1.0 / g->density);
+    /* MeasurePressure (:154-165) */
+    const double P = atoms / g->volume_global * T;
+    /* MeasurePermeability (:185-214): hard-sphere viscosity at the measured T */
+    double area = 1;
+    for (int a = 0; a < 3; ++a)
+        if (a != s->flow_dir) area *= s->L[a];
+    const double visc = 5.0 / (16 * g->diam * g->diam) * sqrt(g->mass * T / M_PI);
+    const double k = q * visc / (area * g->mass * g->density * s->gravity);
+    out[0] = U_E0EV * ke;      /* UnitConverter::energy_to_eV */
+    out[1] = T0 * T;           /* temperature_to_SI */
+    out[2] = flux;
+    out[3] = q;
+    out[4] = P0 * P;           /* pressure_to_SI */
+    out[5] = k * perm0 * 1e4;  /* permeability_to_darcy */
+}

@@ -1,8 +1,8 @@
 /*
  * TEST INFRASTRUCTURE ONLY: a plain-C restatement of the reference DSMC
- * timestep (andeplane/master code/base_code/program/dsmc/) in fp64, used by
- * the tests as the checker for the GPU kernels.  Nothing in the shipped
- * library includes or links it.  It is pinned against the reference's own
+ * timestep and its sampler (andeplane/master code/base_code/program/dsmc/)
+ * in fp64, used by the tests as the checker for the GPU kernels.  Nothing
+ * in the shipped library includes or links it.  It is pinned against the reference's own
  * routines through the golden fixtures in tests/golden/.
  *
  * Draws come from the same counter-based streams as the kernels (philox.h):
@@ -54,5 +54,29 @@ int oracle_sort(const oracle_system *s, long n, const double *r, const int *cell
 void oracle_collide(const oracle_system *s, int num_cells, const int *global_index, const double *coeff,
                     double *vr_max, double *rest, const int *count, const int *start, const int *members, double *v,
                     uint32_t step, oracle_counters *c);
+
+/* The gas quantities the sampler's measurements read (System::initialize,
+ * dsmc/system.cpp:252-314), reduced units. */
+typedef struct oracle_gas {
+    double mass, diam;
+    double density;             /* number density */
+    double atoms_per_molecule;
+    double volume_global;       /* L_x L_y L_z times the world file's float porosity */
+} oracle_gas;
+
+/* One sample of the sampler's profiles added to `sums` (4*bins doubles: per
+ * y bin {count, sum v_z, sum 1/2 m v_z^2}, then the v_x histogram over
+ * [-4, 4] sqrt(temperature/mass)): MeasureCount,
+ * MeasureVelocityDistributionPoiseuille, MeasureTemperatureDistribution and
+ * MeasureVelocityDistribution (dsmc/statisticalproperty.cpp:229-458). */
+void oracle_sample_profiles(const oracle_system *s, long n, const double *r, const double *v, double mass,
+                            double temperature, int bins, double *sums);
+/* The scalar measurements of one sample, in the units their files print:
+ * energy (eV), temperature (K), number and volumetric flow rate (reduced),
+ * pressure (Pa), permeability (darcy); `crossings` is count_periodic along
+ * the flow and `elapsed` the time since the run's start
+ * (dsmc/statisticalproperty.cpp:21-214). */
+void oracle_measures(const oracle_system *s, const oracle_gas *g, long n, const double *v, long long crossings,
+                     double elapsed, double out[6]);
 
 #endif

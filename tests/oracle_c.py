@@ -19,6 +19,11 @@ class System(C.Structure):
                 ("alpha_t", C.c_double), ("cl_vmax", C.c_double)]
 
 
+class Gas(C.Structure):
+    _fields_ = [("mass", C.c_double), ("diam", C.c_double), ("density", C.c_double),
+                ("atoms_per_molecule", C.c_double), ("volume_global", C.c_double)]
+
+
 class Counters(C.Structure):
     _fields_ = [("count_periodic", C.c_longlong * 3), ("wall_hits", C.c_ulonglong), ("reseeds", C.c_ulonglong),
                 ("collisions", C.c_ulonglong), ("candidates", C.c_ulonglong)]
@@ -29,6 +34,7 @@ def _p(a, t=C.c_double):
 
 
 T0 = 1.65088e-21 / 1.3806503e-23   # temperature unit (dsmc/unitconverter.cpp)
+NUMBER_DENSITY0 = 1.0 / (1e-6 * 1e-6 * 1e-6)   # 1 / L0^3, m^-3 (dsmc/unitconverter.cpp:20)
 
 
 class Oracle:
@@ -48,6 +54,11 @@ class Oracle:
         L.oracle_sort.restype = C.c_int
         L.oracle_collide.argtypes = [C.POINTER(System), C.c_int] + [C.c_void_p] * 8 + [C.c_uint32,
                                                                                        C.POINTER(Counters)]
+        L.oracle_sample_profiles.argtypes = [C.POINTER(System), C.c_long, C.POINTER(C.c_double),
+                                             C.POINTER(C.c_double), C.c_double, C.c_double, C.c_int,
+                                             C.POINTER(C.c_double)]
+        L.oracle_measures.argtypes = [C.POINTER(System), C.POINTER(Gas), C.c_long, C.POINTER(C.c_double),
+                                      C.c_longlong, C.c_double, C.POINTER(C.c_double)]
         self.g = geometry
         st = settings
         self.vox = np.ascontiguousarray(geometry.voxels)
@@ -89,6 +100,14 @@ class Oracle:
         self.c = Counters()
         self.r = np.zeros((0, 3))
         self.v = np.zeros((0, 3))
+        # the sampler (StatisticsSampler, dsmc/statisticssampler.cpp:13-42)
+        self.mass = st["mass"]
+        self.temperature = st["temperature"] / T0
+        self.bins = st.get("sampling_bins", 1)
+        self.prof_sums = np.zeros(4 * self.bins)
+        self.t = 0.0
+        self.gas = Gas(mass=st["mass"], diam=st["diam"], density=st.get("density", 0.0) / NUMBER_DENSITY0,
+                       atoms_per_molecule=st["atoms_per_molecule"], volume_global=0.0)
 
     def init(self, n: int):
         self.r = np.zeros((n, 3))
@@ -125,6 +144,29 @@ class Oracle:
         self.move(step)
         self.sort()
         self.collide(step)
+        self.t += self.s.dt  # System::step (dsmc/system.cpp:24-26)
+
+    def sample(self):
+        """StatisticsSampler::sample's profiles after a step (every step
+        sampled): adds into prof_sums."""
+        self.lib.oracle_sample_profiles(C.byref(self.s), len(self.r), _p(self.r), _p(self.v), self.mass,
+                                        self.temperature, self.bins, _p(self.prof_sums))
+
+    def profile_sums(self) -> np.ndarray:
+        """(4, bins): count, sum v_z and sum 1/2 m v_z^2 per y bin, then the
+        v_x histogram (the layout of the reference harness's sums)."""
+        p = self.prof_sums
+        return np.stack([p[0:3 * self.bins:3], p[1:3 * self.bins:3], p[2:3 * self.bins:3], p[3 * self.bins:]])
+
+    def measures(self, volume_global: float) -> np.ndarray:
+        """energy (eV), temperature (K), number and volumetric flow rate,
+        pressure (Pa), permeability (darcy) of the current state."""
+        self.gas.volume_global = volume_global
+        out = np.zeros(6)
+        fd = self.s.flow_dir
+        self.lib.oracle_measures(C.byref(self.s), C.byref(self.gas), len(self.v), _p(self.v),
+                                 self.c.count_periodic[fd], self.t, _p(out))
+        return out
 
     @property
     def cell_global_of_particles(self):

@@ -58,6 +58,33 @@ def test_oracle_reproduces_reference_steps(case):
     assert c["count_periodic"] == ref["count_periodic"]
 
 
+MEASURES = ("energy_eV", "temperature_K", "number_flow_rate", "volumetric_flow_rate", "pressure_Pa",
+            "permeability_darcy")
+
+
+@pytest.mark.parametrize("case", ["small_dt1", "small_dt5", "small_specular", "small_cl"])
+def test_oracle_sampler_reproduces_reference_sampler(case, tmp_path):
+    """The oracle's sampler over the fixture's steps (one sample after each,
+    as the fixture's statistics_interval of 1 has it) gives the reference
+    StatisticsSampler's profile sums and its scalar measurements of the
+    last step, both bit for bit (the same operations in the same order)."""
+    z, meta, g = load(case)
+    st = meta["settings"]
+    o = oracle_c.Oracle(g, st, meta["params"]["rng_seed"])
+    o.init(meta["n"])
+    for step in range(1, meta["params"]["steps"] + 1):
+        o.step(step)
+        o.sample()
+    assert np.array_equal(o.r, z["rK"]) and np.array_equal(o.v, z["vK"])
+    assert np.array_equal(o.profile_sums(), z["prof_sumsK"])
+    # System::volume_global: the box times the world file's float porosity (dsmc/system.cpp:313-314)
+    g.write_world(tmp_path)
+    por = Geometry.read_world(tmp_path / "0000.bin").porosity_global
+    got = o.measures(st["Lx"] * st["Ly"] * st["Lz"] * por)
+    for k, x in zip(MEASURES, got):
+        assert x == meta["measures_final"][k], k
+
+
 KAT = [  # Salmon et al. (SC'11), Random123 kat_vectors: philox4x32, 10 rounds
     ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
     ((0xFFFFFFFF,) * 4, (0xFFFFFFFF, 0xFFFFFFFF), (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)),
