@@ -138,7 +138,9 @@ int dsmc_geometry_packed_spheres(const dsmc_sphere_params *p, uint8_t *voxels, f
  * dsmc/complexgeometry.cpp:196-201).  On the CPU. */
 int dsmc_geometry_finish(uint32_t nx, uint32_t ny, uint32_t nz, int number_of_neighbor_averages,
                          uint8_t *voxels, float *normals, float *tangents1, float *tangents2);
-/* The same stencil on the GPU (device_id), identical output. */
+/* The same stencil on the GPU (device_id), identical output: the normal,
+ * tangent and boundary passes of dsmc/complexgeometry.cpp:928-1063 as
+ * kernels, the order-dependent removals replayed on the host. */
 int dsmc_geometry_finish_gpu(int device_id, uint32_t nx, uint32_t ny, uint32_t nz,
                              int number_of_neighbor_averages, uint8_t *voxels, float *normals,
                              float *tangents1, float *tangents2);
@@ -160,11 +162,20 @@ int dsmc_geometry_finish_gpu_noalloc(int device_id, uint32_t nx, uint32_t ny, ui
 /* ---- context ---------------------------------------------------------- */
 typedef struct dsmc_ctx dsmc_ctx;
 
+/* A context: one GPU, its stream and device buffers, and any number of
+ * systems advanced together.  It takes the place of the per-rank process
+ * state of the reference's main (dsmc/main.cpp:19-30: one System per MPI
+ * rank); precision is DSMC_PREC_SPLIT32 or DSMC_PREC_FP64.  destroy frees
+ * everything (the reference never frees its grid, dsmc/dsmc_io.cpp:205-208). */
 int dsmc_ctx_create(int device_id, int precision, dsmc_ctx **out);
 void dsmc_ctx_destroy(dsmc_ctx *ctx);
 /* Message of the last failed call on ctx (or of the last failed context-free
- * call on this thread when ctx is NULL). */
+ * call on this thread when ctx is NULL): the text the reference prints before
+ * its exit(1) (e.g. dsmc/system.h:137-166) or throws to System::step
+ * (dsmc/system.cpp:41-44), here returned with the DSMC_ERR_* code. */
 const char *dsmc_last_error(const dsmc_ctx *ctx);
+/* Waits until the context's queued work has finished.  No counterpart in the
+ * reference, whose calls are synchronous. */
 int dsmc_sync(dsmc_ctx *ctx);
 
 /* Adds one system (one geometry and its gas; the reference's System,
@@ -174,7 +185,8 @@ int dsmc_sync(dsmc_ctx *ctx);
 int dsmc_system_add(dsmc_ctx *ctx, const dsmc_settings *s, uint32_t nx, uint32_t ny, uint32_t nz,
                     const uint8_t *voxels, const float *normals, const float *tangents1,
                     const float *tangents2, float porosity_global, int *sys_id);
-/* Same, reading s->world/0000.bin. */
+/* Same, reading s->world/0000.bin as the reference's Grid does
+ * (DSMC_IO::read_grid_matrix, dsmc/dsmc_io.cpp:183-220), halo stripped. */
 int dsmc_system_add_world(dsmc_ctx *ctx, const dsmc_settings *s, int *sys_id);
 
 /* The active cells of a voxel grid as System::setup_cells builds them
@@ -199,6 +211,8 @@ typedef struct dsmc_system_info {
     int slots;                  /* particle slots reserved per buffer */
     double volume_global;       /* L_x L_y L_z * porosity_global (dsmc/system.cpp:314) */
 } dsmc_system_info;
+/* The sizes System::initialize derives for a system (dsmc/system.cpp:241-382)
+ * and the slots this library reserves for it. */
 int dsmc_system_info_get(dsmc_ctx *ctx, int sys_id, dsmc_system_info *info);
 
 /* One x-slab of a geometry, for a run over several GPUs (the reference's
@@ -254,7 +268,8 @@ int dsmc_particles_init_field(dsmc_ctx *ctx, int sys_id, int64_t n, const float 
 int dsmc_particles_init_many(dsmc_ctx *ctx, int count, const int *sys_ids, const int64_t *n);
 int dsmc_particles_init_field_many(dsmc_ctx *ctx, int count, const int *sys_ids, const int64_t *n,
                                    const float *const *weights, const float *const *drifts, int device);
-/* Adds one system's per-voxel particle sums {count, sum vx, sum vy, sum vz}
+/* No counterpart in the reference (the warm start's training data).
+ * Adds one system's per-voxel particle sums {count, sum vx, sum vy, sum vz}
  * (4 floats per voxel, geometry voxel order, 16-byte aligned) to field: the
  * steady fields that the warm-start surrogate learns are these sums over
  * many steps.  device != 0: field is device memory of the context's GPU and
@@ -265,8 +280,10 @@ int dsmc_field_accumulate(dsmc_ctx *ctx, int sys_id, float *field, int device);
 /* Replaces a system's particles by n particles in the reference's state-file
  * layout: r[3n], v[3n] fp64 (dsmc/dsmc_io.cpp:82-159).  Particle i gets id i. */
 int dsmc_particles_set(dsmc_ctx *ctx, int sys_id, int64_t n, const double *r, const double *v);
+/* The system's particle count (System::num_molecules_local, dsmc/system.h:85). */
 int dsmc_particles_count(dsmc_ctx *ctx, int sys_id, int64_t *n);
-/* Copies the particles out ordered by id (r[3n], v[3n]; cell: the reference's
+/* Copies the particles out ordered by id (r[3n], v[3n]: the reference's
+ * System::r and System::v, dsmc/system.h:74-75; cell: the reference's
  * global cell index of each particle, may be NULL). */
 int dsmc_particles_get(dsmc_ctx *ctx, int sys_id, int64_t cap, double *r, double *v, int32_t *cell,
                        int64_t *n);
@@ -303,6 +320,11 @@ typedef struct dsmc_tallies {
     double time;                /* t, reduced */
     uint64_t stranded;          /* moves that ended in a cell with no free volume (re-seeded next step) */
 } dsmc_tallies;
+/* get: the counters and current scalars the reference's sampler reads from
+ * System, MoleculeMover and ColliderBase (dsmc/statisticssampler.cpp:45-66,
+ * dsmc/statisticalproperty.cpp:21-101).  reset: zeroes the counters, the cell
+ * moments and the profiles and restarts the flux window at the current time
+ * (as the reference's t0 = t at a run's start, dsmc/main.cpp:51-52). */
 int dsmc_tallies_get(dsmc_ctx *ctx, int sys_id, dsmc_tallies *t);
 int dsmc_tallies_reset(dsmc_ctx *ctx, int sys_id);
 
@@ -351,6 +373,8 @@ int dsmc_profiles_get(dsmc_ctx *ctx, int sys_id, int cap, double *count, double 
  * (n, sum vx, vy, vz, sum vx^2, vy^2, vz^2, sum |v|^2).  Any pointer may be NULL. */
 int dsmc_cells_get(dsmc_ctx *ctx, int sys_id, int cap, int32_t *global_index, int32_t *count,
                    double *vr_max, double *rest, double *moments, double *volume, int *num_cells);
+/* Sets each active cell's Cell::vr_max and Cell::collision_rest
+ * (dsmc/cell.h:18-23), in active-cell order. */
 int dsmc_cells_set_state(dsmc_ctx *ctx, int sys_id, const double *vr_max, const double *rest);
 
 /* Continuation (dsmc/main.cpp:37-55): the step counter, collisions and wall
@@ -369,13 +393,16 @@ int dsmc_continue_from(dsmc_ctx *ctx, int sys_id, double t, uint64_t steps, uint
 int dsmc_checkpoint_save(dsmc_ctx *ctx, const char *path);
 int dsmc_checkpoint_load(dsmc_ctx *ctx, const char *path);
 
-/* Slot capacity policy of the cell-sorted particle buffers: a cell gets
+/* No counterpart in the reference, whose cell member lists are vectors that
+ * grow (Cell::add_molecule, dsmc/cell.cpp:113-140).
+ * Slot capacity policy of the cell-sorted particle buffers: a cell gets
  * ceil(factor * max(expected, present) + pad) slots (default 2.0, 24).  An
  * overflow never loses particles: they spill to an overflow list, the
  * pipeline stops after that step and the host re-lays the buffers out. */
 int dsmc_ctx_set_capacity(dsmc_ctx *ctx, double factor, int pad);
 
-/* Launch shape of the timestep pass: pipelined = 1 when the split-precision
+/* No counterpart in the reference.
+ * Launch shape of the timestep pass: pipelined = 1 when the split-precision
  * production pass (collide_cells, move_cells, place_movers, place_walls) runs
  * dsmc_step (0: the generic cell pass, e.g. fp64 contexts), the grid and
  * block of move_cells, and its per-warp staging ring in particles. */
@@ -414,7 +441,10 @@ int dsmc_ctx_set_timing(dsmc_ctx *ctx, int on);
 int dsmc_pass_times_get(dsmc_ctx *ctx, double ms[4], int64_t *passes);
 
 /* Reads the status of the last pass: bit flags of device-side errors
- * (DSMC_EBIT_*) and the number of particles spilled to the overflow list. */
+ * (DSMC_EBIT_*) and the number of particles spilled to the overflow list.
+ * The reference stops the process where these bits are raised (exit(1) for a
+ * particle in a cell with no free volume, dsmc/system.h:137-140); here the
+ * pass sets a bit and dsmc_step returns DSMC_ERR_STATE for the fatal ones. */
 #define DSMC_EBIT_CELL 1u        /* a particle ended in a cell with no free volume */
 #define DSMC_EBIT_FACET 2u       /* facet search found no face of the hit voxel (re-seeded, counted) */
 #define DSMC_EBIT_RESEED 4u      /* re-seeding found no empty voxel within its limit */
@@ -431,12 +461,16 @@ int dsmc_pass_times_get(dsmc_ctx *ctx, double ms[4], int64_t *passes);
 int dsmc_device_status(dsmc_ctx *ctx, uint32_t *error_bits, uint32_t *spill);
 
 /* The CUDA stream (cudaStream_t) the context enqueues its work on, for
- * callers that order or time their own work against it. */
+ * callers that order or time their own work against it.  No counterpart in
+ * the reference. */
 void *dsmc_stream(dsmc_ctx *ctx);
 
 /* Raw running counters of one system, without synchronising the device
  * beyond the copy: collisions, wall collisions, reseeds, particle steps,
- * count_periodic[3], samples (8 values, as int64). */
+ * count_periodic[3], samples (8 values, as int64): System::collisions,
+ * ColliderBase::num_collisions and MoleculeMover::count_periodic
+ * (dsmc/system.h, dsmc/colliderbase.h, dsmc/moleculemover.h:15) as the
+ * sampler reads them each statistics_interval. */
 int dsmc_counters_get(dsmc_ctx *ctx, int sys_id, int64_t out[8]);
 
 #ifdef __cplusplus
