@@ -138,6 +138,7 @@ struct dsmc_ctx {
     DevBuf<unsigned long long> cursor;
     DevBuf<double> io_r, io_v;
     DevBuf<int> io_cell;
+    DevBuf<double> cell_energy;  // dsmc_tallies_get: per-cell kinetic-energy sums
     // launch shape of the cell pass
     int block = 256;
     int grid = 0;
@@ -1701,8 +1702,10 @@ int dsmc_tallies_get(dsmc_ctx *ctx, int sys_id, dsmc_tallies *t) {
     // from the current velocities, summed per cell and then in cell order.
     const int C = h.active_end - h.active_begin;
     if (C > 0 && ctx->A0.p) {
-        DevBuf<double> ce;
-        CK(ce.alloc(C));
+        // kept by the context: a sampler reading this every few steps
+        // allocates once, not on every read
+        DevBuf<double> &ce = ctx->cell_energy;
+        CK(ce.ensure(C));
         e = is_fp64(ctx) ? fp64::launch_cell_energy(cell_arrays(ctx), particle_arrays(ctx), ctx->cur, ctx->cphase,
                                                     h.active_begin,
                                                     h.active_end, ce.p, ctx->stream)
