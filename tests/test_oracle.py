@@ -130,3 +130,38 @@ def test_oracle_draws_follow_philox():
     o = oracle_c.Oracle(g, st, seed)
     o.init(6)
     assert o.v[5, 0] == pytest.approx(gauss * o.s.sqrt_t_over_m, rel=1e-15)
+
+
+LAYOUT_CASES = [  # (voxels per axis, cells per axis, solid fraction, seed)
+    ((8, 8, 8), (4, 4, 4), 0.0, 1),          # all open
+    ((8, 8, 8), (8, 8, 8), 0.5, 2),          # one voxel per cell: half the cells inactive
+    ((12, 8, 16), (3, 4, 8), 0.6, 3),        # uneven box and cells
+    ((16, 16, 16), (4, 4, 4), 0.97, 4),      # nearly solid: cells with one or two open voxels
+    ((10, 10, 10), (5, 2, 10), 0.3, 5),
+    ((4, 4, 4), (2, 2, 2), 1.0, 6),          # all solid: no active cell
+]
+
+
+@pytest.mark.parametrize("shape,cells,solid,seed", LAYOUT_CASES)
+def test_cell_layout_of_the_library_equals_the_oracle(shape, cells, solid, seed):
+    """System::setup_cells + Cell::update_volume (dsmc/system.cpp:432-490,
+    dsmc/cell.cpp:27-40) restated twice, by the library's host code
+    (dsmc_cells_layout) and by the C oracle: identical on random masks,
+    uneven boxes and cells down to one voxel."""
+    from master_b200.system import Settings, cells_layout
+    rng = np.random.default_rng(seed)
+    g = Geometry.empty(*shape)
+    g.voxels[...] = (rng.random(shape) < solid).astype(np.uint8)
+    st = dict(cells_x=cells[0], cells_y=cells[1], cells_z=cells[2], Lx=0.1 * shape[0], Ly=0.1 * shape[1],
+              Lz=0.1 * shape[2], dt=0.00997, gravity=0.0, flow_direction=-1, wall_temperature=300.0,
+              temperature=300.0, mass=39.948, atoms_per_molecule=1000, diam=3.66e-4)
+    o = oracle_c.Oracle(g, st, 1)
+    s = Settings()
+    for k in ("Lx", "Ly", "Lz", "cells_x", "cells_y", "cells_z", "dt", "diam", "atoms_per_molecule"):
+        setattr(s, k, st[k])
+    lib = cells_layout(s, g)
+    assert np.array_equal(lib["global_index"], o.global_index)
+    assert np.array_equal(lib["volume"], o.volume)
+    assert np.array_equal(lib["coeff"], o.coeff)
+    open_voxels = (g.voxels == 0).sum()
+    assert lib["pixels"].sum() == open_voxels and (lib["pixels"] > 0).all()
