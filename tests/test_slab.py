@@ -1,6 +1,6 @@
 """Host side of the x-slab decomposition (master_b200/slab.py): the
-partition, record routing, and the all-to-all exchange over two gloo ranks
-on the CPU with stand-in slabs (the records are the 32-byte layout of
+partition, record routing, and the all-to-all exchange over two and three gloo
+ranks on the CPU with stand-in slabs (the records are the 32-byte layout of
 dsmc_exchange_take; no GPU)."""
 from __future__ import annotations
 
@@ -96,8 +96,11 @@ def _free_port() -> int:
         return sk.getsockname()[1]
 
 
-def test_two_gloo_ranks_exchange_records_to_their_owners():
-    world, nx, cells_x = 2, 24, 12
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_exchange_records_to_their_owners(world):
+    """Two ranks (each the other's only neighbour) and three (a middle
+    slab with a neighbour on either side)."""
+    nx, cells_x = 24, 12
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
     port = _free_port()
