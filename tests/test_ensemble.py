@@ -1,6 +1,7 @@
 """Runs over several ranks (master_b200/ensemble.py): systems sharded across
 ranks, fp64 tallies gathered with one all-reduce, the slowest rank's time.
-Two gloo ranks on the CPU, as a launch of one process per GPU would run."""
+Two and three gloo ranks on the CPU, as a launch of one process per GPU
+would run them."""
 from __future__ import annotations
 
 import os
@@ -57,11 +58,12 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def test_two_gloo_ranks_gather_every_systems_tallies():
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_gather_every_systems_tallies(world):
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank, args=(r, 2, port, out)) for r in range(2)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, out)) for r in range(world)]
     for p in procs:
         p.start()
     res = [out.get(timeout=120) for _ in procs]
@@ -71,8 +73,8 @@ def test_two_gloo_ranks_gather_every_systems_tallies():
     expect = np.stack([ensemble.tally_row(fake_tallies(s)) for s in range(5)])
     for rank, table, slowest, total, prof in res:
         assert np.array_equal(table, expect)
-        assert slowest == 11.0 and total == 5.0
-        assert np.array_equal(prof, fake_profile(0) + fake_profile(1))
+        assert slowest == 10.0 + world - 1 and total == 5.0
+        assert np.array_equal(prof, sum(fake_profile(r) for r in range(world)))
     tot = ensemble.totals(expect)
     assert tot["collisions"] == sum(1000 + s for s in range(5))
     assert tot["count_periodic_y"] == -sum(range(5))
