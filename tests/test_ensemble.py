@@ -78,3 +78,42 @@ def test_gloo_ranks_gather_every_systems_tallies(world):
     tot = ensemble.totals(expect)
     assert tot["collisions"] == sum(1000 + s for s in range(5))
     assert tot["count_periodic_y"] == -sum(range(5))
+
+
+def _rank_that_may_leave(rank: int, port: int, out):
+    """Rank 1 leaves after joining, before the tally gather; rank 0 gathers."""
+    import datetime
+    import time as _time
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=2, timeout=datetime.timedelta(seconds=10))
+    if rank == 1:
+        os._exit(0)   # leaves between steps: nothing of it in flight
+    t0 = _time.monotonic()
+    try:
+        ensemble.gather_tallies(dist, 2, {0: fake_tallies(0)})
+        out.put(("returned", _time.monotonic() - t0))
+    except Exception as e:  # noqa: BLE001
+        out.put((type(e).__name__, _time.monotonic() - t0))
+    finally:
+        try:
+            dist.destroy_process_group()
+        except Exception:  # noqa: BLE001
+            pass
+
+
+def test_a_rank_that_left_makes_the_gather_fail_not_hang():
+    """Failure detection on the host: a rank that exits between steps turns
+    the survivors' next collective into an error within the process group's
+    timeout, instead of a wait without end."""
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_that_may_leave, args=(r, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    what, secs = out.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+    assert what != "returned", "the gather completed without the rank that left"
+    assert secs < 60
