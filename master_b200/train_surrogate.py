@@ -96,6 +96,15 @@ def predict(net, solid, feat, edge, batch, device):
 
 def evaluate(net, solid, feat, target, halves, edge, batch, device):
     pred = predict(net, solid, feat, edge, batch, device)
+    summary, res = summarize(pred, solid, target, halves)
+    return summary, pred, res
+
+
+def summarize(pred, solid, target, halves):
+    """Held-out errors of predictions pred (n, V, 4) against targets (n, V, 4)
+    whose two half-window estimates are halves (n, 2, V, 4), over the empty
+    voxels of solid (n, V): per geometry and summarised; "field_error" is
+    the warm start's fallback criterion."""
     empty = solid == 0
     res = {"density_rel_l2": [], "drift_x_rel_l2": [], "noise_density_rel_l2": [], "noise_drift_x_rel_l2": [],
            "flux_pred": [], "flux_target": [], "flux_half_diff": []}
@@ -126,7 +135,7 @@ def evaluate(net, solid, feat, target, halves, edge, batch, device):
     summary["field_error_raw"] = float(np.sqrt(err2 / norm2))
     summary["flux_target_noise"] = float(np.sqrt(noise2 / norm2))
     summary["field_error"] = float(np.sqrt(max(0.0, err2 - noise2) / norm2))
-    return summary, pred, res
+    return summary, res
 
 
 def train(net, solid, feat, target, edge, epochs, batch, lr, device, seed=0, lr_min=None, flux_weight=FLUX_WEIGHT,

@@ -1,8 +1,9 @@
 """Host side of the warm start, without a GPU: per-voxel sums finished into
 the surrogate's fields (density relative to the empty-voxel mean, drift in
 VELOCITY_SCALE units), the seeding arrays handed to
-dsmc_particles_init_field(_many), and the per-geometry fallback to the cold
-start (System::setup_molecules, dsmc/system.cpp:398-430)."""
+dsmc_particles_init_field(_many), the per-geometry fallback to the cold
+start (System::setup_molecules, dsmc/system.cpp:398-430), and the held-out
+error summary whose field error decides that fallback."""
 from __future__ import annotations
 
 import numpy as np
@@ -80,3 +81,39 @@ def test_uniform_density_needs_only_a_finite_drift():
     assert warmstart.seedable(p, solid, uniform_density=True)
     p[0, 1] = np.nan
     assert not warmstart.seedable(p, solid, uniform_density=True)
+
+
+def test_held_out_summary_and_the_fallback_criterion():
+    """train_surrogate.summarize: relative L2 errors over empty voxels, the
+    targets' sampling noise from their two halves, and the field error the
+    fallback reads: the flux error with that noise taken out in quadrature."""
+    from master_b200 import train_surrogate as ts
+    rng = np.random.default_rng(3)
+    n, V = 4, 64
+    solid = (rng.random((n, V)) < 0.3).astype(np.uint8)
+    truth = np.zeros((n, V, 4))
+    truth[..., 0] = 1.0 + 0.1 * rng.standard_normal((n, V))
+    truth[..., 1] = 2.0 + 0.5 * rng.standard_normal((n, V))
+    noise = 0.05 * rng.standard_normal((n, 2, V, 4))
+    halves = truth[:, None] + noise
+    target = halves.mean(axis=1)
+    # a prediction equal to the target: no error, field error 0
+    s, res = ts.summarize(target.copy(), solid, target, halves)
+    assert s["density_rel_l2"] == 0 and s["drift_x_rel_l2"] == 0 and s["field_error"] == 0
+    # noise estimate: half the difference of the halves
+    m = solid[0] == 0
+    d = halves[0, 0, m, 1] - halves[0, 1, m, 1]
+    assert res["noise_drift_x_rel_l2"][0] == pytest.approx(0.5 * np.linalg.norm(d) / np.linalg.norm(halves[0, 1, m, 1]))
+    # a prediction whose flux is 10 % high everywhere: the raw flux error is
+    # 10 %, and the field error is that with the noise taken out in quadrature
+    pred = target.copy()
+    pred[..., 1] *= 1.1
+    s, res = ts.summarize(pred, solid, target, halves)
+    assert s["field_error_raw"] == pytest.approx(0.1, rel=1e-9)
+    assert s["field_error"] == pytest.approx(np.sqrt(0.1 ** 2 - s["flux_target_noise"] ** 2), rel=1e-9)
+    assert s["field_error"] < s["field_error_raw"]
+    assert s["flux_rel_err_median"] == pytest.approx(0.1, rel=1e-9)
+    # solid voxels do not count: a wild value there changes nothing
+    pred2 = pred.copy()
+    pred2[solid == 1] = 1e6
+    assert ts.summarize(pred2, solid, target, halves)[0] == s
