@@ -14,6 +14,7 @@ import pytest
 from master_b200.system import Geometry
 
 import oracle_c
+import ref_harness as rh
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 
@@ -165,3 +166,76 @@ def test_cell_layout_of_the_library_equals_the_oracle(shape, cells, solid, seed)
     assert np.array_equal(lib["coeff"], o.coeff)
     open_voxels = (g.voxels == 0).sum()
     assert lib["pixels"].sum() == open_voxels and (lib["pixels"] > 0).all()
+
+
+FRESH = {  # systems beyond the fixtures: other sizes, cells, timesteps, flow axes and walls
+    "thermal_16": dict(n=16, radius_voxels=2, porosity=0.5, geom_seed=21, cells=8, dt_si=1e-11, flow=0,
+                       rng_seed=0x51DE, surface="thermal"),
+    "specular_20_flow_y": dict(n=20, radius_voxels=2.5, porosity=0.7, geom_seed=22, cells=10, dt_si=3e-11, flow=1,
+                               rng_seed=0xF10F, surface="specular"),
+    # alpha_n 0.8: at alpha_n <= ~0.4 the reference's Cercignani-Lampis
+    # sampler needs ~1e6 trials for a particle that meets the wall at twice
+    # the wall's most probable speed, past the 1e5 at which the tape draws
+    # stop the process
+    "cl_16_coarse_cells": dict(n=16, radius_voxels=3, porosity=0.65, geom_seed=23, cells=4, dt_si=2e-11, flow=2,
+                               rng_seed=0xC0C0A, surface="cercignani_lampis", alpha_n=0.8, alpha_t=0.5),
+}
+
+
+@pytest.mark.skipif(not rh.available(), reason="oracle/_ref (the reference built from its sources) is not built")
+@pytest.mark.parametrize("name", sorted(FRESH))
+def test_oracle_matches_a_fresh_reference_run(name, tmp_path):
+    """The oracle against the reference's own routines run now (the tape
+    build, oracle/_ref/libdsmc_ref_tape.so), on systems the fixtures do not
+    hold: the initial state, six full steps sampled after each, every
+    position, velocity, cell, counter, profile sum and measurement bit for
+    bit."""
+    from master_b200.system import acceleration_from_si, time_from_si
+    c = FRESH[name]
+    g = Geometry.packed_spheres(c["n"], c["radius_voxels"], wanted_porosity=c["porosity"], seed=c["geom_seed"])
+    L = 0.1 * c["n"]
+    st = dict(max_molecules=200000, atoms_per_molecule=4000, temperature=300.0, wall_temperature=320.0,
+              statistics_interval=1, sampling_bins=c["cells"], dt=time_from_si(c["dt_si"]),
+              gravity=acceleration_from_si(1e9), flow_direction=c["flow"], seed=c["geom_seed"], density=2.5e24,
+              diam=3.66e-4, mass=6.63e-26 / 1.66053886e-27, Lx=L, Ly=L, Lz=L, cells_x=c["cells"],
+              cells_y=c["cells"], cells_z=c["cells"], surface=c["surface"], alpha_n=c.get("alpha_n", 0.5),
+              alpha_t=c.get("alpha_t", 0.8))
+    R, _ = rh.make_ref_system(g, st, tmp_path / "ref")
+    n, seed, steps = R.n, c["rng_seed"], 6
+    assert n > 100
+    R.init_particles(seed, n)
+    R.reset_counters()
+    o = oracle_c.Oracle(g, st, seed)
+    o.init(n)
+    r, v, _ = R.get_particles()
+    assert np.array_equal(o.r, r) and np.array_equal(o.v, v)
+    cells = R.cells()
+    assert np.array_equal(o.global_index, cells["global_index"]) and np.array_equal(o.coeff, cells["coeff"])
+    for step in range(1, steps + 1):
+        R.accelerate()
+        R.move(seed, step)
+        R.update_cells()
+        R.canonicalize()
+        R.collide(seed, step)
+        R.sample(step)
+        o.step(step)
+        o.sample()
+        r, v, cell = R.get_particles()
+        assert np.array_equal(o.r, r), step
+        assert np.array_equal(o.v, v), step
+        assert np.array_equal(o.cell_global_of_particles, cell), step
+    cells = R.cells()
+    assert np.array_equal(o.vr_max, cells["vr_max"]) and np.array_equal(o.rest, cells["rest"])
+    cnt = R.counters()
+    mine = o.counters()
+    assert mine["count_periodic"] == cnt["count_periodic"] and mine["collisions"] == cnt["collisions"]
+    if c["surface"] == "thermal":  # only the thermal collider counts wall collisions
+        assert mine["wall_collisions"] == cnt["wall_collisions"] > 0
+    assert np.array_equal(o.profile_sums(), R.profile_sums())
+    (tmp_path / "w").mkdir()
+    g.write_world(tmp_path / "w")
+    por = Geometry.read_world(tmp_path / "w" / "0000.bin").porosity_global
+    got = o.measures(st["Lx"] * st["Ly"] * st["Lz"] * por)
+    ref = R.measures()
+    for k, x in zip(MEASURES, got):
+        assert x == ref[k], k
