@@ -190,7 +190,7 @@ FRESH = {  # systems beyond the fixtures: other sizes, cells, timesteps, flow ax
 def test_oracle_matches_a_fresh_reference_run(name, tmp_path):
     """The oracle against the reference's own routines run now (the tape
     build, oracle/_ref/libdsmc_ref_tape.so), on systems the fixtures do not
-    hold: the initial state, six full steps sampled after each, every
+    hold: the initial state, 25 full steps sampled after each, every
     position, velocity, cell, counter, profile sum and measurement bit for
     bit."""
     from master_b200.system import acceleration_from_si, time_from_si
@@ -206,7 +206,7 @@ def test_oracle_matches_a_fresh_reference_run(name, tmp_path):
               Ly=L[1], Lz=L[2], cells_x=cells3[0], cells_y=cells3[1], cells_z=cells3[2], surface=c["surface"],
               alpha_n=c.get("alpha_n", 0.5), alpha_t=c.get("alpha_t", 0.8))
     R, _ = rh.make_ref_system(g, st, tmp_path / "ref")
-    n, seed, steps = R.n, c["rng_seed"], 6
+    n, seed, steps = R.n, c["rng_seed"], 25
     assert n > 100
     R.init_particles(seed, n)
     R.reset_counters()
