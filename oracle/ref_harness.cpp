@@ -68,6 +68,10 @@ void *refh_create(const char *ini_path) {
         h->settings = new Settings(std::string(ini_path));
         h->system = new System();
         h->system->initialize(h->settings, 0);
+        // System::initialize leaves t0 unset; the reference's main sets it
+        // to the start time before the first step (dsmc/main.cpp:51-52), and
+        // the flow-rate measurement divides by t - t0
+        h->system->t0 = h->system->t;
         return h;
     } catch (std::string &e) {
         std::fprintf(stderr, "refh_create: %s\n", e.c_str());
