@@ -62,12 +62,16 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
+        self.out = None
+        fd, name = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        self.path = Path(name)
 
     def __enter__(self):
+        self.out = open(self.path, "w")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.device)], stdout=open(self.path, "w"),
+                                          "-lms", "200", "-i", str(self.device)], stdout=self.out,
                                          stderr=subprocess.DEVNULL)
             time.sleep(0.3)
         except FileNotFoundError:
@@ -82,6 +86,8 @@ class ClockSampler:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+                self.proc.wait()
+        self.out.close()
 
     def summary(self):
         rows = []

@@ -152,8 +152,9 @@ class Ensemble:
         return acc
 
     def ctx_device(self) -> int:
-        import torch
-        return torch.cuda.current_device()
+        """The context's GPU (the CUDA current device may belong to another
+        context by now)."""
+        return self.ctx.device
 
     def close(self):
         self.ctx.close()

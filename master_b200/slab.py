@@ -133,7 +133,7 @@ def exchange_dist(pg, slab: Slab) -> int:
     on_gpu = pg.get_backend() == "nccl"
     if on_gpu:
         # the records stay on the GPU: owners from their voxel column there
-        dev = torch.device("cuda", torch.cuda.current_device())
+        dev = torch.device("cuda", getattr(slab.ctx, "device", torch.cuda.current_device()))
         out = slab.ctx.exchange_take_device(dev)
         dest = slab.destinations_device(out)
     else:

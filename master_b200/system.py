@@ -208,6 +208,7 @@ class Context:
         h = C.c_void_p()
         check(self.lib.dsmc_ctx_create(device, precision, C.byref(h)))
         self.handle = h
+        self.device = device
         self.precision = precision
 
     def close(self):
