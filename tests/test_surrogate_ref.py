@@ -72,3 +72,26 @@ def test_bf16_emulation_changes_the_loss_by_rounding_only():
     b = unet_ref.UNetRef(p, emulate_bf16=False).forward(solid, [0.1]).detach().numpy()
     err = np.linalg.norm(a - b) / np.linalg.norm(b)
     assert 1e-5 < err < 5e-2
+
+
+def test_committed_weights_predict_a_plausible_field():
+    """The trained weights shipped with the library (master_b200/weights/),
+    run through the CPU reference on two unseen 64^3 packs: a finite field
+    whose density averages 1 over the empty voxels (the targets are density
+    over the box mean) and whose mean drift points along the body force (x),
+    with the cross-stream means small against it."""
+    from pathlib import Path
+    from master_b200 import fields
+    z = np.load(Path(sgm.__file__).resolve().parent / "weights" / "surrogate_64.npz")
+    assert z["params"].shape == (sgm.parameter_layout()[1],)
+    net = unet_ref.UNetRef(z["params"].astype(np.float64), emulate_bf16=False)
+    for sp in fields.random_specs(2, 64, seed=9, porosity=(0.45, 0.75), knudsen=(0.3, 3.0)):
+        solid = (sp.geometry().voxels > 0).astype(np.uint8)
+        with torch.no_grad():
+            out = net.forward(solid[None], np.array([np.log10(sp.knudsen)])).numpy()[0].reshape(-1, 4)
+        empty = solid.ravel() == 0
+        assert np.isfinite(out).all()
+        assert abs(out[empty, 0].mean() - 1.0) < 0.05
+        drift = out[empty, 1:].mean(axis=0)
+        assert drift[0] > 0
+        assert np.abs(drift[1:]).max() < 0.2 * drift[0]
