@@ -205,8 +205,16 @@ def test_oracle_matches_a_fresh_reference_run(name, tmp_path):
               seed=c["geom_seed"], density=2.5e24, diam=3.66e-4, mass=6.63e-26 / 1.66053886e-27, Lx=L[0],
               Ly=L[1], Lz=L[2], cells_x=cells3[0], cells_y=cells3[1], cells_z=cells3[2], surface=c["surface"],
               alpha_n=c.get("alpha_n", 0.5), alpha_t=c.get("alpha_t", 0.8))
+    compare_with_fresh_reference(g, st, c["rng_seed"], 25, tmp_path)
+
+
+def compare_with_fresh_reference(g, st: dict, seed: int, steps: int, tmp_path) -> None:
+    """Runs the reference's own routines (the tape build) and the oracle side
+    by side from the same initial state for `steps` full steps, sampled
+    after each, and requires every position, velocity, cell, counter,
+    profile sum and measurement to be identical."""
     R, _ = rh.make_ref_system(g, st, tmp_path / "ref")
-    n, seed, steps = R.n, c["rng_seed"], 25
+    n = R.n
     assert n > 100
     R.init_particles(seed, n)
     R.reset_counters()
@@ -234,7 +242,7 @@ def test_oracle_matches_a_fresh_reference_run(name, tmp_path):
     cnt = R.counters()
     mine = o.counters()
     assert mine["count_periodic"] == cnt["count_periodic"] and mine["collisions"] == cnt["collisions"]
-    if c["surface"] == "thermal":  # only the thermal collider counts wall collisions
+    if st.get("surface", "thermal") == "thermal":  # only the thermal collider counts wall collisions
         assert mine["wall_collisions"] == cnt["wall_collisions"] > 0
     assert np.array_equal(o.profile_sums(), R.profile_sums())
     (tmp_path / "w").mkdir()
@@ -245,3 +253,18 @@ def test_oracle_matches_a_fresh_reference_run(name, tmp_path):
     for k, x in zip(MEASURES, got):
         # without gravity the reference's permeability divides by zero
         assert x == ref[k] or (np.isnan(x) and np.isnan(ref[k])), k
+
+
+@pytest.mark.skipif(not rh.available(), reason="oracle/_ref (the reference built from its sources) is not built")
+def test_oracle_matches_the_reference_on_the_plain_dsmc_workload(tmp_path):
+    """The same on the plain-DSMC workload itself (packed_64: 64^3 voxels of
+    0.1 um, spheres of r = 4 voxels to porosity 0.6, 32^3 cells, F_N = 1000,
+    about 3.9e5 particles, dt = 1e-11 s, g = 1e9 m/s^2 along x), three steps."""
+    from master_b200 import workloads
+    w = workloads.PACKED_64
+    s = w.settings(rng_seed=1, statistics_interval=1)
+    st = {k: getattr(s, k) for k in ("atoms_per_molecule", "temperature", "wall_temperature", "statistics_interval",
+                                     "sampling_bins", "dt", "gravity", "flow_direction", "seed", "density", "diam",
+                                     "mass", "Lx", "Ly", "Lz", "cells_x", "cells_y", "cells_z")}
+    st["max_molecules"] = 1_000_000
+    compare_with_fresh_reference(w.geometry(), st, 0x64C0F1, 3, tmp_path)
