@@ -174,23 +174,28 @@ def finish_field(sums: np.ndarray, solid: np.ndarray) -> np.ndarray:
     return out
 
 
-def _seed_arrays(field_out: np.ndarray, solid: np.ndarray, uniform_density: bool = False):
+def _seed_arrays(field_out: np.ndarray, solid: np.ndarray, uniform_density: bool = False,
+                 zero_drift: bool = False):
     empty = solid.ravel() == 0
     dens = np.ones(len(empty)) if uniform_density else np.maximum(field_out[:, 0], 0.0)
     w = np.ascontiguousarray(np.where(empty, dens, 0.0), np.float32)
-    drift = np.ascontiguousarray(field_out[:, 1:4] * VELOCITY_SCALE, np.float32)
+    if zero_drift:
+        drift = np.zeros((len(empty), 3), np.float32)
+    else:
+        drift = np.ascontiguousarray(field_out[:, 1:4] * VELOCITY_SCALE, np.float32)
     return w, drift
 
 
 def warm_start_many(ctx: Context, systems, field_outs, solids, counts, uniform_density: bool = False,
-                    group: int = 64) -> None:
+                    group: int = 64, zero_drift: bool = False) -> None:
     """warm_start for many systems of one context, `group` systems per
     dsmc_particles_init_field_many call (each call re-lays the context out
     once).  uniform_density: seed uniformly over the empty voxels (the cold
-    start's density) with the fields' drift."""
+    start's density) with the fields' drift; zero_drift: seed the fields'
+    density at rest (a Maxwellian without drift, as the cold start)."""
     for g0 in range(0, len(systems), group):
         sl = slice(g0, g0 + group)
-        arrs = [_seed_arrays(f, so, uniform_density) for f, so in zip(field_outs[sl], solids[sl])]
+        arrs = [_seed_arrays(f, so, uniform_density, zero_drift) for f, so in zip(field_outs[sl], solids[sl])]
         k = len(arrs)
         ids = (C.c_int * k)(*[S.id for S in systems[sl]])
         n = (C.c_int64 * k)(*[int(c) for c in counts[sl]])

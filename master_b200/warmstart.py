@@ -59,12 +59,15 @@ def seedable(pred, solid, uniform_density: bool = False) -> bool:
 def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: int = 1000, tol: float = 0.02,
             field_error: float = 0.0, max_field_error: float = 0.10, device: int = 0, rng_seed: int = 500,
             capacity: tuple | None = None, force: bool = False, measured: tuple | None = None,
-            uniform_density: bool = False, log=print) -> dict:
+            uniform_density: bool = False, zero_drift: bool = False, log=print) -> dict:
     """Runs the cold ensemble, then the warm one (one context at a time, so
     the two never share the device memory), `steps` steps each, and returns
     the steps and wall time to steady of both.  uniform_density: seed the
     particles uniformly over the empty voxels, as the cold start does, with
-    the predicted drift (the density channel left out)."""
+    the predicted drift (the density channel left out); zero_drift: seed the
+    predicted density at rest (the drift channel left out).  With
+    `measured`, the same two switches seed one channel of the DSMC's own
+    steady fields alone."""
     import torch
     rep = {"geometries": len(specs), "steps": steps, "every": every, "window": window, "hold": hold, "tol": tol,
            "surrogate_field_error": field_error, "max_field_error": max_field_error,
@@ -116,10 +119,12 @@ def compare(net, specs, steps: int, every: int = 10, window: int = 1000, hold: i
     for i, (p, solid) in enumerate(zip(preds, solids)):
         (seeded if seedable(p, solid, uniform_density) else fallback).append(i)
     fields.warm_start_many(warm.ctx, [warm.systems[i] for i in seeded], [preds[i] for i in seeded],
-                           [solids[i] for i in seeded], [counts_n[i] for i in seeded], uniform_density=uniform_density)
+                           [solids[i] for i in seeded], [counts_n[i] for i in seeded], uniform_density=uniform_density,
+                           zero_drift=zero_drift)
     warm.init_cold([warm.systems[i] for i in fallback], [counts_n[i] for i in fallback])
     rep["seed_s"] = time.perf_counter() - t0
     rep["density"] = "uniform" if uniform_density else "field"
+    rep["drift"] = "zero" if zero_drift else "field"
     rep["fallback"] = fallback
     if preds[0] is not None:
         rep["predicted_mean_drift_x"] = [float(p[(g.voxels.ravel() == 0), 1].mean()) for p, g in zip(preds, geoms)]
@@ -176,6 +181,8 @@ def main(argv=None):
                     help="control: seed from fields the DSMC measures itself instead of the network's")
     ap.add_argument("--density", choices=("field", "uniform"), default="field",
                     help="seed density: the field's, or uniform over the empty voxels with the field's drift")
+    ap.add_argument("--drift", choices=("field", "zero"), default="field",
+                    help="seed drift: the field's, or none (the field's density at rest)")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     net, held = load_net(a.weights)
@@ -183,7 +190,8 @@ def main(argv=None):
                                 per_cell=a.per_cell)
     rep = compare(net, specs, a.steps, every=a.every, field_error=float(held.get("field_error", 0.0)),
                   capacity=tuple(a.capacity) if a.capacity else None, force=a.force,
-                  measured=tuple(a.measured) if a.measured else None, uniform_density=a.density == "uniform")
+                  measured=tuple(a.measured) if a.measured else None, uniform_density=a.density == "uniform",
+                  zero_drift=a.drift == "zero")
     rep["surrogate_held_out"] = held
     if a.out:
         from pathlib import Path

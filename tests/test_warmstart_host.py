@@ -117,3 +117,14 @@ def test_held_out_summary_and_the_fallback_criterion():
     pred2 = pred.copy()
     pred2[solid == 1] = 1e6
     assert ts.summarize(pred2, solid, target, halves)[0] == s
+
+
+def test_density_only_seeding_has_no_drift():
+    """zero_drift: the field's density at rest, the control that leaves the
+    drift channel out."""
+    sums, solid = sums_and_solid()
+    out = fields.finish_field(sums, solid)
+    w, drift = fields._seed_arrays(out, solid, zero_drift=True)
+    w_field, _ = fields._seed_arrays(out, solid)
+    np.testing.assert_array_equal(w, w_field)
+    assert drift.dtype == np.float32 and drift.shape == (len(solid), 3) and not drift.any()
